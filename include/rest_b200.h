@@ -1,0 +1,156 @@
+/*
+ * rest_b200.h -- C ABI of librest_b200.so, the B200 (sm_100a) RI Coulomb /
+ * exchange Fock build of REST (jeanwsr/rest, src/scf_io).
+ *
+ * The entry points replace REST's Rust free functions one for one; each
+ * declaration names the function it stands in for (file:line in REST).  All
+ * matrices use REST's storage conventions:
+ *
+ *   MatrixFull[r, c]   column-major, element (i, j) at i + r*j
+ *   MatrixUpper        packed upper triangle, column by column:
+ *                      (i <= j) at j*(j+1)/2 + i          (npair = n(n+1)/2)
+ *   RIFull[n, n, N]    (mu, nu, P) at mu + n*nu + n*n*P   ("ri3fn")
+ *   rimatr             MatrixFull[npair, N]: column P is the packed upper
+ *                      triangle of B_P                      ("rimatr")
+ *
+ * Spin-resolved arguments are stored spin after spin: dm is spin_channel
+ * consecutive n*n matrices, eigv spin_channel consecutive n*num_state
+ * matrices, occupation spin_channel consecutive num_state vectors, and every
+ * output spin_channel consecutive results.  REST's second, one-element
+ * placeholder slot for spin_channel == 1 is not written.
+ *
+ * Conventions: every call returns a status (RIJK_OK == 0).  Host pointers stay
+ * owned by the caller; device memory is owned by the context.  Host-pointer
+ * calls are synchronous; the *_dev calls take device pointers and enqueue on
+ * the given stream (NULL = the context's stream) without synchronising.  A
+ * context is not thread-safe: use one per host thread.  There is no CPU
+ * fallback: without a usable sm_100 device rijk_ctx_create fails.
+ */
+#ifndef REST_B200_H
+#define REST_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum rijk_status {
+  RIJK_OK = 0,
+  RIJK_ERR_ARG = 1,        /* invalid argument (sizes, null pointers, spin)        */
+  RIJK_ERR_CUDA = 2,       /* CUDA runtime error; see rijk_ctx_last_error           */
+  RIJK_ERR_NOT_SPD = 3,    /* metric not positive definite (failing pivot given)   */
+  RIJK_ERR_NO_TENSOR = 4,  /* no fitted tensor loaded in the context               */
+  RIJK_ERR_TIMEOUT = 5,    /* a device-side wait ran out of its time budget         */
+  RIJK_ERR_NOMEM = 6,      /* device allocation failed                              */
+  RIJK_ERR_NONFINITE = 7,  /* NaN/Inf found in an input                             */
+  RIJK_ERR_TOO_LARGE = 8   /* size beyond a documented maximum                      */
+};
+
+typedef struct rijk_ctx rijk_ctx;
+
+/* ---- context --------------------------------------------------------------- */
+int rijk_ctx_create(int device, rijk_ctx** out);
+int rijk_ctx_destroy(rijk_ctx* ctx);
+const char* rijk_ctx_last_error(const rijk_ctx* ctx);
+const char* rijk_status_string(int status);
+/* Sizes of the loaded tensor (0 if none) and device bytes it occupies. */
+int rijk_ctx_info(const rijk_ctx* ctx, int64_t* num_basis, int64_t* num_auxbas, int64_t* tensor_bytes);
+/* The context's CUDA stream (a cudaStream_t). */
+void* rijk_ctx_stream(rijk_ctx* ctx);
+/* Device pointer of the tile-packed tensor and its row stride in doubles. */
+int rijk_ctx_tensor(rijk_ctx* ctx, const double** d_tensor, int64_t* row_stride);
+/* Wait for the work enqueued on `stream` (NULL = the context's stream) and
+ * report a device-side timeout recorded since the last check. */
+int rijk_ctx_synchronize(rijk_ctx* ctx, void* stream);
+
+/* ---- fitted tensor producers ------------------------------------------------ */
+/* Load a fitted tensor computed elsewhere.
+ * Replaces the SCF::rimatr produced by prepare_rimatr_for_ri_v_rayon_v02
+ * (src/molecule_io/mod.rs:1563-1721), consumed by the _rimatr_ functions. */
+int rijk_set_rimatr(rijk_ctx* ctx, const double* rimatr, int64_t num_basis, int64_t num_auxbas);
+/* Replaces the SCF::ri3fn produced by prepare_ri3fn_for_ri_v_full_rayon
+ * (src/molecule_io/mod.rs:1275-1393).  The upper triangle of each B_P is used. */
+int rijk_set_ri3fn(rijk_ctx* ctx, const double* ri3fn, int64_t num_basis, int64_t num_auxbas);
+/* Download the context's tensor as rimatr (npair x num_auxbas). */
+int rijk_get_rimatr(rijk_ctx* ctx, double* rimatr);
+/* Tensors produced on the device (e.g. by a device integral engine): allocate a
+ * zero tensor for (num_basis, num_auxbas), then load aux rows [p0, p0+np) from
+ * device memory, rimatr rows (layout 0, npair doubles each) or ri3fn blocks
+ * (layout 1, n*n doubles each).  Same roles as rijk_set_rimatr/_ri3fn. */
+int rijk_tensor_alloc(rijk_ctx* ctx, int64_t num_basis, int64_t num_auxbas);
+int rijk_tensor_load_rows_dev(rijk_ctx* ctx, const double* d_rows, int64_t p0, int64_t np, int layout,
+                              void* stream);
+
+/* Metric step on the device: V = (P|Q) (num_auxbas^2, column-major) is
+ * Cholesky-factored, V = L L^T, and the three-centre integrals int3c
+ * ((mu nu|P) in rimatr layout) are fitted as B = int3c L^-T.  This is the
+ * Cholesky variant REST keeps beside its live V^-1/2 whitening
+ * (src/molecule_io/mod.rs:1582-1583, :1672-1675).  On RIJK_ERR_NOT_SPD,
+ * *failed_pivot (if non-NULL) holds the 1-based index of the first
+ * non-positive pivot; otherwise 0. */
+int rijk_build_rimatr_cholesky(rijk_ctx* ctx, const double* aux_v, const double* int3c, int64_t num_basis,
+                               int64_t num_auxbas, int64_t* failed_pivot);
+/* Fit with a caller-supplied metric factor M (num_auxbas^2, column-major):
+ * B = int3c M, i.e. the _dgemm(tmp_ovlp_matr, aux_v) of
+ * src/molecule_io/mod.rs:1672-1675 with aux_v = V^-1/2 from lapack_power. */
+int rijk_fit_rimatr(rijk_ctx* ctx, const double* metric_factor, const double* int3c, int64_t num_basis,
+                    int64_t num_auxbas);
+
+/* ---- Coulomb (J) ------------------------------------------------------------ */
+/* vj_upper_with_ri_v_sync (src/scf_io/mod.rs:2428-2488):
+ * per P, w_P = sum_{mu,nu} B_P[mu,nu] D[mu,nu]; J = scaling_factor sum_P upper(B_P) w_P.
+ * dm: spin_channel x (n x n); vj: spin_channel x npair. */
+int rijk_vj_upper_with_ri_v(rijk_ctx* ctx, const double* dm, int spin_channel, double scaling_factor, double* vj);
+/* vj_upper_with_rimatr_v_sync (src/scf_io/mod.rs:2490-2561):
+ * w_P = 2 sum_{mu<=nu} B[P,mu nu] D_{mu nu} - sum_mu B[P,mu mu] D_{mu mu}. */
+int rijk_vj_upper_with_rimatr_v(rijk_ctx* ctx, const double* dm, int spin_channel, double scaling_factor,
+                                double* vj);
+/* vj_full_with_ri_v (src/scf_io/mod.rs:2564-2602): full n x n J per spin. */
+int rijk_vj_full_with_ri_v(rijk_ctx* ctx, const double* dm, int spin_channel, double scaling_factor, double* vj_full);
+
+/* ---- exchange (K) ----------------------------------------------------------- */
+/* vk_upper_with_ri_v_sync (src/scf_io/mod.rs:2758-2834), occupied-orbital form:
+ * per P, X = B_P C[:, :homo+1], K += X diag(occ) X^T; vk = scaling_factor upper(K).
+ * eigv: spin_channel x (n x num_state); homo[spin]; occupation: spin_channel x
+ * num_state (entries >= 0). */
+int rijk_vk_upper_with_ri_v(rijk_ctx* ctx, const double* eigv, int64_t num_state, const int64_t* homo,
+                            const double* occupation, int spin_channel, double scaling_factor, double* vk);
+/* vk_upper_with_ri_v_use_dm_only_sync (src/scf_io/mod.rs:2640-2701):
+ * per P, K += B_P D B_P (both B_P symmetric from their upper triangle). */
+int rijk_vk_upper_with_ri_v_use_dm_only(rijk_ctx* ctx, const double* dm, int spin_channel, double scaling_factor,
+                                        double* vk);
+/* vk_upper_with_rimatr_use_dm_only_sync (src/scf_io/mod.rs:2703-2756): the same
+ * contraction for a tensor loaded as rimatr. */
+int rijk_vk_upper_with_rimatr_use_dm_only(rijk_ctx* ctx, const double* dm, int spin_channel, double scaling_factor,
+                                          double* vk);
+/* vk_full_fromdm_with_ri_v (src/scf_io/mod.rs:2603-2638): K = sum_P B_P D B_P^T
+ * for an arbitrary (possibly non-symmetric) D; full n x n output per spin. */
+int rijk_vk_full_fromdm_with_ri_v(rijk_ctx* ctx, const double* dm, int spin_channel, double scaling_factor,
+                                  double* vk_full);
+
+/* ---- device-resident forms (same semantics, device pointers) ----------------- */
+/* dm_mode 0 = rijk_vj_upper_with_ri_v, 1 = rijk_vj_upper_with_rimatr_v. */
+int rijk_vj_upper_dev(rijk_ctx* ctx, const double* d_dm, int spin_channel, double scaling_factor, int dm_mode,
+                      double* d_vj, void* stream);
+/* d_homo is a host array; d_eigv / d_occupation / d_vk are device arrays. */
+int rijk_vk_upper_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int64_t* homo,
+                          const double* d_occupation, int spin_channel, double scaling_factor, double* d_vk,
+                          void* stream);
+int rijk_vk_upper_dm_dev(rijk_ctx* ctx, const double* d_dm, int spin_channel, double scaling_factor, double* d_vk,
+                         void* stream);
+
+/* ---- SCF pieces around the build ------------------------------------------- */
+/* generate_density_matrix (src/scf_io/mod.rs:441-478): D = (C occ) C^T over the
+ * first homo+1 columns, per spin; dm: spin_channel x (n x n). */
+int rijk_density_matrix(rijk_ctx* ctx, const double* eigv, int64_t num_basis, int64_t num_state,
+                        const int64_t* homo, const double* occupation, int spin_channel, double* dm);
+/* SCF::par_energy_contraction (src/scf_io/mod.rs:1787-1802):
+ * 1/2 sum_ij a_ij b_ij from two MatrixUpper of length npair. */
+double rijk_energy_contraction(const double* a_upper, const double* b_upper, int64_t npair);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* REST_B200_H */

@@ -1,0 +1,632 @@
+// C ABI of librest_b200.so: context, tensor producers and the REST-shaped
+// vj/vk entry points (declared in include/rest_b200.h).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+
+#include <algorithm>
+#include <string>
+
+#include "../../include/rest_b200.h"
+#include "rijk_common.cuh"
+#include "rijk_internal.h"
+
+using rijk::Geom;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+int64_t round_up(int64_t a, int64_t b) { return cdiv(a, b) * b; }
+
+}  // namespace
+
+struct rijk_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Geom g;
+  bool have = false;
+  int64_t naux_pad = 0;
+  double* dB = nullptr;
+  size_t dB_bytes = 0;
+  int* d_err = nullptr;   // device-side wait timeouts
+  int* d_info = nullptr;  // Cholesky failing pivot
+  DevBuf stage, W, w, Jpart, Cw, X, Kpart, din, dout, docc, mV, mLinv, mT, mLinvd, mOut;
+  size_t scratch_budget = (size_t)4 << 30;
+  std::string last;
+};
+
+namespace {
+
+int set_err(rijk_ctx* c, int code, const std::string& msg) {
+  if (c) c->last = msg;
+  return code;
+}
+
+int cuda_fail(rijk_ctx* c, cudaError_t e, const char* what) {
+  return set_err(c, RIJK_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define RIJK_CK(call)                                         \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);  \
+  } while (0)
+
+int ensure(rijk_ctx* ctx, DevBuf& b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.bytes >= bytes) return RIJK_OK;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, RIJK_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  b.bytes = bytes;
+  return RIJK_OK;
+}
+
+#define RIJK_TRY(x)               \
+  do {                            \
+    int r_ = (x);                 \
+    if (r_ != RIJK_OK) return r_; \
+  } while (0)
+
+cudaStream_t pick(rijk_ctx* ctx, void* s) { return s ? static_cast<cudaStream_t>(s) : ctx->stream; }
+
+// Launch errors are reported immediately; device-side timeouts at the next sync.
+int after_launch(rijk_ctx* ctx, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, what);
+  return RIJK_OK;
+}
+
+int sync_and_check(rijk_ctx* ctx, cudaStream_t st) {
+  RIJK_CK(cudaStreamSynchronize(st));
+  int h = 0;
+  RIJK_CK(cudaMemcpy(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h != 0) {
+    RIJK_CK(cudaMemset(ctx->d_err, 0, sizeof(int)));
+    return set_err(ctx, RIJK_ERR_TIMEOUT, "a device-side wait exceeded its time budget");
+  }
+  return RIJK_OK;
+}
+
+int check_spin(rijk_ctx* ctx, int spin) {
+  if (spin != 1 && spin != 2) return set_err(ctx, RIJK_ERR_ARG, "spin_channel must be 1 or 2");
+  return RIJK_OK;
+}
+
+int need_tensor(rijk_ctx* ctx) {
+  if (!ctx) return RIJK_ERR_ARG;
+  if (!ctx->have) return set_err(ctx, RIJK_ERR_NO_TENSOR, "no fitted tensor loaded");
+  RIJK_CK(cudaSetDevice(ctx->device));
+  return RIJK_OK;
+}
+
+// Allocate the tile-packed tensor for (n, naux); pad rows are zero.
+int alloc_tensor(rijk_ctx* ctx, int64_t n, int64_t naux) {
+  if (n <= 0 || naux <= 0) return set_err(ctx, RIJK_ERR_ARG, "num_basis and num_auxbas must be positive");
+  if (n > 46000) return set_err(ctx, RIJK_ERR_TOO_LARGE, "num_basis above 46000");
+  Geom g = rijk::make_geom(n, naux);
+  const int64_t naux_pad = round_up(naux, rijk::TS);
+  const size_t bytes = (size_t)naux_pad * g.ldB * sizeof(double);
+  if (ctx->dB && ctx->dB_bytes != bytes) {
+    cudaFree(ctx->dB);
+    ctx->dB = nullptr;
+    ctx->dB_bytes = 0;
+  }
+  if (!ctx->dB) {
+    cudaError_t e = cudaMalloc(&ctx->dB, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      ctx->dB = nullptr;
+      ctx->have = false;
+      return set_err(ctx, RIJK_ERR_NOMEM, "tensor allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    ctx->dB_bytes = bytes;
+  }
+  if (naux_pad > naux)
+    RIJK_CK(cudaMemsetAsync(ctx->dB + naux * g.ldB, 0, (size_t)(naux_pad - naux) * g.ldB * sizeof(double),
+                            ctx->stream));
+  ctx->g = g;
+  ctx->naux_pad = naux_pad;
+  ctx->have = false;
+  return RIJK_OK;
+}
+
+// Upload a host tensor (rimatr rows of npair, or ri3fn blocks of n*n) in chunks.
+int upload_tensor(rijk_ctx* ctx, const double* host, int64_t n, int64_t naux, int kind) {
+  RIJK_CK(cudaSetDevice(ctx->device));
+  RIJK_TRY(alloc_tensor(ctx, n, naux));
+  const Geom& g = ctx->g;
+  const int64_t row = kind == 0 ? g.npair : n * n;
+  const int64_t rows_per = std::max<int64_t>(1, std::min<int64_t>(naux, ((int64_t)256 << 20) / (row * 8)));
+  RIJK_TRY(ensure(ctx, ctx->stage, (size_t)rows_per * row * 8));
+  double* st = static_cast<double*>(ctx->stage.p);
+  for (int64_t p0 = 0; p0 < naux; p0 += rows_per) {
+    const int64_t np = std::min(rows_per, naux - p0);
+    RIJK_CK(cudaMemcpyAsync(st, host + p0 * row, (size_t)np * row * 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (kind == 0)
+      rijk::launch_pack_rimatr(g, st, np, ctx->dB + p0 * g.ldB, ctx->stream);
+    else
+      rijk::launch_pack_ri3fn(g, st, np, ctx->dB + p0 * g.ldB, ctx->stream);
+    RIJK_TRY(after_launch(ctx, "pack tensor"));
+  }
+  RIJK_TRY(sync_and_check(ctx, ctx->stream));
+  ctx->have = true;
+  return RIJK_OK;
+}
+
+int upload_square_padded(rijk_ctx* ctx, const double* host, int64_t n, int64_t np, DevBuf& dst) {
+  RIJK_TRY(ensure(ctx, ctx->stage, (size_t)n * n * 8));
+  RIJK_TRY(ensure(ctx, dst, (size_t)np * np * 8));
+  RIJK_CK(cudaMemcpyAsync(ctx->stage.p, host, (size_t)n * n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  rijk::launch_pad_matrix(static_cast<double*>(ctx->stage.p), n, np, static_cast<double*>(dst.p), ctx->stream);
+  return after_launch(ctx, "pad metric");
+}
+
+}  // namespace
+
+namespace rijk {
+void launch_fit_copy_back(const double* out, int64_t kc, double* dB, int64_t ldB, int64_t k0, int64_t rows,
+                          cudaStream_t st);
+}
+
+namespace {
+
+// B <- B * F (F = L^-T with klim upper, or a dense factor), chunked over the
+// stored columns k so that the product never overwrites its own input.
+int fit_in_place(rijk_ctx* ctx, const double* dF, int64_t ldf, int tb, int klim) {
+  const Geom& g = ctx->g;
+  const int64_t np = ctx->naux_pad;
+  int64_t chunk = std::max<int64_t>(1024, (((int64_t)512 << 20) / (np * 8)) / 1024 * 1024);
+  chunk = std::min(chunk, g.ldB);
+  RIJK_TRY(ensure(ctx, ctx->mOut, (size_t)chunk * np * 8));
+  double* out = static_cast<double*>(ctx->mOut.p);
+  for (int64_t k0 = 0; k0 < g.ldB; k0 += chunk) {
+    const int64_t kc = std::min(chunk, g.ldB - k0);
+    rijk::launch_dgemm(kc, np, np, 1.0, ctx->dB + k0, g.ldB, 0, dF, ldf, tb, 0.0, out, kc, klim, 0, 1, 0, 0, 0,
+                       ctx->d_err, ctx->stream);
+    RIJK_TRY(after_launch(ctx, "fit gemm"));
+    rijk::launch_fit_copy_back(out, kc, ctx->dB, g.ldB, k0, np, ctx->stream);
+    RIJK_TRY(after_launch(ctx, "fit copy"));
+  }
+  return RIJK_OK;
+}
+
+// ---- J ----------------------------------------------------------------------
+int vj_dev(rijk_ctx* ctx, const double* d_dm, int spin, double scale, int mode, int out_kind, double* d_out,
+           cudaStream_t st) {
+  const Geom& g = ctx->g;
+  const int splits = rijk::j_pass2_splits(g);
+  RIJK_TRY(ensure(ctx, ctx->W, (size_t)spin * g.ldB * 8));
+  RIJK_TRY(ensure(ctx, ctx->w, (size_t)spin * g.naux * 8));
+  RIJK_TRY(ensure(ctx, ctx->Jpart, (size_t)splits * spin * g.ldB * 8));
+  double* W = static_cast<double*>(ctx->W.p);
+  double* w = static_cast<double*>(ctx->w.p);
+  double* Jp = static_cast<double*>(ctx->Jpart.p);
+  rijk::launch_j_weights(g, d_dm, spin, mode, W, st);
+  rijk::launch_j_pass1(g, ctx->dB, W, spin, w, st);
+  rijk::launch_j_pass2(g, ctx->dB, w, spin, splits, Jp, st);
+  rijk::launch_j_finalize(g, Jp, spin, splits, scale, out_kind, d_out, st);
+  return after_launch(ctx, "vj");
+}
+
+// ---- K, occupied-orbital form -------------------------------------------------
+int vk_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int64_t* homo, const double* d_occ,
+               int spin, double scale, double* d_out, cudaStream_t st) {
+  const Geom& g = ctx->g;
+  int64_t nw[2] = {0, 0};
+  for (int s = 0; s < spin; ++s) {
+    nw[s] = homo[s] + 1;
+    if (homo[s] < 0 || nw[s] > num_state) return set_err(ctx, RIJK_ERR_ARG, "homo out of range");
+  }
+  const int64_t ldx = round_up(g.n, 128);
+  const int64_t coff[2] = {0, round_up(nw[0], rijk::TS)};
+  const int64_t ocols = round_up(spin == 2 ? coff[1] + nw[1] : nw[0], 64);
+  RIJK_TRY(ensure(ctx, ctx->Cw, (size_t)ldx * ocols * 8));
+  double* Cw = static_cast<double*>(ctx->Cw.p);
+  rijk::launch_k_prepare_c(g, d_eigv, g.n, g.n * num_state, d_occ, num_state, nw, spin, ldx, ocols, Cw, st);
+  const int64_t per_p = ldx * ocols * 8;
+  const int64_t pchunk = std::max<int64_t>(1, std::min<int64_t>(g.naux, (int64_t)ctx->scratch_budget / per_p));
+  RIJK_TRY(ensure(ctx, ctx->X, (size_t)pchunk * per_p));
+  const int splits_max = rijk::k_rank_splits(g, pchunk, 0);
+  RIJK_TRY(ensure(ctx, ctx->Kpart, (size_t)splits_max * rijk::k_block_pairs(g, 0) * 128 * 128 * 8));
+  double* X = static_cast<double*>(ctx->X.p);
+  double* Kp = static_cast<double*>(ctx->Kpart.p);
+  for (int64_t p0 = 0; p0 < g.naux; p0 += pchunk) {
+    const int64_t np = std::min(pchunk, g.naux - p0);
+    rijk::launch_half_transform(g, ctx->dB, p0, np, Cw, ldx, ocols, X, ldx, ldx * ocols, ctx->d_err, st);
+    for (int s = 0; s < spin; ++s) {
+      if (nw[s] == 0) continue;
+      const int splits = rijk::k_rank_splits(g, np, 0);
+      rijk::launch_k_rank_update(g, X, ldx, ldx * ocols, np, coff[s], nw[s], splits, 0, Kp, ctx->d_err, st);
+      rijk::launch_k_finalize(g, Kp, splits, 0, scale, p0 > 0 ? 1 : 0, 0, d_out + s * g.npair, st);
+    }
+  }
+  return after_launch(ctx, "vk occ");
+}
+
+// ---- K, density form ----------------------------------------------------------
+int vk_dm_dev(rijk_ctx* ctx, const double* d_dm, int spin, double scale, int full, double* d_out, cudaStream_t st) {
+  const Geom& g = ctx->g;
+  const int64_t ldx = round_up(g.n, 128);
+  RIJK_TRY(ensure(ctx, ctx->Cw, (size_t)ldx * ldx * 8));
+  double* Dp = static_cast<double*>(ctx->Cw.p);
+  const int64_t per_p = ldx * ldx * 8;
+  const int64_t pchunk = std::max<int64_t>(1, std::min<int64_t>(g.naux, (int64_t)ctx->scratch_budget / per_p));
+  RIJK_TRY(ensure(ctx, ctx->X, (size_t)pchunk * per_p));
+  const int splits_max = rijk::k_rank_splits(g, pchunk, full);
+  RIJK_TRY(ensure(ctx, ctx->Kpart, (size_t)splits_max * rijk::k_block_pairs(g, full) * 128 * 128 * 8));
+  double* T = static_cast<double*>(ctx->X.p);
+  double* Kp = static_cast<double*>(ctx->Kpart.p);
+  const int64_t per_out = full ? g.n * g.n : g.npair;
+  for (int s = 0; s < spin; ++s) {
+    rijk::launch_pad_square(d_dm + s * g.n * g.n, g.n, g.n, ldx, Dp, st);
+    for (int64_t p0 = 0; p0 < g.naux; p0 += pchunk) {
+      const int64_t np = std::min(pchunk, g.naux - p0);
+      rijk::launch_half_transform(g, ctx->dB, p0, np, Dp, ldx, ldx, T, ldx, ldx * ldx, ctx->d_err, st);
+      const int splits = rijk::k_rank_splits(g, np, full);
+      rijk::launch_k_dm_update(g, T, ldx, ldx * ldx, ctx->dB, p0, np, splits, full, Kp, ctx->d_err, st);
+      rijk::launch_k_finalize(g, Kp, splits, full, scale, p0 > 0 ? 1 : 0, full ? 1 : 0, d_out + s * per_out, st);
+    }
+  }
+  return after_launch(ctx, "vk dm");
+}
+
+// Host-pointer wrapper: copy inputs in, run, copy the result out, synchronise.
+template <class F>
+int host_call(rijk_ctx* ctx, const double* h_in, size_t in_doubles, double* h_out, size_t out_doubles, F&& body) {
+  RIJK_TRY(ensure(ctx, ctx->din, in_doubles * 8));
+  RIJK_TRY(ensure(ctx, ctx->dout, out_doubles * 8));
+  double* din = static_cast<double*>(ctx->din.p);
+  double* dout = static_cast<double*>(ctx->dout.p);
+  RIJK_CK(cudaMemcpyAsync(din, h_in, in_doubles * 8, cudaMemcpyHostToDevice, ctx->stream));
+  RIJK_TRY(body(din, dout));
+  RIJK_CK(cudaMemcpyAsync(h_out, dout, out_doubles * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_and_check(ctx, ctx->stream);
+}
+
+}  // namespace
+
+// ============================================================================
+// extern "C"
+// ============================================================================
+extern "C" {
+
+const char* rijk_status_string(int status) {
+  switch (status) {
+    case RIJK_OK: return "ok";
+    case RIJK_ERR_ARG: return "invalid argument";
+    case RIJK_ERR_CUDA: return "CUDA error";
+    case RIJK_ERR_NOT_SPD: return "metric is not positive definite";
+    case RIJK_ERR_NO_TENSOR: return "no fitted tensor loaded";
+    case RIJK_ERR_TIMEOUT: return "device-side wait timed out";
+    case RIJK_ERR_NOMEM: return "device out of memory";
+    case RIJK_ERR_NONFINITE: return "non-finite input";
+    case RIJK_ERR_TOO_LARGE: return "size above the supported maximum";
+    default: return "unknown status";
+  }
+}
+
+int rijk_ctx_create(int device, rijk_ctx** out) {
+  if (!out) return RIJK_ERR_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+    cudaGetLastError();
+    return RIJK_ERR_CUDA;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return RIJK_ERR_CUDA;
+  if (prop.major != 10) return RIJK_ERR_CUDA;  // built for sm_100a only
+  if (cudaSetDevice(device) != cudaSuccess) return RIJK_ERR_CUDA;
+  rijk_ctx* c = new rijk_ctx();
+  c->device = device;
+  if (const char* s = getenv("RIJK_SCRATCH_BYTES")) {
+    const long long v = atoll(s);
+    if (v > (1 << 20)) c->scratch_budget = (size_t)v;
+  }
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess || cudaMalloc(&c->d_info, sizeof(int)) != cudaSuccess ||
+      cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess || cudaMemset(c->d_info, 0, sizeof(int)) != cudaSuccess) {
+    rijk_ctx_destroy(c);
+    return RIJK_ERR_CUDA;
+  }
+  *out = c;
+  return RIJK_OK;
+}
+
+int rijk_ctx_destroy(rijk_ctx* ctx) {
+  if (!ctx) return RIJK_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  DevBuf* bufs[] = {&ctx->stage, &ctx->W,   &ctx->w,    &ctx->Jpart, &ctx->Cw,    &ctx->X,      &ctx->Kpart, &ctx->din,
+                    &ctx->dout,  &ctx->docc, &ctx->mV, &ctx->mLinv, &ctx->mT, &ctx->mLinvd, &ctx->mOut};
+  for (DevBuf* b : bufs)
+    if (b->p) cudaFree(b->p);
+  if (ctx->dB) cudaFree(ctx->dB);
+  if (ctx->d_err) cudaFree(ctx->d_err);
+  if (ctx->d_info) cudaFree(ctx->d_info);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return RIJK_OK;
+}
+
+const char* rijk_ctx_last_error(const rijk_ctx* ctx) { return ctx ? ctx->last.c_str() : "null context"; }
+
+int rijk_ctx_info(const rijk_ctx* ctx, int64_t* num_basis, int64_t* num_auxbas, int64_t* tensor_bytes) {
+  if (!ctx) return RIJK_ERR_ARG;
+  if (num_basis) *num_basis = ctx->have ? ctx->g.n : 0;
+  if (num_auxbas) *num_auxbas = ctx->have ? ctx->g.naux : 0;
+  if (tensor_bytes) *tensor_bytes = ctx->have ? (int64_t)ctx->dB_bytes : 0;
+  return RIJK_OK;
+}
+
+void* rijk_ctx_stream(rijk_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int rijk_ctx_tensor(rijk_ctx* ctx, const double** d_tensor, int64_t* row_stride) {
+  RIJK_TRY(need_tensor(ctx));
+  if (d_tensor) *d_tensor = ctx->dB;
+  if (row_stride) *row_stride = ctx->g.ldB;
+  return RIJK_OK;
+}
+
+int rijk_ctx_synchronize(rijk_ctx* ctx, void* stream) {
+  if (!ctx) return RIJK_ERR_ARG;
+  RIJK_CK(cudaSetDevice(ctx->device));
+  return sync_and_check(ctx, pick(ctx, stream));
+}
+
+int rijk_set_rimatr(rijk_ctx* ctx, const double* rimatr, int64_t num_basis, int64_t num_auxbas) {
+  if (!ctx || !rimatr) return set_err(ctx, RIJK_ERR_ARG, "null argument");
+  return upload_tensor(ctx, rimatr, num_basis, num_auxbas, 0);
+}
+
+int rijk_set_ri3fn(rijk_ctx* ctx, const double* ri3fn, int64_t num_basis, int64_t num_auxbas) {
+  if (!ctx || !ri3fn) return set_err(ctx, RIJK_ERR_ARG, "null argument");
+  return upload_tensor(ctx, ri3fn, num_basis, num_auxbas, 1);
+}
+
+int rijk_tensor_alloc(rijk_ctx* ctx, int64_t num_basis, int64_t num_auxbas) {
+  if (!ctx) return RIJK_ERR_ARG;
+  RIJK_CK(cudaSetDevice(ctx->device));
+  RIJK_TRY(alloc_tensor(ctx, num_basis, num_auxbas));
+  RIJK_CK(cudaMemsetAsync(ctx->dB, 0, ctx->dB_bytes, ctx->stream));
+  RIJK_TRY(sync_and_check(ctx, ctx->stream));
+  ctx->have = true;
+  return RIJK_OK;
+}
+
+int rijk_tensor_load_rows_dev(rijk_ctx* ctx, const double* d_rows, int64_t p0, int64_t np, int layout,
+                              void* stream) {
+  RIJK_TRY(need_tensor(ctx));
+  if (!d_rows || p0 < 0 || np <= 0 || p0 + np > ctx->g.naux || (layout != 0 && layout != 1))
+    return set_err(ctx, RIJK_ERR_ARG, "bad row range or layout");
+  if (layout == 0)
+    rijk::launch_pack_rimatr(ctx->g, d_rows, np, ctx->dB + p0 * ctx->g.ldB, pick(ctx, stream));
+  else
+    rijk::launch_pack_ri3fn(ctx->g, d_rows, np, ctx->dB + p0 * ctx->g.ldB, pick(ctx, stream));
+  return after_launch(ctx, "load rows");
+}
+
+int rijk_get_rimatr(rijk_ctx* ctx, double* rimatr) {
+  RIJK_TRY(need_tensor(ctx));
+  if (!rimatr) return set_err(ctx, RIJK_ERR_ARG, "null argument");
+  const Geom& g = ctx->g;
+  const int64_t rows_per = std::max<int64_t>(1, std::min<int64_t>(g.naux, ((int64_t)256 << 20) / (g.npair * 8)));
+  RIJK_TRY(ensure(ctx, ctx->stage, (size_t)rows_per * g.npair * 8));
+  double* st = static_cast<double*>(ctx->stage.p);
+  for (int64_t p0 = 0; p0 < g.naux; p0 += rows_per) {
+    const int64_t np = std::min(rows_per, g.naux - p0);
+    rijk::launch_unpack_rimatr(g, ctx->dB + p0 * g.ldB, np, st, ctx->stream);
+    RIJK_TRY(after_launch(ctx, "unpack tensor"));
+    RIJK_CK(cudaMemcpyAsync(rimatr + p0 * g.npair, st, (size_t)np * g.npair * 8, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  }
+  return sync_and_check(ctx, ctx->stream);
+}
+
+int rijk_build_rimatr_cholesky(rijk_ctx* ctx, const double* aux_v, const double* int3c, int64_t num_basis,
+                               int64_t num_auxbas, int64_t* failed_pivot) {
+  if (failed_pivot) *failed_pivot = 0;
+  if (!ctx || !aux_v || !int3c) return set_err(ctx, RIJK_ERR_ARG, "null argument");
+  RIJK_TRY(upload_tensor(ctx, int3c, num_basis, num_auxbas, 0));
+  ctx->have = false;
+  const int64_t np = ctx->naux_pad;
+  RIJK_TRY(upload_square_padded(ctx, aux_v, num_auxbas, np, ctx->mV));
+  RIJK_TRY(ensure(ctx, ctx->mLinvd, (size_t)np * rijk::TS * 8));
+  RIJK_TRY(ensure(ctx, ctx->mLinv, (size_t)np * np * 8));
+  RIJK_TRY(ensure(ctx, ctx->mT, (size_t)np * np * 8));
+  double* V = static_cast<double*>(ctx->mV.p);
+  double* Linvd = static_cast<double*>(ctx->mLinvd.p);
+  double* Linv = static_cast<double*>(ctx->mLinv.p);
+  double* T = static_cast<double*>(ctx->mT.p);
+  RIJK_CK(cudaMemsetAsync(ctx->d_info, 0, sizeof(int), ctx->stream));
+  rijk::run_potrf(V, np, np, Linvd, ctx->d_info, ctx->d_err, ctx->stream);
+  RIJK_TRY(after_launch(ctx, "potrf"));
+  RIJK_TRY(sync_and_check(ctx, ctx->stream));
+  int info = 0;
+  RIJK_CK(cudaMemcpy(&info, ctx->d_info, sizeof(int), cudaMemcpyDeviceToHost));
+  if (info != 0) {
+    if (failed_pivot) *failed_pivot = info;
+    return set_err(ctx, RIJK_ERR_NOT_SPD, "metric not positive definite at pivot " + std::to_string(info));
+  }
+  rijk::run_trtri(V, np, np, Linvd, Linv, T, ctx->d_err, ctx->stream);
+  RIJK_TRY(after_launch(ctx, "trtri"));
+  // B^T = L^-1 (Q|mu nu)  <=>  B[k, P] = sum_Q int3c[k, Q] Linv[P, Q]
+  RIJK_TRY(fit_in_place(ctx, Linv, np, 1, 2));
+  RIJK_TRY(sync_and_check(ctx, ctx->stream));
+  ctx->have = true;
+  return RIJK_OK;
+}
+
+int rijk_fit_rimatr(rijk_ctx* ctx, const double* metric_factor, const double* int3c, int64_t num_basis,
+                    int64_t num_auxbas) {
+  if (!ctx || !metric_factor || !int3c) return set_err(ctx, RIJK_ERR_ARG, "null argument");
+  RIJK_TRY(upload_tensor(ctx, int3c, num_basis, num_auxbas, 0));
+  ctx->have = false;
+  const int64_t np = ctx->naux_pad;
+  RIJK_TRY(upload_square_padded(ctx, metric_factor, num_auxbas, np, ctx->mV));
+  RIJK_TRY(fit_in_place(ctx, static_cast<double*>(ctx->mV.p), np, 0, 0));
+  RIJK_TRY(sync_and_check(ctx, ctx->stream));
+  ctx->have = true;
+  return RIJK_OK;
+}
+
+// ---- J ------------------------------------------------------------------------
+int rijk_vj_upper_dev(rijk_ctx* ctx, const double* d_dm, int spin_channel, double scaling_factor, int dm_mode,
+                      double* d_vj, void* stream) {
+  RIJK_TRY(need_tensor(ctx));
+  RIJK_TRY(check_spin(ctx, spin_channel));
+  if (!d_dm || !d_vj || (dm_mode != 0 && dm_mode != 1)) return set_err(ctx, RIJK_ERR_ARG, "bad argument");
+  return vj_dev(ctx, d_dm, spin_channel, scaling_factor, dm_mode, 0, d_vj, pick(ctx, stream));
+}
+
+static int vj_host(rijk_ctx* ctx, const double* dm, int spin, double scale, int mode, int out_kind, double* out) {
+  RIJK_TRY(need_tensor(ctx));
+  RIJK_TRY(check_spin(ctx, spin));
+  if (!dm || !out) return set_err(ctx, RIJK_ERR_ARG, "null argument");
+  const Geom& g = ctx->g;
+  const size_t per = out_kind == 0 ? (size_t)g.npair : (size_t)(g.n * g.n);
+  return host_call(ctx, dm, (size_t)spin * g.n * g.n, out, spin * per, [&](double* din, double* dout) {
+    return vj_dev(ctx, din, spin, scale, mode, out_kind, dout, ctx->stream);
+  });
+}
+
+int rijk_vj_upper_with_ri_v(rijk_ctx* ctx, const double* dm, int spin_channel, double scaling_factor, double* vj) {
+  return vj_host(ctx, dm, spin_channel, scaling_factor, 0, 0, vj);
+}
+int rijk_vj_upper_with_rimatr_v(rijk_ctx* ctx, const double* dm, int spin_channel, double scaling_factor,
+                                double* vj) {
+  return vj_host(ctx, dm, spin_channel, scaling_factor, 1, 0, vj);
+}
+int rijk_vj_full_with_ri_v(rijk_ctx* ctx, const double* dm, int spin_channel, double scaling_factor, double* vj_full) {
+  return vj_host(ctx, dm, spin_channel, scaling_factor, 0, 1, vj_full);
+}
+
+// ---- K ------------------------------------------------------------------------
+int rijk_vk_upper_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int64_t* homo,
+                          const double* d_occupation, int spin_channel, double scaling_factor, double* d_vk,
+                          void* stream) {
+  RIJK_TRY(need_tensor(ctx));
+  RIJK_TRY(check_spin(ctx, spin_channel));
+  if (!d_eigv || !homo || !d_occupation || !d_vk || num_state <= 0)
+    return set_err(ctx, RIJK_ERR_ARG, "bad argument");
+  return vk_occ_dev(ctx, d_eigv, num_state, homo, d_occupation, spin_channel, scaling_factor, d_vk,
+                    pick(ctx, stream));
+}
+
+int rijk_vk_upper_with_ri_v(rijk_ctx* ctx, const double* eigv, int64_t num_state, const int64_t* homo,
+                            const double* occupation, int spin_channel, double scaling_factor, double* vk) {
+  RIJK_TRY(need_tensor(ctx));
+  RIJK_TRY(check_spin(ctx, spin_channel));
+  if (!eigv || !homo || !occupation || !vk || num_state <= 0) return set_err(ctx, RIJK_ERR_ARG, "bad argument");
+  for (int s = 0; s < spin_channel; ++s) {
+    if (homo[s] < 0 || homo[s] >= num_state) return set_err(ctx, RIJK_ERR_ARG, "homo out of range");
+    for (int64_t i = 0; i <= homo[s]; ++i)
+      if (!(occupation[s * num_state + i] >= 0.0)) return set_err(ctx, RIJK_ERR_ARG, "negative occupation");
+  }
+  const Geom& g = ctx->g;
+  const size_t ne = (size_t)spin_channel * g.n * num_state;
+  RIJK_TRY(ensure(ctx, ctx->docc, (size_t)spin_channel * num_state * 8));
+  RIJK_CK(cudaMemcpyAsync(ctx->docc.p, occupation, (size_t)spin_channel * num_state * 8, cudaMemcpyHostToDevice,
+                          ctx->stream));
+  return host_call(ctx, eigv, ne, vk, (size_t)spin_channel * g.npair, [&](double* din, double* dout) {
+    return vk_occ_dev(ctx, din, num_state, homo, static_cast<double*>(ctx->docc.p), spin_channel, scaling_factor,
+                      dout, ctx->stream);
+  });
+}
+
+int rijk_vk_upper_dm_dev(rijk_ctx* ctx, const double* d_dm, int spin_channel, double scaling_factor, double* d_vk,
+                         void* stream) {
+  RIJK_TRY(need_tensor(ctx));
+  RIJK_TRY(check_spin(ctx, spin_channel));
+  if (!d_dm || !d_vk) return set_err(ctx, RIJK_ERR_ARG, "bad argument");
+  return vk_dm_dev(ctx, d_dm, spin_channel, scaling_factor, 0, d_vk, pick(ctx, stream));
+}
+
+static int vk_dm_host(rijk_ctx* ctx, const double* dm, int spin, double scale, int full, double* out) {
+  RIJK_TRY(need_tensor(ctx));
+  RIJK_TRY(check_spin(ctx, spin));
+  if (!dm || !out) return set_err(ctx, RIJK_ERR_ARG, "null argument");
+  const Geom& g = ctx->g;
+  const size_t per = full ? (size_t)(g.n * g.n) : (size_t)g.npair;
+  return host_call(ctx, dm, (size_t)spin * g.n * g.n, out, spin * per, [&](double* din, double* dout) {
+    return vk_dm_dev(ctx, din, spin, scale, full, dout, ctx->stream);
+  });
+}
+
+int rijk_vk_upper_with_ri_v_use_dm_only(rijk_ctx* ctx, const double* dm, int spin_channel, double scaling_factor,
+                                        double* vk) {
+  return vk_dm_host(ctx, dm, spin_channel, scaling_factor, 0, vk);
+}
+int rijk_vk_upper_with_rimatr_use_dm_only(rijk_ctx* ctx, const double* dm, int spin_channel, double scaling_factor,
+                                          double* vk) {
+  return vk_dm_host(ctx, dm, spin_channel, scaling_factor, 0, vk);
+}
+int rijk_vk_full_fromdm_with_ri_v(rijk_ctx* ctx, const double* dm, int spin_channel, double scaling_factor,
+                                  double* vk_full) {
+  return vk_dm_host(ctx, dm, spin_channel, scaling_factor, 1, vk_full);
+}
+
+// ---- density matrix and energy -----------------------------------------------
+int rijk_density_matrix(rijk_ctx* ctx, const double* eigv, int64_t num_basis, int64_t num_state, const int64_t* homo,
+                        const double* occupation, int spin_channel, double* dm) {
+  if (!ctx || !eigv || !homo || !occupation || !dm || num_basis <= 0 || num_state <= 0)
+    return set_err(ctx, RIJK_ERR_ARG, "bad argument");
+  RIJK_TRY(check_spin(ctx, spin_channel));
+  RIJK_CK(cudaSetDevice(ctx->device));
+  const int64_t n = num_basis;
+  const int64_t ld = round_up(n, 128);
+  Geom g = rijk::make_geom(n, 1);
+  RIJK_TRY(ensure(ctx, ctx->din, (size_t)spin_channel * n * num_state * 8));
+  RIJK_TRY(ensure(ctx, ctx->docc, (size_t)spin_channel * num_state * 8));
+  RIJK_TRY(ensure(ctx, ctx->dout, (size_t)spin_channel * ld * ld * 8));
+  double* din = static_cast<double*>(ctx->din.p);
+  double* dout = static_cast<double*>(ctx->dout.p);
+  RIJK_CK(cudaMemcpyAsync(din, eigv, (size_t)spin_channel * n * num_state * 8, cudaMemcpyHostToDevice, ctx->stream));
+  RIJK_CK(cudaMemcpyAsync(ctx->docc.p, occupation, (size_t)spin_channel * num_state * 8, cudaMemcpyHostToDevice,
+                          ctx->stream));
+  for (int s = 0; s < spin_channel; ++s) {
+    const int64_t nw[2] = {homo[s] + 1, 0};
+    if (homo[s] < 0 || nw[0] > num_state) return set_err(ctx, RIJK_ERR_ARG, "homo out of range");
+    for (int64_t i = 0; i < nw[0]; ++i)
+      if (!(occupation[s * num_state + i] >= 0.0)) return set_err(ctx, RIJK_ERR_ARG, "negative occupation");
+    const int64_t kc = round_up(nw[0], 64);
+    RIJK_TRY(ensure(ctx, ctx->Cw, (size_t)ld * kc * 8));
+    double* Cw = static_cast<double*>(ctx->Cw.p);
+    rijk::launch_k_prepare_c(g, din + s * n * num_state, n, 0, static_cast<double*>(ctx->docc.p) + s * num_state, 0,
+                             nw, 1, ld, kc, Cw, ctx->stream);
+    rijk::launch_dgemm(ld, ld, kc, 1.0, Cw, ld, 0, Cw, ld, 1, 0.0, dout + s * ld * ld, ld, 0, 0, 1, 0, 0, 0,
+                       ctx->d_err, ctx->stream);
+    RIJK_TRY(after_launch(ctx, "density"));
+  }
+  for (int s = 0; s < spin_channel; ++s)
+    RIJK_CK(cudaMemcpy2DAsync(dm + s * n * n, n * 8, dout + s * ld * ld, ld * 8, n * 8, n, cudaMemcpyDeviceToHost,
+                              ctx->stream));
+  return sync_and_check(ctx, ctx->stream);
+}
+
+double rijk_energy_contraction(const double* a, const double* b, int64_t npair) {
+  if (!a || !b || npair <= 0) return 0.0;
+  double tot = 0.0, dg = 0.0;
+  for (int64_t k = 0; k < npair; ++k) tot += a[k] * b[k];
+  for (int64_t j = 0;; ++j) {
+    const int64_t d = j * (j + 1) / 2 + j;
+    if (d >= npair) break;
+    dg += a[d] * b[d];
+  }
+  return (2.0 * tot - dg) * 0.5;
+}
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+// Host-side launchers of the RI J/K kernels (internal to librest_b200.so).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rijk {
+
+// Geometry of the tile-packed tensor held by a context.
+struct Geom {
+  int64_t n = 0;      // num_basis
+  int64_t naux = 0;   // num_auxbas
+  int64_t nt = 0;     // ceil(n / 32)
+  int64_t ntp = 0;    // nt (nt + 1) / 2
+  int64_t ldB = 0;    // ntp * 1024 doubles per aux row
+  int64_t npair = 0;  // n (n + 1) / 2
+};
+Geom make_geom(int64_t n, int64_t naux);
+
+// --- layout conversion -------------------------------------------------------
+// rimatr (REST MatrixFull[npair, N], column P = packed upper of B_P), rows
+// [p0, p0 + np) -> tile-packed rows [p0, p0 + np) of dB.
+void launch_pack_rimatr(const Geom& g, const double* src, int64_t np, double* dst, cudaStream_t st);
+// ri3fn (REST RIFull[n,n,N]), aux rows [p0, p0+np): upper triangle is the source.
+void launch_pack_ri3fn(const Geom& g, const double* src, int64_t np, double* dst, cudaStream_t st);
+// tile-packed rows -> rimatr rows.
+void launch_unpack_rimatr(const Geom& g, const double* src, int64_t np, double* dst, cudaStream_t st);
+
+// --- J ------------------------------------------------------------------------
+// mode 0: full n*n dot (vj_upper_with_ri_v); mode 1: packed-upper formula
+// (vj_upper_with_rimatr_v).  dm: nspin matrices n*n column-major, stride n*n.
+void launch_j_weights(const Geom& g, const double* dm, int nspin, int mode, double* W, cudaStream_t st);
+// w[s*naux + P] = sum_k B[P,k] W[s*ldB + k]
+void launch_j_pass1(const Geom& g, const double* B, const double* W, int nspin, double* w, cudaStream_t st);
+// number of P-splits pass 2 uses (scratch = splits * nspin * ldB doubles)
+int j_pass2_splits(const Geom& g);
+void launch_j_pass2(const Geom& g, const double* B, const double* w, int nspin, int splits, double* Jpart,
+                    cudaStream_t st);
+// out_kind 0: packed upper (nspin x npair); 1: full n x n (nspin x n*n)
+void launch_j_finalize(const Geom& g, const double* Jpart, int nspin, int splits, double scale, int out_kind,
+                       double* out, cudaStream_t st);
+
+// --- K ------------------------------------------------------------------------
+// Cw[s] (ldc x ocols, column-major, zero padded) = C_s[:, :nw_s] * sqrt(occ_s)
+void launch_k_prepare_c(const Geom& g, const double* eigv, int64_t ld_eigv, int64_t stride_eigv,
+                        const double* occ, int64_t stride_occ, const int64_t* nw, int nspin, int64_t ldc,
+                        int64_t ocols, double* Cw, cudaStream_t st);
+// dense n x n (ld = n) -> padded ldc x ldc copy (zero padding)
+void launch_pad_square(const double* src, int64_t n, int64_t ldsrc, int64_t ldc, double* dst, cudaStream_t st);
+
+// X[p] = B_{p0+p} * W for p in [0, np): W is ldw x ncol (ncol multiple of 64),
+// X[p] is ldx x ncol column-major with ldx = round_up(n, 128), stride sxp.
+void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
+                           int64_t ncol, double* X, int64_t ldx, int64_t sxp, int* err, cudaStream_t st);
+// Kpart[split][q] (128x128 blocks q over block pairs) = sum over p in split,
+// columns [c0, c0+ncol) of X:  X_p X_p^T.  full = 0: pairs Ib<=Jb; 1: all pairs.
+int k_rank_splits(const Geom& g, int64_t np, int full);
+void launch_k_rank_update(const Geom& g, const double* X, int64_t ldx, int64_t sxp, int64_t np, int64_t c0,
+                          int64_t ncol, int splits, int full, double* Kpart, int* err, cudaStream_t st);
+// Kpart[split][q] = sum_p T_p B_{p0+p}  (dm form: T_p = B_p D)
+void launch_k_dm_update(const Geom& g, const double* T, int64_t ldt, int64_t stp, const double* B, int64_t p0,
+                        int64_t np, int splits, int full, double* Kpart, int* err, cudaStream_t st);
+int64_t k_block_pairs(const Geom& g, int full);
+// out (+)= scale * sum_split Kpart; out_kind 0: packed upper, 1: full n x n.
+void launch_k_finalize(const Geom& g, const double* Kpart, int splits, int full, double scale, int accumulate,
+                       int out_kind, double* out, cudaStream_t st);
+
+// --- dense FP64 GEMM on the DMMA mainloop (metric step) -----------------------
+// C[MxN] = alpha op(A) op(B) + beta C, all column-major, M,N,K multiples of 32,
+// pointers 16-byte aligned, leading dimensions even.  klim: bit 0 = op(A)
+// lower (k <= m), bit 1 = op(B) upper (k <= n), bit 2 = op(A) upper (k >= m),
+// bit 3 = op(B) lower (k >= n).  lower_only: skip C blocks above the diagonal.
+// batch: gridDim.z copies with element offsets sa, sb, sc between them.
+void launch_dgemm(int64_t M, int64_t N, int64_t K, double alpha, const double* A, int64_t lda, int ta,
+                  const double* B, int64_t ldb, int tb, double beta, double* C, int64_t ldc, int klim, int lower_only,
+                  int batch, int64_t sa, int64_t sb, int64_t sc, int* err, cudaStream_t st);
+
+// --- metric -----------------------------------------------------------------
+// In-place lower Cholesky of the np x np (np multiple of 32) matrix A (lda).
+// Linvd receives the inverses of the 32x32 diagonal blocks.  *d_info = first
+// failing pivot (1-based) or 0.
+void run_potrf(double* A, int64_t np, int64_t lda, double* Linvd, int* d_info, int* err, cudaStream_t st);
+// Linv (np x np, ld) = inverse of the lower-triangular L (ld); T is np x np scratch.
+void run_trtri(const double* L, int64_t np, int64_t ld, const double* Linvd, double* Linv, double* T, int* err,
+               cudaStream_t st);
+// Copy a dense n x n (ld n) matrix into a zero-padded np x np (ld np) buffer.
+void launch_pad_matrix(const double* src, int64_t n, int64_t np, double* dst, cudaStream_t st);
+
+}  // namespace rijk

@@ -1,0 +1,577 @@
+// RI J/K kernels on the tile-packed fitted tensor (FP64 plain form).
+//
+// J (REST vj_upper_with_ri_v_sync / vj_upper_with_rimatr_v_sync,
+// src/scf_io/mod.rs:2428-2561) is HBM-bound and runs as two streaming passes:
+//   pass 1  w_P = sum_k B[P,k] W[k]   (W = D folded into the tile layout)
+//   pass 2  J_k = sum_P B[P,k] w_P    (split over P, partials reduced in order)
+// K (vk_upper_with_ri_v_sync, :2758-2834; dm forms :2640-2756) runs on the FP64
+// tensor cores (DMMA) as a batched half-transform X_P = B_P C followed by a
+// split-k rank update K = sum_P X_P X_P^T over 128x128 blocks of K.
+#include <math.h>
+
+#include <algorithm>
+
+#include "rijk_dmma.cuh"
+#include "rijk_internal.h"
+
+namespace rijk {
+
+Geom make_geom(int64_t n, int64_t naux) {
+  Geom g;
+  g.n = n;
+  g.naux = naux;
+  g.nt = (n + TS - 1) / TS;
+  g.ntp = g.nt * (g.nt + 1) / 2;
+  g.ldB = g.ntp * TILE_ELEMS;
+  g.npair = n * (n + 1) / 2;
+  return g;
+}
+
+static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+static inline int64_t round_up(int64_t a, int64_t b) { return cdiv(a, b) * b; }
+
+// Largest J with J (J + 1) / 2 <= t.
+__device__ __forceinline__ int64_t tri_root(int64_t t) {
+  int64_t j = (int64_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while (j * (j + 1) / 2 > t) --j;
+  while ((j + 1) * (j + 2) / 2 <= t) ++j;
+  return j;
+}
+
+// ============================================================================
+// layout conversion
+// ============================================================================
+// One CTA per stored tile (blockIdx.x), aux rows strided over blockIdx.y.
+// src_kind 0: rimatr rows (npair each); 1: ri3fn blocks (n*n each).
+__global__ void __launch_bounds__(256) k_pack(int64_t n, int64_t npair, int64_t ldB, const double* __restrict__ src,
+                                              int src_kind, int64_t np, double* __restrict__ dst) {
+  const int64_t t = blockIdx.x;
+  const int64_t J = tri_root(t), I = t - J * (J + 1) / 2;
+  for (int64_t p = blockIdx.y; p < np; p += gridDim.y) {
+    for (int e = threadIdx.x; e < TILE_ELEMS; e += blockDim.x) {
+      const int r = e & 31, c = e >> 5;
+      const int64_t mu = I * TS + r, nu = J * TS + c;
+      double v = 0.0;
+      if (mu < n && nu < n) {
+        const int64_t i = mu < nu ? mu : nu, j = mu < nu ? nu : mu;
+        v = src_kind == 0 ? src[p * npair + packed_upper_index(i, j)] : src[p * n * n + i + n * j];
+      }
+      dst[p * ldB + t * TILE_ELEMS + e] = v;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_unpack_rimatr(int64_t n, int64_t npair, int64_t ldB,
+                                                       const double* __restrict__ src, int64_t np,
+                                                       double* __restrict__ dst) {
+  for (int64_t p = blockIdx.y; p < np; p += gridDim.y) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < npair; t += (int64_t)gridDim.x * blockDim.x) {
+      const int64_t j = tri_root(t), i = t - j * (j + 1) / 2;
+      const int64_t tile = tile_pair_index(i / TS, j / TS);
+      dst[p * npair + t] = src[p * ldB + tile * TILE_ELEMS + (i % TS) + TS * (j % TS)];
+    }
+  }
+}
+
+void launch_pack_rimatr(const Geom& g, const double* src, int64_t np, double* dst, cudaStream_t st) {
+  if (np <= 0) return;
+  dim3 grid((unsigned)g.ntp, (unsigned)std::min<int64_t>(np, 65535));
+  k_pack<<<grid, 256, 0, st>>>(g.n, g.npair, g.ldB, src, 0, np, dst);
+}
+void launch_pack_ri3fn(const Geom& g, const double* src, int64_t np, double* dst, cudaStream_t st) {
+  if (np <= 0) return;
+  dim3 grid((unsigned)g.ntp, (unsigned)std::min<int64_t>(np, 65535));
+  k_pack<<<grid, 256, 0, st>>>(g.n, g.npair, g.ldB, src, 1, np, dst);
+}
+void launch_unpack_rimatr(const Geom& g, const double* src, int64_t np, double* dst, cudaStream_t st) {
+  if (np <= 0) return;
+  dim3 grid((unsigned)std::min<int64_t>(cdiv(g.npair, 256), 4096), (unsigned)std::min<int64_t>(np, 65535));
+  k_unpack_rimatr<<<grid, 256, 0, st>>>(g.n, g.npair, g.ldB, src, np, dst);
+}
+
+// ============================================================================
+// J
+// ============================================================================
+// W[s*ldB + k]: the density folded onto the stored tile elements so that
+// w_P = sum_k B[P,k] W[k] reproduces REST's per-P scalar:
+//   mode 0 (full dot, scf_io/mod.rs:2451-2457): off-diagonal tiles carry
+//          D[mu,nu] + D[nu,mu], diagonal tiles D[mu,nu] (both triangles stored);
+//   mode 1 (packed formula, :2513-2527): off-diagonal tiles 2 D[mu,nu] (mu < nu),
+//          diagonal tiles D[min, max], which sums to 2 sum_{mu<=nu} - sum_diag.
+__global__ void __launch_bounds__(256) k_j_weights(int64_t n, int64_t ldB, const double* __restrict__ dm, int nspin,
+                                                   int mode, double* __restrict__ W) {
+  const int64_t total = (int64_t)nspin * ldB;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = e / ldB, k = e - s * ldB;
+    const int64_t t = k >> 10;
+    const int rc = (int)(k & 1023), r = rc & 31, c = rc >> 5;
+    const int64_t J = tri_root(t), I = t - J * (J + 1) / 2;
+    const int64_t mu = I * TS + r, nu = J * TS + c;
+    double v = 0.0;
+    if (mu < n && nu < n) {
+      const double* D = dm + s * n * n;
+      if (I < J) {
+        v = mode == 0 ? D[mu + n * nu] + D[nu + n * mu] : 2.0 * D[mu + n * nu];
+      } else {
+        const int64_t i = mu < nu ? mu : nu, j = mu < nu ? nu : mu;
+        v = mode == 0 ? D[mu + n * nu] : D[i + n * j];
+      }
+    }
+    W[e] = v;
+  }
+}
+
+void launch_j_weights(const Geom& g, const double* dm, int nspin, int mode, double* W, cudaStream_t st) {
+  const int64_t total = nspin * g.ldB;
+  const unsigned blocks = (unsigned)std::min<int64_t>(cdiv(total, 256), 148 * 16);
+  k_j_weights<<<blocks, 256, 0, st>>>(g.n, g.ldB, dm, nspin, mode, W);
+}
+
+__device__ __forceinline__ double2 ld_stream(const double2* p) { return __ldcs(p); }
+
+template <int NS>
+__device__ __forceinline__ void block_reduce_store(double (&s)[NS], double* out, int64_t stride) {
+  __shared__ double red[NS][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NS; ++i)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s[i] += __shfl_xor_sync(0xffffffffu, s[i], o);
+  if (lane == 0)
+#pragma unroll
+    for (int i = 0; i < NS; ++i) red[i][warp] = s[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+      double t = 0.0;
+      for (int w = 0; w < nw; ++w) t += red[i][w];
+      out[i * stride] = t;
+    }
+  }
+}
+
+// Pass 1: one CTA per aux row P; the row streams once from HBM (evict-first),
+// the weights stay in L2.  Fixed summation order: deterministic.
+template <int NS>
+__global__ void __launch_bounds__(256) k_j_pass1(const double* __restrict__ B, const double* __restrict__ W,
+                                                 int64_t ldB, int64_t naux, double* __restrict__ w) {
+  const int64_t P = blockIdx.x;
+  const double2* b = reinterpret_cast<const double2*>(B + P * ldB);
+  const double2* w0 = reinterpret_cast<const double2*>(W);
+  const double2* w1 = reinterpret_cast<const double2*>(W + ldB);
+  const int64_t nq = ldB / 2;
+  double s[NS];
+  double s2[NS];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) s[i] = s2[i] = 0.0;
+  int64_t q = threadIdx.x;
+  constexpr int U = 4;
+  for (; q + (U - 1) * 256 < nq; q += U * 256) {
+    double2 x[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) x[u] = ld_stream(b + q + u * 256);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const double2 a = __ldg(w0 + q + u * 256);
+      s[0] = fma(x[u].x, a.x, s[0]);
+      s2[0] = fma(x[u].y, a.y, s2[0]);
+      if (NS == 2) {
+        const double2 c = __ldg(w1 + q + u * 256);
+        s[NS - 1] = fma(x[u].x, c.x, s[NS - 1]);
+        s2[NS - 1] = fma(x[u].y, c.y, s2[NS - 1]);
+      }
+    }
+  }
+  for (; q < nq; q += 256) {
+    const double2 xv = ld_stream(b + q);
+    const double2 a = __ldg(w0 + q);
+    s[0] = fma(xv.x, a.x, s[0]);
+    s2[0] = fma(xv.y, a.y, s2[0]);
+    if (NS == 2) {
+      const double2 c = __ldg(w1 + q);
+      s[NS - 1] = fma(xv.x, c.x, s[NS - 1]);
+      s2[NS - 1] = fma(xv.y, c.y, s2[NS - 1]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NS; ++i) s[i] += s2[i];
+  block_reduce_store<NS>(s, w + P, naux);
+}
+
+void launch_j_pass1(const Geom& g, const double* B, const double* W, int nspin, double* w, cudaStream_t st) {
+  if (nspin == 2)
+    k_j_pass1<2><<<(unsigned)g.naux, 256, 0, st>>>(B, W, g.ldB, g.naux, w);
+  else
+    k_j_pass1<1><<<(unsigned)g.naux, 256, 0, st>>>(B, W, g.ldB, g.naux, w);
+}
+
+int j_pass2_splits(const Geom& g) {
+  const int64_t threads_per_split = g.ldB / 2;
+  const int64_t target = 148LL * 2048 * 2;
+  int64_t s = cdiv(target, threads_per_split);
+  s = std::max<int64_t>(1, std::min<int64_t>(s, std::min<int64_t>(g.naux, 64)));
+  return (int)s;
+}
+
+// Pass 2: each thread owns two adjacent stored elements (16 bytes) and walks
+// the aux rows of its split; warps read 512 contiguous bytes per row.
+template <int NS>
+__global__ void __launch_bounds__(256) k_j_pass2(const double* __restrict__ B, const double* __restrict__ w,
+                                                 int64_t ldB, int64_t naux, int splits, double* __restrict__ Jpart) {
+  const int64_t nq = ldB / 2;
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int sp = blockIdx.y;
+  const int64_t p0 = naux * sp / splits, p1 = naux * (sp + 1) / splits;
+  if (q >= nq) return;
+  const double2* b = reinterpret_cast<const double2*>(B) + q;
+  double2 a[NS];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) a[i] = make_double2(0.0, 0.0);
+  int64_t p = p0;
+  constexpr int U = 4;
+  for (; p + U - 1 < p1; p += U) {
+    double2 x[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) x[u] = ld_stream(b + (p + u) * nq);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+#pragma unroll
+      for (int i = 0; i < NS; ++i) {
+        const double wp = __ldg(w + i * naux + p + u);
+        a[i].x = fma(x[u].x, wp, a[i].x);
+        a[i].y = fma(x[u].y, wp, a[i].y);
+      }
+    }
+  }
+  for (; p < p1; ++p) {
+    const double2 xv = ld_stream(b + p * nq);
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+      const double wp = __ldg(w + i * naux + p);
+      a[i].x = fma(xv.x, wp, a[i].x);
+      a[i].y = fma(xv.y, wp, a[i].y);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NS; ++i) reinterpret_cast<double2*>(Jpart + ((int64_t)sp * NS + i) * ldB)[q] = a[i];
+}
+
+void launch_j_pass2(const Geom& g, const double* B, const double* w, int nspin, int splits, double* Jpart,
+                    cudaStream_t st) {
+  dim3 grid((unsigned)cdiv(g.ldB / 2, 256), (unsigned)splits);
+  if (nspin == 2)
+    k_j_pass2<2><<<grid, 256, 0, st>>>(B, w, g.ldB, g.naux, splits, Jpart);
+  else
+    k_j_pass2<1><<<grid, 256, 0, st>>>(B, w, g.ldB, g.naux, splits, Jpart);
+}
+
+__global__ void __launch_bounds__(256) k_j_finalize(int64_t n, int64_t npair, int64_t ldB,
+                                                    const double* __restrict__ Jpart, int nspin, int splits,
+                                                    double scale, int out_kind, double* __restrict__ out) {
+  const int64_t per = out_kind == 0 ? npair : n * n;
+  const int64_t total = nspin * per;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = e / per, t = e - s * per;
+    int64_t i, j;
+    if (out_kind == 0) {
+      j = tri_root(t);
+      i = t - j * (j + 1) / 2;
+    } else {
+      const int64_t mu = t % n, nu = t / n;
+      i = mu < nu ? mu : nu;
+      j = mu < nu ? nu : mu;
+    }
+    const int64_t k = tile_pair_index(i / TS, j / TS) * TILE_ELEMS + (i % TS) + TS * (j % TS);
+    double v = 0.0;
+    for (int sp = 0; sp < splits; ++sp) v += Jpart[((int64_t)sp * nspin + s) * ldB + k];
+    out[e] = v * scale;
+  }
+}
+
+void launch_j_finalize(const Geom& g, const double* Jpart, int nspin, int splits, double scale, int out_kind,
+                       double* out, cudaStream_t st) {
+  const int64_t total = nspin * (out_kind == 0 ? g.npair : g.n * g.n);
+  const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), 148 * 16));
+  k_j_finalize<<<blocks, 256, 0, st>>>(g.n, g.npair, g.ldB, Jpart, nspin, splits, scale, out_kind, out);
+}
+
+// ============================================================================
+// K
+// ============================================================================
+// Right operand of the half-transform: the occupied columns of each spin,
+// scaled by sqrt(occupation), so that (B_P Cw)(B_P Cw)^T = B_P C occ C^T B_P
+// (REST forms Y = X diag(occ) and Y X^T, scf_io/mod.rs:2797-2803).  Spin s
+// occupies columns [coff_s, coff_s + nw_s) with coff_1 = round_up(nw_0, 32).
+__global__ void __launch_bounds__(256) k_prepare_c(int64_t n, const double* __restrict__ eigv, int64_t ld_eigv,
+                                                   int64_t stride_eigv, const double* __restrict__ occ,
+                                                   int64_t stride_occ, int64_t nw0, int64_t nw1, int64_t coff1,
+                                                   int nspin, int64_t ldc, int64_t ocols, double* __restrict__ Cw) {
+  const int64_t total = ldc * ocols;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = e % ldc, col = e / ldc;
+    double v = 0.0;
+    int s = -1;
+    int64_t i = 0;
+    if (col < nw0) {
+      s = 0;
+      i = col;
+    } else if (nspin == 2 && col >= coff1 && col < coff1 + nw1) {
+      s = 1;
+      i = col - coff1;
+    }
+    if (s >= 0 && row < n) v = eigv[s * stride_eigv + row + ld_eigv * i] * sqrt(occ[s * stride_occ + i]);
+    Cw[e] = v;
+  }
+}
+
+void launch_k_prepare_c(const Geom& g, const double* eigv, int64_t ld_eigv, int64_t stride_eigv, const double* occ,
+                        int64_t stride_occ, const int64_t* nw, int nspin, int64_t ldc, int64_t ocols, double* Cw,
+                        cudaStream_t st) {
+  const int64_t coff1 = round_up(nw[0], TS);
+  const int64_t total = ldc * ocols;
+  const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), 148 * 16));
+  k_prepare_c<<<blocks, 256, 0, st>>>(g.n, eigv, ld_eigv, stride_eigv, occ, stride_occ, nw[0], nspin == 2 ? nw[1] : 0,
+                                      coff1, nspin, ldc, ocols, Cw);
+}
+
+__global__ void __launch_bounds__(256) k_pad_square(const double* __restrict__ src, int64_t n, int64_t ldsrc,
+                                                    int64_t ldc, double* __restrict__ dst) {
+  const int64_t total = ldc * ldc;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e % ldc, c = e / ldc;
+    dst[e] = (r < n && c < n) ? src[r + ldsrc * c] : 0.0;
+  }
+}
+
+void launch_pad_square(const double* src, int64_t n, int64_t ldsrc, int64_t ldc, double* dst, cudaStream_t st) {
+  const int64_t total = ldc * ldc;
+  const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), 148 * 16));
+  k_pad_square<<<blocks, 256, 0, st>>>(src, n, ldsrc, ldc, dst);
+}
+
+// ---- half-transform: X_p = B_p W ------------------------------------------
+using HtCfg = DmmaCfg<2, 2, 2, 2, 3>;  // 64 x 64 CTA tile, 4 warps of 32 x 32
+
+struct HalfTransformSched {
+  const double* Bp;  // row P of the tile-packed tensor
+  const double* W;
+  int64_t ldw;
+  int nt, I0, col0;
+  __device__ SlotSrc a(int kt, int mt) const {
+    const int I = I0 + mt, J = kt;
+    if (I >= nt) return {nullptr, TS, 0};
+    if (I <= J) return {Bp + tile_pair_index(I, J) * TILE_ELEMS, TS, 0};
+    return {Bp + tile_pair_index(J, I) * TILE_ELEMS, TS, 1};
+  }
+  __device__ SlotSrc b(int kt, int ntl) const {
+    return {W + (int64_t)kt * TS + (int64_t)(col0 + ntl * TS) * ldw, ldw, 0};
+  }
+};
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS) k_half_transform(const double* __restrict__ B, int64_t ldB, int64_t p0,
+                                                                 int nrb, const double* __restrict__ W, int64_t ldw,
+                                                                 int nt, double* __restrict__ X, int64_t ldx,
+                                                                 int64_t sxp, int* err) {
+  extern __shared__ __align__(128) double smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_DOUBLES);
+  const int64_t rb = blockIdx.x;
+  const int64_t pl = rb / nrb;
+  const int I0 = (int)(rb % nrb) * Cfg::MT;
+  const int col0 = blockIdx.y * Cfg::BN;
+  HalfTransformSched sc{B + (p0 + pl) * ldB, W, ldw, nt, I0, col0};
+  double acc[Cfg::FM][Cfg::FN][2];
+  if (!dmma_mainloop<Cfg>(sc, nt, smem, bars, acc, err)) return;
+  double* Xp = X + pl * sxp + (int64_t)I0 * TS + (int64_t)col0 * ldx;
+  dmma_for_each<Cfg>(acc, [&](int m, int n, double v0, double v1) {
+    Xp[m + (int64_t)n * ldx] = v0;
+    Xp[m + (int64_t)(n + 1) * ldx] = v1;
+  });
+}
+
+void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
+                           int64_t ncol, double* X, int64_t ldx, int64_t sxp, int* err, cudaStream_t st) {
+  using Cfg = HtCfg;
+  cudaFuncSetAttribute(k_half_transform<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+  const int nrb = (int)(ldx / Cfg::BM);
+  dim3 grid((unsigned)(np * nrb), (unsigned)(ncol / Cfg::BN));
+  k_half_transform<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(B, g.ldB, p0, nrb, W, ldw, (int)g.nt, X, ldx,
+                                                                      sxp, err);
+}
+
+// ---- rank update: Kpart = sum_p X_p X_p^T ------------------------------------
+using RkCfg = DmmaCfg<4, 4, 2, 4, 3>;  // 128 x 128 CTA tile, 8 warps of 64 x 32
+constexpr int KB = RkCfg::BM;          // K block edge (128)
+
+int64_t k_block_pairs(const Geom& g, int full) {
+  const int64_t nkb = cdiv(g.n, KB);
+  return full ? nkb * nkb : nkb * (nkb + 1) / 2;
+}
+
+__device__ __forceinline__ void block_pair(int64_t q, int full, int64_t nkb, int64_t& Ib, int64_t& Jb) {
+  if (full) {
+    Ib = q % nkb;
+    Jb = q / nkb;
+  } else {
+    Jb = tri_root(q);
+    Ib = q - Jb * (Jb + 1) / 2;
+  }
+}
+
+int k_rank_splits(const Geom& g, int64_t np, int full) {
+  const int64_t pairs = k_block_pairs(g, full);
+  int64_t s = cdiv(2 * 148, pairs);
+  s = std::max<int64_t>(1, std::min<int64_t>(s, np));
+  return (int)s;
+}
+
+struct RankSched {
+  const double* X;
+  int64_t ldx, sxp;
+  int64_t p0;
+  int ctiles, c0t;  // column tiles per P, first column tile
+  int64_t mrow0, nrow0;
+  __device__ SlotSrc a(int kt, int mt) const {
+    const int64_t p = p0 + kt / ctiles;
+    const int ic = c0t + kt % ctiles;
+    return {X + p * sxp + mrow0 + mt * TS + (int64_t)ic * TS * ldx, ldx, 0};
+  }
+  __device__ SlotSrc b(int kt, int ntl) const {
+    const int64_t p = p0 + kt / ctiles;
+    const int ic = c0t + kt % ctiles;
+    return {X + p * sxp + nrow0 + ntl * TS + (int64_t)ic * TS * ldx, ldx, 1};
+  }
+};
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS) k_rank_update(const double* __restrict__ X, int64_t ldx, int64_t sxp,
+                                                              int64_t np, int c0t, int ctiles, int splits, int full,
+                                                              int64_t nkb, int64_t pairs, double* __restrict__ Kpart,
+                                                              int* err) {
+  extern __shared__ __align__(128) double smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_DOUBLES);
+  const int64_t q = blockIdx.x;
+  const int sp = blockIdx.y;
+  int64_t Ib, Jb;
+  block_pair(q, full, nkb, Ib, Jb);
+  const int64_t pa = np * sp / splits, pb = np * (sp + 1) / splits;
+  RankSched sc{X, ldx, sxp, pa, ctiles, c0t, Ib * Cfg::BM, Jb * Cfg::BN};
+  double acc[Cfg::FM][Cfg::FN][2];
+  const int ktiles = (int)((pb - pa) * ctiles);
+  if (!dmma_mainloop<Cfg>(sc, ktiles, smem, bars, acc, err)) return;
+  double* out = Kpart + ((int64_t)sp * pairs + q) * (Cfg::BM * Cfg::BN);
+  dmma_for_each<Cfg>(acc, [&](int m, int n, double v0, double v1) {
+    out[m + Cfg::BM * n] = v0;
+    out[m + Cfg::BM * (n + 1)] = v1;
+  });
+}
+
+void launch_k_rank_update(const Geom& g, const double* X, int64_t ldx, int64_t sxp, int64_t np, int64_t c0,
+                          int64_t ncol, int splits, int full, double* Kpart, int* err, cudaStream_t st) {
+  using Cfg = RkCfg;
+  cudaFuncSetAttribute(k_rank_update<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+  const int64_t nkb = cdiv(g.n, KB);
+  const int64_t pairs = k_block_pairs(g, full);
+  const int c0t = (int)(c0 / TS);
+  const int ctiles = (int)cdiv(ncol, TS);
+  dim3 grid((unsigned)pairs, (unsigned)splits);
+  k_rank_update<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(X, ldx, sxp, np, c0t, ctiles, splits, full, nkb,
+                                                                   pairs, Kpart, err);
+}
+
+// ---- dm form: Kpart = sum_p T_p B_p ------------------------------------------
+struct KdmSched {
+  const double* T;
+  int64_t ldt, stp;
+  const double* B;
+  int64_t ldB;
+  int64_t pg0;  // global aux index of local p = 0
+  int64_t p0;   // first local p of this split
+  int nt;
+  int64_t mrow0;
+  int nb0;  // first nu tile of this CTA
+  __device__ SlotSrc a(int kt, int mt) const {
+    const int64_t p = p0 + kt / nt;
+    const int kb = kt % nt;
+    return {T + p * stp + mrow0 + mt * TS + (int64_t)kb * TS * ldt, ldt, 0};
+  }
+  __device__ SlotSrc b(int kt, int ntl) const {
+    const int64_t p = p0 + kt / nt;
+    const int kb = kt % nt;
+    const int nb = nb0 + ntl;
+    if (nb >= nt) return {nullptr, TS, 0};
+    const double* Bp = B + (pg0 + p) * ldB;
+    if (kb <= nb) return {Bp + tile_pair_index(kb, nb) * TILE_ELEMS, TS, 0};
+    return {Bp + tile_pair_index(nb, kb) * TILE_ELEMS, TS, 1};
+  }
+};
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS) k_dm_update(const double* __restrict__ T, int64_t ldt, int64_t stp,
+                                                            const double* __restrict__ B, int64_t ldB, int64_t pg0,
+                                                            int64_t np, int nt, int splits, int full, int64_t nkb,
+                                                            int64_t pairs, double* __restrict__ Kpart, int* err) {
+  extern __shared__ __align__(128) double smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_DOUBLES);
+  const int64_t q = blockIdx.x;
+  const int sp = blockIdx.y;
+  int64_t Ib, Jb;
+  block_pair(q, full, nkb, Ib, Jb);
+  const int64_t pa = np * sp / splits, pb = np * (sp + 1) / splits;
+  KdmSched sc{T, ldt, stp, B, ldB, pg0, pa, nt, Ib * Cfg::BM, (int)(Jb * Cfg::NT)};
+  double acc[Cfg::FM][Cfg::FN][2];
+  const int ktiles = (int)((pb - pa) * nt);
+  if (!dmma_mainloop<Cfg>(sc, ktiles, smem, bars, acc, err)) return;
+  double* out = Kpart + ((int64_t)sp * pairs + q) * (Cfg::BM * Cfg::BN);
+  dmma_for_each<Cfg>(acc, [&](int m, int n, double v0, double v1) {
+    out[m + Cfg::BM * n] = v0;
+    out[m + Cfg::BM * (n + 1)] = v1;
+  });
+}
+
+void launch_k_dm_update(const Geom& g, const double* T, int64_t ldt, int64_t stp, const double* B, int64_t p0,
+                        int64_t np, int splits, int full, double* Kpart, int* err, cudaStream_t st) {
+  using Cfg = RkCfg;
+  cudaFuncSetAttribute(k_dm_update<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+  const int64_t nkb = cdiv(g.n, KB);
+  const int64_t pairs = k_block_pairs(g, full);
+  dim3 grid((unsigned)pairs, (unsigned)splits);
+  k_dm_update<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(T, ldt, stp, B, g.ldB, p0, np, (int)g.nt, splits,
+                                                                 full, nkb, pairs, Kpart, err);
+}
+
+__global__ void __launch_bounds__(256) k_k_finalize(int64_t n, int64_t npair, const double* __restrict__ Kpart,
+                                                    int splits, int full, int64_t nkb, int64_t pairs, double scale,
+                                                    int accumulate, int out_kind, double* __restrict__ out) {
+  const int64_t total = out_kind == 0 ? npair : n * n;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i, j;
+    if (out_kind == 0) {
+      j = tri_root(e);
+      i = e - j * (j + 1) / 2;
+    } else {
+      i = e % n;
+      j = e / n;
+    }
+    const int64_t Ib = i / KB, Jb = j / KB;
+    const int64_t q = full ? Ib + nkb * Jb : Jb * (Jb + 1) / 2 + Ib;
+    const int64_t off = (i % KB) + (int64_t)KB * (j % KB);
+    double v = 0.0;
+    for (int sp = 0; sp < splits; ++sp) v += Kpart[((int64_t)sp * pairs + q) * (KB * KB) + off];
+    v *= scale;
+    out[e] = accumulate ? out[e] + v : v;
+  }
+}
+
+void launch_k_finalize(const Geom& g, const double* Kpart, int splits, int full, double scale, int accumulate,
+                       int out_kind, double* out, cudaStream_t st) {
+  const int64_t nkb = cdiv(g.n, KB);
+  const int64_t pairs = k_block_pairs(g, full);
+  const int64_t total = out_kind == 0 ? g.npair : g.n * g.n;
+  const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), 148 * 16));
+  k_k_finalize<<<blocks, 256, 0, st>>>(g.n, g.npair, Kpart, splits, full, nkb, pairs, scale, accumulate, out_kind,
+                                       out);
+}
+
+}  // namespace rijk

@@ -1,0 +1,249 @@
+"""Host-side mirror of REST's RI J/K interface over the C ABI.
+
+``RIJK`` owns one device context holding the fitted tensor (REST's
+``SCF::rimatr`` / ``SCF::ri3fn``).  Its methods carry the names, argument
+meaning and return shapes of REST's free functions in ``src/scf_io/mod.rs``:
+they take spin-resolved lists of column-major (Fortran-order) matrices and
+return a list of two packed upper triangles (``MatrixUpper``), the second a
+one-element placeholder when ``spin_channel == 1`` -- exactly as REST does.
+Errors raise ``RijkError`` (REST panics).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._abi import RijkError, lib
+
+
+def _f64(a, shape=None) -> np.ndarray:
+    a = np.asarray(a, dtype=np.float64)
+    if shape is not None and a.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def _stack_spin(mats, spin_channel: int, shape) -> np.ndarray:
+    """Spin-resolved list -> one contiguous buffer of column-major matrices."""
+    out = np.empty((spin_channel,) + tuple(reversed(shape)), dtype=np.float64)
+    for s in range(spin_channel):
+        m = _f64(mats[s], tuple(shape))
+        out[s] = m.T  # row-major view of the transpose == column-major data
+    return out
+
+
+def _rest_list(parts):
+    """REST returns Vec of length 2 with a 1-element placeholder in slot 1."""
+    out = list(parts)
+    while len(out) < 2:
+        out.append(np.zeros(1))
+    return out
+
+
+class RIJK:
+    """A device context holding one fitted three-centre tensor."""
+
+    def __init__(self, device: int = 0):
+        L = lib()
+        h = C.c_void_p()
+        st = L.rijk_ctx_create(int(device), C.byref(h))
+        if st != 0:
+            raise RijkError(st, f"cannot open an sm_100 context on device {device}")
+        self._h = h
+        self.num_basis = 0
+        self.num_auxbas = 0
+
+    # -- plumbing ----------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().rijk_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, st: int, failed_pivot: int = 0):
+        if st != 0:
+            msg = lib().rijk_ctx_last_error(self._h)
+            raise RijkError(st, msg.decode() if msg else "", failed_pivot)
+
+    @property
+    def npair(self) -> int:
+        return self.num_basis * (self.num_basis + 1) // 2
+
+    @property
+    def stream(self) -> int:
+        return lib().rijk_ctx_stream(self._h) or 0
+
+    def tensor_bytes(self) -> int:
+        b = C.c_int64()
+        self._check(lib().rijk_ctx_info(self._h, None, None, C.byref(b)))
+        return b.value
+
+    def synchronize(self, stream: int = 0):
+        self._check(lib().rijk_ctx_synchronize(self._h, C.c_void_p(stream or None)))
+
+    # -- fitted tensor -----------------------------------------------------
+    def set_rimatr(self, rimatr: np.ndarray, num_basis: int):
+        """rimatr: MatrixFull[npair, N] (Fortran order)."""
+        npair = num_basis * (num_basis + 1) // 2
+        r = np.asfortranarray(_f64(rimatr))
+        if r.shape[0] != npair:
+            raise ValueError("rimatr must have num_basis*(num_basis+1)/2 rows")
+        self._check(lib().rijk_set_rimatr(self._h, _ptr(r), num_basis, r.shape[1]))
+        self.num_basis, self.num_auxbas = num_basis, r.shape[1]
+
+    def set_ri3fn(self, ri3fn: np.ndarray):
+        """ri3fn: RIFull[n, n, N] (Fortran order)."""
+        r = np.asfortranarray(_f64(ri3fn))
+        n, n2, naux = r.shape
+        if n != n2:
+            raise ValueError("ri3fn must be n x n x N")
+        self._check(lib().rijk_set_ri3fn(self._h, _ptr(r), n, naux))
+        self.num_basis, self.num_auxbas = n, naux
+
+    def tensor_alloc(self, num_basis: int, num_auxbas: int):
+        self._check(lib().rijk_tensor_alloc(self._h, num_basis, num_auxbas))
+        self.num_basis, self.num_auxbas = num_basis, num_auxbas
+
+    def tensor_load_rows_dev(self, d_rows: int, p0: int, np_rows: int, layout: int = 0, stream: int = 0):
+        self._check(lib().rijk_tensor_load_rows_dev(self._h, C.c_void_p(d_rows), p0, np_rows, layout,
+                                                    C.c_void_p(stream or None)))
+
+    def get_rimatr(self) -> np.ndarray:
+        out = np.empty((self.npair, self.num_auxbas), order="F")
+        self._check(lib().rijk_get_rimatr(self._h, _ptr(out)))
+        return out
+
+    def build_rimatr_cholesky(self, aux_v: np.ndarray, int3c: np.ndarray, num_basis: int):
+        """Metric V = L L^T and B = int3c L^-T on the device."""
+        v = np.asfortranarray(_f64(aux_v))
+        m = np.asfortranarray(_f64(int3c))
+        piv = C.c_int64(0)
+        st = lib().rijk_build_rimatr_cholesky(self._h, _ptr(v), _ptr(m), num_basis, m.shape[1], C.byref(piv))
+        self._check(st, piv.value)
+        self.num_basis, self.num_auxbas = num_basis, m.shape[1]
+
+    def fit_rimatr(self, metric_factor: np.ndarray, int3c: np.ndarray, num_basis: int):
+        """B = int3c M for a caller-supplied factor (e.g. REST's V^-1/2)."""
+        f = np.asfortranarray(_f64(metric_factor))
+        m = np.asfortranarray(_f64(int3c))
+        self._check(lib().rijk_fit_rimatr(self._h, _ptr(f), _ptr(m), num_basis, m.shape[1]))
+        self.num_basis, self.num_auxbas = num_basis, m.shape[1]
+
+    # -- J -------------------------------------------------------------------
+    def _vj(self, fn, dm, spin_channel, scaling_factor, full=False):
+        n = self.num_basis
+        d = _stack_spin(dm, spin_channel, (n, n))
+        per = n * n if full else self.npair
+        out = np.empty(spin_channel * per)
+        self._check(fn(self._h, _ptr(d), spin_channel, float(scaling_factor), _ptr(out)))
+        if full:
+            return _rest_list([out[s * per:(s + 1) * per].reshape(n, n, order="F") for s in range(spin_channel)])
+        return _rest_list([out[s * per:(s + 1) * per].copy() for s in range(spin_channel)])
+
+    def vj_upper_with_ri_v(self, dm, spin_channel: int, scaling_factor: float):
+        """REST ``vj_upper_with_ri_v_sync`` (scf_io/mod.rs:2428)."""
+        return self._vj(lib().rijk_vj_upper_with_ri_v, dm, spin_channel, scaling_factor)
+
+    def vj_upper_with_rimatr_v(self, dm, spin_channel: int, scaling_factor: float):
+        """REST ``vj_upper_with_rimatr_v_sync`` (scf_io/mod.rs:2490)."""
+        return self._vj(lib().rijk_vj_upper_with_rimatr_v, dm, spin_channel, scaling_factor)
+
+    def vj_full_with_ri_v(self, dm, spin_channel: int, scaling_factor: float):
+        """REST ``vj_full_with_ri_v`` (scf_io/mod.rs:2564)."""
+        return self._vj(lib().rijk_vj_full_with_ri_v, dm, spin_channel, scaling_factor, full=True)
+
+    # -- K -------------------------------------------------------------------
+    def vk_upper_with_ri_v(self, eigv, homo, occupation, spin_channel: int, scaling_factor: float):
+        """REST ``vk_upper_with_ri_v_sync`` (scf_io/mod.rs:2758): occupied-orbital form."""
+        n = self.num_basis
+        num_state = np.asarray(eigv[0]).shape[1]
+        c = _stack_spin(eigv, spin_channel, (n, num_state))
+        occ = np.ascontiguousarray(np.stack([_f64(occupation[s])[:num_state] for s in range(spin_channel)]))
+        hm = (C.c_int64 * 2)(*[int(homo[s]) if s < spin_channel else 0 for s in range(2)])
+        out = np.empty(spin_channel * self.npair)
+        st = lib().rijk_vk_upper_with_ri_v(
+            self._h, _ptr(c), num_state, hm, _ptr(occ), spin_channel, float(scaling_factor), _ptr(out)
+        )
+        self._check(st)
+        p = self.npair
+        return _rest_list([out[s * p:(s + 1) * p].copy() for s in range(spin_channel)])
+
+    def _vk_dm(self, fn, dm, spin_channel, scaling_factor, full=False):
+        n = self.num_basis
+        d = _stack_spin(dm, spin_channel, (n, n))
+        per = n * n if full else self.npair
+        out = np.empty(spin_channel * per)
+        self._check(fn(self._h, _ptr(d), spin_channel, float(scaling_factor), _ptr(out)))
+        if full:
+            return _rest_list([out[s * per:(s + 1) * per].reshape(n, n, order="F") for s in range(spin_channel)])
+        return _rest_list([out[s * per:(s + 1) * per].copy() for s in range(spin_channel)])
+
+    def vk_upper_with_ri_v_use_dm_only(self, dm, spin_channel: int, scaling_factor: float):
+        """REST ``vk_upper_with_ri_v_use_dm_only_sync`` (scf_io/mod.rs:2640)."""
+        return self._vk_dm(lib().rijk_vk_upper_with_ri_v_use_dm_only, dm, spin_channel, scaling_factor)
+
+    def vk_upper_with_rimatr_use_dm_only(self, dm, spin_channel: int, scaling_factor: float):
+        """REST ``vk_upper_with_rimatr_use_dm_only_sync`` (scf_io/mod.rs:2703)."""
+        return self._vk_dm(lib().rijk_vk_upper_with_rimatr_use_dm_only, dm, spin_channel, scaling_factor)
+
+    def vk_full_fromdm_with_ri_v(self, dm, spin_channel: int, scaling_factor: float):
+        """REST ``vk_full_fromdm_with_ri_v`` (scf_io/mod.rs:2603)."""
+        return self._vk_dm(lib().rijk_vk_full_fromdm_with_ri_v, dm, spin_channel, scaling_factor, full=True)
+
+    # -- device-resident forms (raw device pointers, e.g. torch .data_ptr()) --
+    def vj_upper_dev(self, d_dm: int, spin_channel: int, scaling_factor: float, dm_mode: int, d_vj: int,
+                     stream: int = 0):
+        self._check(lib().rijk_vj_upper_dev(self._h, C.c_void_p(d_dm), spin_channel, float(scaling_factor),
+                                            int(dm_mode), C.c_void_p(d_vj), C.c_void_p(stream or None)))
+
+    def vk_upper_occ_dev(self, d_eigv: int, num_state: int, homo, d_occ: int, spin_channel: int,
+                         scaling_factor: float, d_vk: int, stream: int = 0):
+        hm = (C.c_int64 * 2)(*[int(homo[s]) if s < spin_channel else 0 for s in range(2)])
+        self._check(lib().rijk_vk_upper_occ_dev(self._h, C.c_void_p(d_eigv), num_state, hm, C.c_void_p(d_occ),
+                                                spin_channel, float(scaling_factor), C.c_void_p(d_vk),
+                                                C.c_void_p(stream or None)))
+
+    def vk_upper_dm_dev(self, d_dm: int, spin_channel: int, scaling_factor: float, d_vk: int, stream: int = 0):
+        self._check(lib().rijk_vk_upper_dm_dev(self._h, C.c_void_p(d_dm), spin_channel, float(scaling_factor),
+                                               C.c_void_p(d_vk), C.c_void_p(stream or None)))
+
+    # -- SCF pieces --------------------------------------------------------
+    def density_matrix(self, eigv, homo, occupation, spin_channel: int):
+        """REST ``generate_density_matrix`` (scf_io/mod.rs:441): list of n x n D."""
+        e0 = np.asarray(eigv[0])
+        n, num_state = e0.shape
+        c = _stack_spin(eigv, spin_channel, (n, num_state))
+        occ = np.ascontiguousarray(np.stack([_f64(occupation[s])[:num_state] for s in range(spin_channel)]))
+        hm = (C.c_int64 * 2)(*[int(homo[s]) if s < spin_channel else 0 for s in range(2)])
+        out = np.empty(spin_channel * n * n)
+        self._check(lib().rijk_density_matrix(self._h, _ptr(c), n, num_state, hm, _ptr(occ), spin_channel, _ptr(out)))
+        return [out[s * n * n:(s + 1) * n * n].reshape(n, n, order="F") for s in range(spin_channel)]
+
+
+def energy_contraction(a_upper: np.ndarray, b_upper: np.ndarray) -> float:
+    """REST ``SCF::par_energy_contraction`` (scf_io/mod.rs:1787)."""
+    a = np.ascontiguousarray(_f64(a_upper))
+    b = np.ascontiguousarray(_f64(b_upper))
+    if a.shape != b.shape:
+        raise ValueError("shape mismatch")
+    return float(lib().rijk_energy_contraction(_ptr(a), _ptr(b), a.size))

@@ -1,0 +1,272 @@
+"""GPU parity of the RI J/K build against the FP64 oracle, through the C ABI.
+
+Tolerance (the FP64 plain form's contract): max |GPU - oracle| <= 1e-10 per
+element of every J/K matrix.
+"""
+import numpy as np
+import pytest
+
+from oracle import rijk_oracle as O
+from rest_b200.synth import host_case
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+SHAPES = [(1, 3, 1), (5, 17, 2), (7, 33, 3), (24, 113, 5), (33, 70, 4), (37, 150, 6), (100, 400, 16), (200, 800, 33)]
+
+
+def _maxdiff(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))))
+
+
+def _second_spin(case, seed):
+    rng = np.random.default_rng(seed)
+    c2 = np.asfortranarray(np.linalg.qr(rng.standard_normal((case.n, max(1, case.nocc - 1))))[0])
+    return c2, np.asfortranarray(c2 @ c2.T)
+
+
+@pytest.mark.parametrize("n,naux,nocc", SHAPES)
+def test_vj_upper_rimatr_and_ri3fn(ctx, n, naux, nocc):
+    case = host_case(n, naux, nocc, seed=100 + n)
+    _, dm2 = _second_spin(case, n)
+    ri3 = O.ri3fn_from_rimatr(case.rimatr, n)
+    for spin in (1, 2):
+        dm = [case.dm, dm2][:spin]
+        ctx.set_rimatr(case.rimatr, n)
+        got = ctx.vj_upper_with_rimatr_v(dm, spin, 1.0)
+        ref = O.vj_upper_with_rimatr_v(case.rimatr, dm, spin, 1.0)
+        for s in range(spin):
+            assert _maxdiff(got[s], ref[s]) <= TOL
+        ctx.set_ri3fn(ri3)
+        got = ctx.vj_upper_with_ri_v(dm, spin, 0.5)
+        ref = O.vj_upper_with_ri_v(ri3, dm, spin, 0.5)
+        for s in range(spin):
+            assert _maxdiff(got[s], ref[s]) <= TOL
+        if spin == 1:
+            assert got[1].shape == (1,)  # REST's placeholder slot
+
+
+@pytest.mark.parametrize("n,naux,nocc", [(7, 33, 3), (37, 150, 6)])
+def test_vj_modes_differ_exactly_as_rest_for_nonsymmetric_dm(ctx, n, naux, nocc):
+    case = host_case(n, naux, nocc, seed=5)
+    rng = np.random.default_rng(9)
+    d = np.asfortranarray(rng.standard_normal((n, n)))
+    ctx.set_rimatr(case.rimatr, n)
+    ri3 = O.ri3fn_from_rimatr(case.rimatr, n)
+    a = ctx.vj_upper_with_ri_v([d], 1, 1.0)[0]
+    b = ctx.vj_upper_with_rimatr_v([d], 1, 1.0)[0]
+    assert _maxdiff(a, O.vj_upper_with_ri_v(ri3, [d], 1, 1.0)[0]) <= TOL
+    assert _maxdiff(b, O.vj_upper_with_rimatr_v(case.rimatr, [d], 1, 1.0)[0]) <= TOL
+    assert _maxdiff(a, b) > 1e-6  # the two REST formulas disagree for non-symmetric D
+    jf = ctx.vj_full_with_ri_v([d], 1, 2.0)[0]
+    assert _maxdiff(jf, O.vj_full_with_ri_v(ri3, [d], 1, 2.0)[0]) <= TOL
+
+
+@pytest.mark.parametrize("n,naux,nocc", SHAPES)
+def test_vk_occupied_form(ctx, n, naux, nocc):
+    case = host_case(n, naux, nocc, seed=200 + n)
+    c2, _ = _second_spin(case, n + 1)
+    ctx.set_rimatr(case.rimatr, n)
+    ri3 = O.ri3fn_from_rimatr(case.rimatr, n)
+    num_state = nocc + 2
+    e1 = np.zeros((n, num_state), order="F")
+    e1[:, :nocc] = case.c_occ
+    e2 = np.zeros((n, num_state), order="F")
+    e2[:, : c2.shape[1]] = c2
+    occ1 = np.zeros(num_state)
+    occ1[:nocc] = 2.0
+    occ2 = np.zeros(num_state)
+    occ2[: c2.shape[1]] = 1.0
+    occ2[0] = 0.5
+    for spin, scale in ((1, -0.5), (2, -1.0)):
+        eig = [e1, e2][:spin]
+        homo = [nocc - 1, c2.shape[1] - 1][:spin]
+        occ = [occ1, occ2][:spin]
+        got = ctx.vk_upper_with_ri_v(eig, homo, occ, spin, scale)
+        ref = O.vk_upper_with_ri_v(ri3, eig, homo, occ, spin, scale)
+        for s in range(spin):
+            assert _maxdiff(got[s], ref[s]) <= TOL
+
+
+@pytest.mark.parametrize("n,naux,nocc", SHAPES[:-1])
+def test_vk_density_forms(ctx, n, naux, nocc):
+    case = host_case(n, naux, nocc, seed=300 + n)
+    _, dm2 = _second_spin(case, n + 2)
+    ri3 = O.ri3fn_from_rimatr(case.rimatr, n)
+    for spin in (1, 2):
+        dm = [case.dm, dm2][:spin]
+        ctx.set_ri3fn(ri3)
+        got = ctx.vk_upper_with_ri_v_use_dm_only(dm, spin, -0.5)
+        ref = O.vk_upper_with_ri_v_use_dm_only(ri3, dm, spin, -0.5)
+        for s in range(spin):
+            assert _maxdiff(got[s], ref[s]) <= TOL
+        ctx.set_rimatr(case.rimatr, n)
+        got = ctx.vk_upper_with_rimatr_use_dm_only(dm, spin, -1.0)
+        ref = O.vk_upper_with_rimatr_use_dm_only(case.rimatr, dm, spin, -1.0)
+        for s in range(spin):
+            assert _maxdiff(got[s], ref[s]) <= TOL
+
+
+@pytest.mark.parametrize("n,naux,nocc", [(5, 17, 2), (37, 150, 6), (130, 300, 8)])
+def test_vk_full_from_nonsymmetric_dm(ctx, n, naux, nocc):
+    case = host_case(n, naux, nocc, seed=400 + n)
+    rng = np.random.default_rng(n)
+    d = np.asfortranarray(rng.standard_normal((n, n)) / n)
+    ctx.set_rimatr(case.rimatr, n)
+    ri3 = O.ri3fn_from_rimatr(case.rimatr, n)
+    got = ctx.vk_full_fromdm_with_ri_v([d], 1, 1.0)[0]
+    ref = O.vk_full_fromdm_with_ri_v(ri3, [d], 1, 1.0)[0]
+    assert _maxdiff(got, ref) <= TOL
+    assert _maxdiff(got, got.T) > 1e-8  # non-symmetric D gives a non-symmetric K
+
+
+@pytest.mark.parametrize("n,naux", [(1, 3), (33, 70), (200, 800)])
+def test_tensor_round_trip_is_bit_exact(ctx, n, naux):
+    case = host_case(n, naux, 1, seed=n)
+    ctx.set_rimatr(case.rimatr, n)
+    assert np.array_equal(ctx.get_rimatr(), case.rimatr)
+    ctx.set_ri3fn(O.ri3fn_from_rimatr(case.rimatr, n))
+    assert np.array_equal(ctx.get_rimatr(), case.rimatr)
+
+
+def _spd(naux, seed, eps=1e-2):
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((naux, naux + 5))
+    return np.asfortranarray(g @ g.T / naux + eps * np.eye(naux))
+
+
+@pytest.mark.parametrize("n,naux", [(5, 17), (24, 113), (40, 330)])
+def test_metric_cholesky_fit(ctx, n, naux):
+    case = host_case(n, naux, 2, seed=600 + n)
+    v = _spd(naux, naux)
+    int3c = case.rimatr
+    ctx.build_rimatr_cholesky(v, int3c, n)
+    got = ctx.get_rimatr()
+    ref = O.fit_rimatr_cholesky(int3c, v)
+    scale = max(1.0, float(np.max(np.abs(ref))))
+    assert _maxdiff(got, ref) <= 1e-11 * scale * naux
+    # J/K from the device fit equal those from REST's V^-1/2 whitening
+    b_half = O.fit_rimatr(int3c, O.metric_inv_sqrt(v))
+    j_ref = O.vj_upper_with_rimatr_v(b_half, [case.dm], 1, 1.0)[0]
+    j_got = ctx.vj_upper_with_rimatr_v([case.dm], 1, 1.0)[0]
+    assert _maxdiff(j_got, j_ref) <= 1e-9 * max(1.0, float(np.max(np.abs(j_ref))))
+
+
+def test_metric_factor_fit_matches_rest_whitening(ctx):
+    n, naux = 24, 113
+    case = host_case(n, naux, 5, seed=11)
+    v = _spd(naux, 3)
+    m = O.metric_inv_sqrt(v)
+    ctx.fit_rimatr(m, case.rimatr, n)
+    ref = O.fit_rimatr(case.rimatr, m)
+    assert _maxdiff(ctx.get_rimatr(), ref) <= 1e-12 * naux * max(1.0, float(np.max(np.abs(ref))))
+
+
+def test_non_spd_metric_reports_the_failing_pivot(ctx):
+    from rest_b200 import RijkError
+
+    n, naux = 5, 40
+    case = host_case(n, naux, 2, seed=1)
+    v = _spd(naux, 4)
+    v[37, 37] = -5.0
+    with pytest.raises(RijkError) as ei:
+        ctx.build_rimatr_cholesky(v, case.rimatr, n)
+    assert ei.value.status == 3
+    assert ei.value.failed_pivot == 38
+    # the context is still usable afterwards
+    ctx.set_rimatr(case.rimatr, n)
+    ctx.vj_upper_with_rimatr_v([case.dm], 1, 1.0)
+
+
+def test_bad_arguments_are_rejected(ctx):
+    from rest_b200 import RijkError
+
+    case = host_case(7, 20, 2, seed=1)
+    ctx.set_rimatr(case.rimatr, 7)
+    with pytest.raises(RijkError) as ei:
+        ctx.vj_upper_with_rimatr_v([case.dm, case.dm, case.dm], 3, 1.0)
+    assert ei.value.status == 1
+    e = np.zeros((7, 3), order="F")
+    with pytest.raises(RijkError):
+        ctx.vk_upper_with_ri_v([e], [5], [np.ones(3)], 1, 1.0)  # homo beyond num_state
+    with pytest.raises(RijkError):
+        ctx.vk_upper_with_ri_v([e], [1], [np.array([1.0, -1.0, 0.0])], 1, 1.0)  # negative occupation
+
+
+def test_density_matrix(ctx):
+    rng = np.random.default_rng(8)
+    n = 45
+    c = np.asfortranarray(rng.standard_normal((n, n)))
+    occ, homo, _ = O.occupation_integer(n, 7.0, 2.0)
+    got = ctx.density_matrix([c], [homo], [occ], 1)[0]
+    assert _maxdiff(got, O.density_matrix(c, occ, homo)) <= TOL
+
+
+def test_full_size_n600_against_oracle(ctx):
+    """The middle sweep size end to end: host-drawn tensor, J and K vs the oracle."""
+    n = 600
+    case = host_case(n, seed=7)
+    ctx.set_rimatr(case.rimatr, n)
+    j = ctx.vj_upper_with_rimatr_v([case.dm], 1, 1.0)[0]
+    assert _maxdiff(j, O.vj_upper_with_rimatr_v(case.rimatr, [case.dm], 1, 1.0)[0]) <= TOL
+    occ = np.ones(case.nocc)
+    k = ctx.vk_upper_with_ri_v([case.c_occ], [case.nocc - 1], [occ], 1, -1.0)[0]
+    # oracle K in the occupied form straight from rimatr, P by P
+    ii, jj = O.upper_pairs(n)
+    kref = np.zeros((n, n))
+    for p in range(case.naux):
+        bp = np.zeros((n, n))
+        bp[ii, jj] = case.rimatr[:, p]
+        bp[jj, ii] = case.rimatr[:, p]
+        x = bp @ case.c_occ
+        kref += x @ x.T
+    assert _maxdiff(k, -kref[ii, jj]) <= TOL
+
+
+def test_full_size_n1200_properties(ctx):
+    """Largest sweep size (28 GB tensor, device-drawn): size-independent identities."""
+    import torch
+
+    from rest_b200.synth import device_case
+
+    n = 1200
+    with torch.cuda.stream(torch.cuda.ExternalStream(ctx.stream)):
+        _n1200_body(ctx, n)
+
+
+def _n1200_body(ctx, n):
+    import torch
+
+    from rest_b200.synth import device_case
+
+    c_cm, dm = device_case(ctx, n, seed=99)
+    nocc = c_cm.shape[0]
+    npair = n * (n + 1) // 2
+    dev = c_cm.device
+    st = torch.cuda.current_stream().cuda_stream
+    occ = torch.ones(nocc, dtype=torch.float64, device=dev)
+    k_occ = torch.empty(npair, dtype=torch.float64, device=dev)
+    k_dm = torch.empty(npair, dtype=torch.float64, device=dev)
+    ctx.vk_upper_occ_dev(c_cm.data_ptr(), nocc, [nocc - 1], occ.data_ptr(), 1, -1.0, k_occ.data_ptr(), st)
+    ctx.vk_upper_dm_dev(dm.data_ptr(), 1, -1.0, k_dm.data_ptr(), st)
+    # J is linear in D: J(2D) - 2 J(D) == 0, and <D, J(D)> = sum_P w_P^2 >= 0
+    j1 = torch.empty(npair, dtype=torch.float64, device=dev)
+    j2 = torch.empty(npair, dtype=torch.float64, device=dev)
+    dm2 = (2.0 * dm).contiguous()
+    ctx.vj_upper_dev(dm.data_ptr(), 1, 1.0, 1, j1.data_ptr(), st)
+    ctx.vj_upper_dev(dm2.data_ptr(), 1, 1.0, 1, j2.data_ptr(), st)
+    ctx.synchronize(st)
+    torch.cuda.synchronize()
+    # occupied-orbital K and density K are two independent kernel paths
+    assert float((k_occ - k_dm).abs().max()) <= TOL
+    assert float((j2 - 2.0 * j1).abs().max()) <= TOL
+    # REST's packed order is (i <= j) sorted by j then i == tril_indices (r=j, c=i)
+    il = torch.tril_indices(n, n, device=dev)
+    d_up = dm[il[1], il[0]]
+    diag = torch.arange(n, device=dev)
+    dg = diag * (diag + 1) // 2 + diag
+    e = 2.0 * torch.dot(d_up, j1) - torch.dot(d_up[dg], j1[dg])
+    assert float(e) > 0
+    ek = 2.0 * torch.dot(d_up, k_occ) - torch.dot(d_up[dg], k_occ[dg])
+    assert float(ek) < 0
