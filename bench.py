@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark of the RI-JK Fock build (REST src/scf_io vj/vk) on B200.
+
+One step = one FP64 Fock build on the synthetic kernel-sweep workload
+(n = 1200 basis functions, N = 4800 auxiliary functions, nocc = 200):
+J (vj_upper_with_rimatr_v) + K in the occupied-orbital form
+(vk_upper_with_ri_v), with the fitted tensor resident in HBM (28 GB packed,
+29 GB tile-packed, larger than the 126 MB L2 so no flush is needed).
+
+  value  = (J + K algorithmic FLOPs) / device time of the step, TFLOP/s
+           (CUDA events on the launching stream, max over ranks)
+  e2e    = the same build through the host C ABI (host density / orbitals
+           in, host J / K out, pinned buffers, copies inside the timed region)
+
+--impl reference times REST's CPU algorithm restated in C (oracle/cpu_rijk.c,
+OpenMP over the aux index, single-threaded OpenBLAS per P as REST does) on a
+bounded sample of the same workload with all host threads.
+
+With --gpus N (launched under torchrun) every rank runs an independent
+replica on its own molecule: the kernel sweep has no exchange step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def workload(n: int) -> dict:
+    naux, nocc = 4 * n, n // 6
+    npair = n * (n + 1) // 2
+    return {
+        "n": n,
+        "naux": naux,
+        "nocc": nocc,
+        "npair": npair,
+        "j_flops": 4.0 * naux * npair,
+        "k_flops": 4.0 * naux * n * n * nocc,
+        "half_flops": 2.0 * naux * n * n * nocc,  # X_P = B_P C, per build
+        "rank_flops": 2.0 * naux * n * n * nocc,  # K += X_P X_P^T, per build
+        "j_pass_bytes": 8.0 * naux * npair,  # one pass over packed B
+    }
+
+
+def config_of(w: dict, ngpu: int) -> dict:
+    return {
+        "workload": f"synthetic RI-JK sweep, FP64 plain form: n={w['n']}, N={w['naux']}, nocc={w['nocc']}; "
+        "one Fock build (J + occupied-orbital K) per step",
+        "num_basis": w["n"],
+        "num_auxbas": w["naux"],
+        "nocc": w["nocc"],
+        "tensor": "packed upper B[P, mu<=nu], FP64, resident in HBM",
+        "l2": "inputs larger than L2 (28 GB tensor vs 126 MB L2); no flush needed",
+        "parallelism": f"replicas x{ngpu}" if ngpu > 1 else "single GPU",
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self, busy_mhz_floor: float = 600.0) -> dict:
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    rows.append((float(p[1]), float(p[2]), p[5:9]))
+                except ValueError:
+                    continue
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        busy = [r for r in rows if r[0] >= busy_mhz_floor] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in busy for i in range(4) if r[2][i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(r[0] for r in busy), "sm_max_mhz": max(r[1] for r in busy),
+                "reasons": reasons, "samples": len(busy)}
+
+
+# ---------------------------------------------------------------------------
+# CPU leg (REST's algorithm restated in C)
+# ---------------------------------------------------------------------------
+def cpu_sample_run(w: dict, target_s: float, seed: int = 2024):
+    """Time one bounded-sample Fock build on the host; returns (TFLOP/s, threads, sample text)."""
+    import numpy as np
+
+    from oracle import rijk_oracle as O
+    from oracle.cpu_baseline import CpuRijk
+    from rest_b200.synth import host_case
+
+    cpu = CpuRijk()
+    n, nocc = w["n"], w["nocc"]
+    probe = max(1, min(w["naux"], cpu.nthreads))
+    case = host_case(n, w["naux"], nocc, seed=seed, rows=(0, probe))
+    ri3 = O.ri3fn_from_rimatr(case.rimatr, n)
+    occ = np.ones(nocc)
+    t0 = time.perf_counter()
+    cpu.vk_upper_with_ri_v(ri3, case.c_occ, nocc - 1, occ, -1.0)
+    per_row = (time.perf_counter() - t0) / probe
+    rows = int(max(probe, min(w["naux"], target_s / max(per_row, 1e-6))))
+    rows = max(cpu.nthreads, (rows // cpu.nthreads) * cpu.nthreads) if rows >= cpu.nthreads else rows
+    case = host_case(n, w["naux"], nocc, seed=seed, rows=(0, rows))
+    ri3 = O.ri3fn_from_rimatr(case.rimatr, n)
+
+    def step():
+        t = time.perf_counter()
+        cpu.vj_upper_with_rimatr(case.rimatr, n, case.dm, 1.0)
+        cpu.vk_upper_with_ri_v(ri3, case.c_occ, nocc - 1, occ, -1.0)
+        return time.perf_counter() - t
+
+    flops = 4.0 * rows * w["npair"] + 4.0 * rows * n * n * nocc
+    sample = (f"{rows} of {w['naux']} aux rows of the n={n} workload (J a2 + K a3 on those rows), "
+              f"REST algorithm restated in C with OpenMP + OpenBLAS; REST binary unavailable on this box")
+    return step, flops, cpu.nthreads, sample
+
+
+def run_reference(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    step, flops, threads, sample = cpu_sample_run(w, target_s=4.0)
+    for _ in range(args.warmup):
+        step()
+    times = [step() for _ in range(args.steps)]
+    t = sum(times) / len(times)
+    v = flops / t / 1e12
+    line = {
+        "impl": "reference",
+        "metric": "RI-JK TFLOP/s",
+        "value": v,
+        "unit": "TFLOP/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded NumPy draw of the kernel-sweep workload)",
+        "config": config_of(w, 1),
+        "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def measure_dgemm_peak(torch) -> float:
+    """FP64 dense peak of this GPU, measured now: cuBLAS DGEMM 8192^3 (best of 5)."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    a @ b
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * 8192 ** 3 / best / 1e12
+
+
+def run_ours(args, w):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from rest_b200 import RIJK, lib
+    from rest_b200.synth import device_case
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+
+    fp64_peak = measure_dgemm_peak(torch)
+    ctx = RIJK(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    torch.cuda.set_stream(stream)
+    c_cm, dm = device_case(ctx, w["n"], w["naux"], w["nocc"], seed=1000 + rank)
+    n, nocc, npair = w["n"], w["nocc"], w["npair"]
+    occ = torch.ones(nocc, dtype=torch.float64, device="cuda")
+    vj = torch.empty(npair, dtype=torch.float64, device="cuda")
+    vk = torch.empty(npair, dtype=torch.float64, device="cuda")
+    st = ctx.stream
+
+    def step():
+        ctx.vj_upper_dev(dm.data_ptr(), 1, 1.0, 1, vj.data_ptr(), st)
+        ctx.vk_upper_occ_dev(c_cm.data_ptr(), nocc, [nocc - 1], occ.data_ptr(), 1, -1.0, vk.data_ptr(), st)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    ctx.synchronize(st)
+    ctx.profile(True)
+    ctx.profile_read()
+    barrier()
+    launches0 = RIJK.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = (RIJK.kernel_launches() - launches0) // args.steps
+    ctx.synchronize(st)
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    dt = e0.elapsed_time(e1) / 1e3
+    if pg:
+        t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        dt = float(t)
+    t_step = dt / args.steps
+    flops = w["j_flops"] + w["k_flops"]
+    value = world * flops / t_step / 1e12
+
+    # roofline of the dominant kernel class (live events over the timed region)
+    cls_time = {k: v[0] / 1e3 / args.steps for k, v in prof.items()}
+    dom = max(cls_time, key=cls_time.get)
+    algo = {"k_half": (w["half_flops"], "tensor"), "k_rank": (w["rank_flops"], "tensor"),
+            "j_pass1": (w["j_pass_bytes"], "hbm"), "j_pass2": (w["j_pass_bytes"], "hbm")}
+    peaks = json.load(open(MEASURED_PEAKS)) if os.path.exists(MEASURED_PEAKS) else {}
+    work, bound = algo.get(dom, (w["half_flops"], "tensor"))
+    dom_launches = max(1, prof[dom][1] // args.steps)
+    if bound == "tensor":
+        achieved = work / cls_time[dom] / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak,
+                "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 via torch.matmul (FP64 has no "
+                               "entry in MEASURED_PEAKS.json; tcgen05 has no FP64 kind, DMMA is the FP64 tensor path)"}
+    else:
+        achieved = work / cls_time[dom] / 1e9
+        peak = peaks.get("hbm_gbs", 6650.0)
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6.65 TB/s"}
+    roof["kernel"] = dom
+    roof["launches_per_step"] = dom_launches
+    roof["traffic"] = TRAFFIC_PER_BUILD.get(dom)
+    # J kernels' own HBM roofline, reported beside the dominant one
+    j_rates = {}
+    for k in ("j_pass1", "j_pass2"):
+        if cls_time.get(k):
+            j_rates[k] = w["j_pass_bytes"] / cls_time[k] / 1e9
+
+    # e2e through the host C ABI, pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        L = lib()
+        h_dm = torch.empty(n * n, dtype=torch.float64).pin_memory()
+        h_dm.copy_(dm.reshape(-1).cpu())
+        h_c = torch.empty(n * nocc, dtype=torch.float64).pin_memory()
+        h_c.copy_(c_cm.reshape(-1).cpu())
+        h_occ = torch.ones(nocc, dtype=torch.float64).pin_memory()
+        h_vj = torch.empty(npair, dtype=torch.float64).pin_memory()
+        h_vk = torch.empty(npair, dtype=torch.float64).pin_memory()
+        homo = (C.c_int64 * 2)(nocc - 1, 0)
+
+        def e2e_step():
+            r1 = L.rijk_vj_upper_with_rimatr_v(ctx.handle, C.c_void_p(h_dm.data_ptr()), 1, 1.0,
+                                               C.c_void_p(h_vj.data_ptr()))
+            r2 = L.rijk_vk_upper_with_ri_v(ctx.handle, C.c_void_p(h_c.data_ptr()), nocc, homo,
+                                           C.c_void_p(h_occ.data_ptr()), 1, -1.0, C.c_void_p(h_vk.data_ptr()))
+            if r1 or r2:
+                raise RuntimeError(f"e2e call failed: {r1} {r2}")
+
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        te = time.perf_counter() - t0
+        if pg:
+            t = torch.tensor([te], dtype=torch.float64, device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            te = float(t)
+        h2d = (n * n + n * nocc + nocc) * 8
+        d2h = 2 * npair * 8
+        e2e = {"value": world * flops / (te / args.steps) / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": te / args.steps * 1e3,
+               "how": "rijk_vj_upper_with_rimatr_v + rijk_vk_upper_with_ri_v on pinned host buffers, wall clock"}
+
+    cpu_base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        stepf, cflops, threads, sample = cpu_sample_run(w, target_s=6.0)
+        stepf()
+        times = [stepf() for _ in range(2)]
+        cpu_base = {"value": cflops / min(times) / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+                    "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": "RI-JK TFLOP/s",
+            "value": value,
+            "unit": "TFLOP/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": max(3, args.warmup),
+            "ms_per_step": t_step * 1e3,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded torch CUDA draw of the kernel-sweep workload)",
+            "config": config_of(w, world),
+            "roofline": roof,
+            "j_hbm_gbs": j_rates,
+            "kernel_ms_per_step": {k: v * 1e3 for k, v in cls_time.items() if v},
+            "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+            "e2e": e2e,
+            "cpu_baseline": cpu_base,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+# DRAM bytes per build of each kernel class from the ncu capture summarised in
+# profiles/ (None until captured).
+TRAFFIC_PER_BUILD: dict = {}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=1200, help="num_basis of the sweep workload")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    w = workload(args.n)
+    if args.impl == "reference":
+        return run_reference(args, w)
+    return run_ours(args, w)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -60,6 +60,26 @@ int rijk_ctx_info(const rijk_ctx* ctx, int64_t* num_basis, int64_t* num_auxbas, 
 void* rijk_ctx_stream(rijk_ctx* ctx);
 /* Device pointer of the tile-packed tensor and its row stride in doubles. */
 int rijk_ctx_tensor(rijk_ctx* ctx, const double** d_tensor, int64_t* row_stride);
+/* Number of CUDA kernels this library has launched in this process (all
+ * contexts); a caller can difference it around a region to count launches. */
+int64_t rijk_kernel_launches(void);
+/* Per-kernel-class CUDA-event timers (REST's TimeRecords, src/utilities/mod.rs:27-84,
+ * for device work).  When enabled, every J/K launch is bracketed by events on
+ * its own stream.  rijk_ctx_profile_read synchronises, writes the accumulated
+ * milliseconds and launch counts of each class (arrays of RIJK_PROF_NCLASS)
+ * and resets them. */
+enum rijk_prof_class {
+  RIJK_PROF_J_PASS1 = 0,    /* w_P = B . D                      */
+  RIJK_PROF_J_PASS2 = 1,    /* J = B^T w                        */
+  RIJK_PROF_J_OTHER = 2,    /* density folding, reduction       */
+  RIJK_PROF_K_HALF = 3,     /* X_P = B_P C (or B_P D)           */
+  RIJK_PROF_K_RANK = 4,     /* K += X_P X_P^T                   */
+  RIJK_PROF_K_DM = 5,       /* K += (B_P D) B_P                 */
+  RIJK_PROF_K_OTHER = 6,    /* operand preparation, reduction   */
+  RIJK_PROF_NCLASS = 7
+};
+int rijk_ctx_profile(rijk_ctx* ctx, int enable);
+int rijk_ctx_profile_read(rijk_ctx* ctx, double* ms, int64_t* launches);
 /* Wait for the work enqueued on `stream` (NULL = the context's stream) and
  * report a device-side timeout recorded since the last check. */
 int rijk_ctx_synchronize(rijk_ctx* ctx, void* stream);

@@ -50,6 +50,9 @@ SIGNATURES = {
     "rijk_ctx_stream": (C.c_void_p, [_ctxp]),
     "rijk_ctx_tensor": (C.c_int, [_ctxp, C.POINTER(C.c_void_p), _i64p]),
     "rijk_ctx_synchronize": (C.c_int, [_ctxp, C.c_void_p]),
+    "rijk_kernel_launches": (C.c_int64, []),
+    "rijk_ctx_profile": (C.c_int, [_ctxp, C.c_int]),
+    "rijk_ctx_profile_read": (C.c_int, [_ctxp, _dp, _i64p]),
     "rijk_set_rimatr": (C.c_int, [_ctxp, C.c_void_p, C.c_int64, C.c_int64]),
     "rijk_set_ri3fn": (C.c_int, [_ctxp, C.c_void_p, C.c_int64, C.c_int64]),
     "rijk_get_rimatr": (C.c_int, [_ctxp, C.c_void_p]),

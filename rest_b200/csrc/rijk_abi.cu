@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <string>
+#include <vector>
 
 #include "../../include/rest_b200.h"
 #include "rijk_common.cuh"
@@ -40,7 +41,53 @@ struct rijk_ctx {
   DevBuf stage, W, w, Jpart, Cw, X, Kpart, din, dout, docc, mV, mLinv, mT, mLinvd, mOut;
   size_t scratch_budget = (size_t)4 << 30;
   std::string last;
+  // per-kernel-class event timers
+  struct ProfRec {
+    int cls;
+    cudaEvent_t a, b;
+  };
+  bool prof = false;
+  std::vector<ProfRec> prof_pending;
+  std::vector<cudaEvent_t> ev_pool;
+  double prof_ms[RIJK_PROF_NCLASS] = {};
+  int64_t prof_n[RIJK_PROF_NCLASS] = {};
 };
+
+namespace {
+
+cudaEvent_t ev_get(rijk_ctx* c) {
+  if (!c->ev_pool.empty()) {
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Brackets the launches issued in its scope with events when profiling is on.
+struct ProfScope {
+  rijk_ctx* c;
+  int cls;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr;
+  ProfScope(rijk_ctx* c_, int cls_, cudaStream_t st_) : c(c_), cls(cls_), st(st_) {
+    if (c->prof) {
+      a = ev_get(c);
+      cudaEventRecord(a, st);
+    }
+  }
+  ~ProfScope() {
+    if (c->prof && a) {
+      cudaEvent_t b = ev_get(c);
+      cudaEventRecord(b, st);
+      c->prof_pending.push_back({cls, a, b});
+    }
+  }
+};
+
+}  // namespace
 
 namespace {
 
@@ -214,10 +261,22 @@ int vj_dev(rijk_ctx* ctx, const double* d_dm, int spin, double scale, int mode, 
   double* W = static_cast<double*>(ctx->W.p);
   double* w = static_cast<double*>(ctx->w.p);
   double* Jp = static_cast<double*>(ctx->Jpart.p);
-  rijk::launch_j_weights(g, d_dm, spin, mode, W, st);
-  rijk::launch_j_pass1(g, ctx->dB, W, spin, w, st);
-  rijk::launch_j_pass2(g, ctx->dB, w, spin, splits, Jp, st);
-  rijk::launch_j_finalize(g, Jp, spin, splits, scale, out_kind, d_out, st);
+  {
+    ProfScope ps(ctx, RIJK_PROF_J_OTHER, st);
+    rijk::launch_j_weights(g, d_dm, spin, mode, W, st);
+  }
+  {
+    ProfScope ps(ctx, RIJK_PROF_J_PASS1, st);
+    rijk::launch_j_pass1(g, ctx->dB, W, spin, w, st);
+  }
+  {
+    ProfScope ps(ctx, RIJK_PROF_J_PASS2, st);
+    rijk::launch_j_pass2(g, ctx->dB, w, spin, splits, Jp, st);
+  }
+  {
+    ProfScope ps(ctx, RIJK_PROF_J_OTHER, st);
+    rijk::launch_j_finalize(g, Jp, spin, splits, scale, out_kind, d_out, st);
+  }
   return after_launch(ctx, "vj");
 }
 
@@ -235,7 +294,10 @@ int vk_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int
   const int64_t ocols = round_up(spin == 2 ? coff[1] + nw[1] : nw[0], 64);
   RIJK_TRY(ensure(ctx, ctx->Cw, (size_t)ldx * ocols * 8));
   double* Cw = static_cast<double*>(ctx->Cw.p);
-  rijk::launch_k_prepare_c(g, d_eigv, g.n, g.n * num_state, d_occ, num_state, nw, spin, ldx, ocols, Cw, st);
+  {
+    ProfScope ps(ctx, RIJK_PROF_K_OTHER, st);
+    rijk::launch_k_prepare_c(g, d_eigv, g.n, g.n * num_state, d_occ, num_state, nw, spin, ldx, ocols, Cw, st);
+  }
   const int64_t per_p = ldx * ocols * 8;
   const int64_t pchunk = std::max<int64_t>(1, std::min<int64_t>(g.naux, (int64_t)ctx->scratch_budget / per_p));
   RIJK_TRY(ensure(ctx, ctx->X, (size_t)pchunk * per_p));
@@ -245,11 +307,18 @@ int vk_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int
   double* Kp = static_cast<double*>(ctx->Kpart.p);
   for (int64_t p0 = 0; p0 < g.naux; p0 += pchunk) {
     const int64_t np = std::min(pchunk, g.naux - p0);
-    rijk::launch_half_transform(g, ctx->dB, p0, np, Cw, ldx, ocols, X, ldx, ldx * ocols, ctx->d_err, st);
+    {
+      ProfScope ps(ctx, RIJK_PROF_K_HALF, st);
+      rijk::launch_half_transform(g, ctx->dB, p0, np, Cw, ldx, ocols, X, ldx, ldx * ocols, ctx->d_err, st);
+    }
     for (int s = 0; s < spin; ++s) {
       if (nw[s] == 0) continue;
       const int splits = rijk::k_rank_splits(g, np, 0);
-      rijk::launch_k_rank_update(g, X, ldx, ldx * ocols, np, coff[s], nw[s], splits, 0, Kp, ctx->d_err, st);
+      {
+        ProfScope ps(ctx, RIJK_PROF_K_RANK, st);
+        rijk::launch_k_rank_update(g, X, ldx, ldx * ocols, np, coff[s], nw[s], splits, 0, Kp, ctx->d_err, st);
+      }
+      ProfScope ps(ctx, RIJK_PROF_K_OTHER, st);
       rijk::launch_k_finalize(g, Kp, splits, 0, scale, p0 > 0 ? 1 : 0, 0, d_out + s * g.npair, st);
     }
   }
@@ -271,12 +340,22 @@ int vk_dm_dev(rijk_ctx* ctx, const double* d_dm, int spin, double scale, int ful
   double* Kp = static_cast<double*>(ctx->Kpart.p);
   const int64_t per_out = full ? g.n * g.n : g.npair;
   for (int s = 0; s < spin; ++s) {
-    rijk::launch_pad_square(d_dm + s * g.n * g.n, g.n, g.n, ldx, Dp, st);
+    {
+      ProfScope ps(ctx, RIJK_PROF_K_OTHER, st);
+      rijk::launch_pad_square(d_dm + s * g.n * g.n, g.n, g.n, ldx, Dp, st);
+    }
     for (int64_t p0 = 0; p0 < g.naux; p0 += pchunk) {
       const int64_t np = std::min(pchunk, g.naux - p0);
-      rijk::launch_half_transform(g, ctx->dB, p0, np, Dp, ldx, ldx, T, ldx, ldx * ldx, ctx->d_err, st);
+      {
+        ProfScope ps(ctx, RIJK_PROF_K_HALF, st);
+        rijk::launch_half_transform(g, ctx->dB, p0, np, Dp, ldx, ldx, T, ldx, ldx * ldx, ctx->d_err, st);
+      }
       const int splits = rijk::k_rank_splits(g, np, full);
-      rijk::launch_k_dm_update(g, T, ldx, ldx * ldx, ctx->dB, p0, np, splits, full, Kp, ctx->d_err, st);
+      {
+        ProfScope ps(ctx, RIJK_PROF_K_DM, st);
+        rijk::launch_k_dm_update(g, T, ldx, ldx * ldx, ctx->dB, p0, np, splits, full, Kp, ctx->d_err, st);
+      }
+      ProfScope ps(ctx, RIJK_PROF_K_OTHER, st);
       rijk::launch_k_finalize(g, Kp, splits, full, scale, p0 > 0 ? 1 : 0, full ? 1 : 0, d_out + s * per_out, st);
     }
   }
@@ -354,6 +433,11 @@ int rijk_ctx_destroy(rijk_ctx* ctx) {
                     &ctx->dout,  &ctx->docc, &ctx->mV, &ctx->mLinv, &ctx->mT, &ctx->mLinvd, &ctx->mOut};
   for (DevBuf* b : bufs)
     if (b->p) cudaFree(b->p);
+  for (auto& r : ctx->prof_pending) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->dB) cudaFree(ctx->dB);
   if (ctx->d_err) cudaFree(ctx->d_err);
   if (ctx->d_info) cudaFree(ctx->d_info);
@@ -373,6 +457,36 @@ int rijk_ctx_info(const rijk_ctx* ctx, int64_t* num_basis, int64_t* num_auxbas, 
 }
 
 void* rijk_ctx_stream(rijk_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int64_t rijk_kernel_launches(void) { return rijk::launch_count(); }
+
+int rijk_ctx_profile(rijk_ctx* ctx, int enable) {
+  if (!ctx) return RIJK_ERR_ARG;
+  ctx->prof = enable != 0;
+  return RIJK_OK;
+}
+
+int rijk_ctx_profile_read(rijk_ctx* ctx, double* ms, int64_t* launches) {
+  if (!ctx) return RIJK_ERR_ARG;
+  RIJK_CK(cudaSetDevice(ctx->device));
+  for (auto& r : ctx->prof_pending) {
+    RIJK_CK(cudaEventSynchronize(r.b));
+    float t = 0.f;
+    RIJK_CK(cudaEventElapsedTime(&t, r.a, r.b));
+    ctx->prof_ms[r.cls] += t;
+    ctx->prof_n[r.cls] += 1;
+    ctx->ev_pool.push_back(r.a);
+    ctx->ev_pool.push_back(r.b);
+  }
+  ctx->prof_pending.clear();
+  for (int i = 0; i < RIJK_PROF_NCLASS; ++i) {
+    if (ms) ms[i] = ctx->prof_ms[i];
+    if (launches) launches[i] = ctx->prof_n[i];
+    ctx->prof_ms[i] = 0.0;
+    ctx->prof_n[i] = 0;
+  }
+  return RIJK_OK;
+}
 
 int rijk_ctx_tensor(rijk_ctx* ctx, const double** d_tensor, int64_t* row_stride) {
   RIJK_TRY(need_tensor(ctx));

@@ -16,6 +16,11 @@ struct Geom {
 };
 Geom make_geom(int64_t n, int64_t naux);
 
+// Process-wide count of kernels this library has launched (every launch_*
+// and run_* helper adds the launches it issues).
+void count_launch(int64_t k = 1);
+int64_t launch_count();
+
 // --- layout conversion -------------------------------------------------------
 // rimatr (REST MatrixFull[npair, N], column P = packed upper of B_P), rows
 // [p0, p0 + np) -> tile-packed rows [p0, p0 + np) of dB.

@@ -76,16 +76,19 @@ __global__ void __launch_bounds__(256) k_unpack_rimatr(int64_t n, int64_t npair,
 void launch_pack_rimatr(const Geom& g, const double* src, int64_t np, double* dst, cudaStream_t st) {
   if (np <= 0) return;
   dim3 grid((unsigned)g.ntp, (unsigned)std::min<int64_t>(np, 65535));
+  count_launch();
   k_pack<<<grid, 256, 0, st>>>(g.n, g.npair, g.ldB, src, 0, np, dst);
 }
 void launch_pack_ri3fn(const Geom& g, const double* src, int64_t np, double* dst, cudaStream_t st) {
   if (np <= 0) return;
   dim3 grid((unsigned)g.ntp, (unsigned)std::min<int64_t>(np, 65535));
+  count_launch();
   k_pack<<<grid, 256, 0, st>>>(g.n, g.npair, g.ldB, src, 1, np, dst);
 }
 void launch_unpack_rimatr(const Geom& g, const double* src, int64_t np, double* dst, cudaStream_t st) {
   if (np <= 0) return;
   dim3 grid((unsigned)std::min<int64_t>(cdiv(g.npair, 256), 4096), (unsigned)std::min<int64_t>(np, 65535));
+  count_launch();
   k_unpack_rimatr<<<grid, 256, 0, st>>>(g.n, g.npair, g.ldB, src, np, dst);
 }
 
@@ -124,6 +127,7 @@ __global__ void __launch_bounds__(256) k_j_weights(int64_t n, int64_t ldB, const
 void launch_j_weights(const Geom& g, const double* dm, int nspin, int mode, double* W, cudaStream_t st) {
   const int64_t total = nspin * g.ldB;
   const unsigned blocks = (unsigned)std::min<int64_t>(cdiv(total, 256), 148 * 16);
+  count_launch();
   k_j_weights<<<blocks, 256, 0, st>>>(g.n, g.ldB, dm, nspin, mode, W);
 }
 
@@ -200,6 +204,7 @@ __global__ void __launch_bounds__(256) k_j_pass1(const double* __restrict__ B, c
 }
 
 void launch_j_pass1(const Geom& g, const double* B, const double* W, int nspin, double* w, cudaStream_t st) {
+  count_launch();
   if (nspin == 2)
     k_j_pass1<2><<<(unsigned)g.naux, 256, 0, st>>>(B, W, g.ldB, g.naux, w);
   else
@@ -260,6 +265,7 @@ __global__ void __launch_bounds__(256) k_j_pass2(const double* __restrict__ B, c
 void launch_j_pass2(const Geom& g, const double* B, const double* w, int nspin, int splits, double* Jpart,
                     cudaStream_t st) {
   dim3 grid((unsigned)cdiv(g.ldB / 2, 256), (unsigned)splits);
+  count_launch();
   if (nspin == 2)
     k_j_pass2<2><<<grid, 256, 0, st>>>(B, w, g.ldB, g.naux, splits, Jpart);
   else
@@ -293,6 +299,7 @@ void launch_j_finalize(const Geom& g, const double* Jpart, int nspin, int splits
                        double* out, cudaStream_t st) {
   const int64_t total = nspin * (out_kind == 0 ? g.npair : g.n * g.n);
   const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), 148 * 16));
+  count_launch();
   k_j_finalize<<<blocks, 256, 0, st>>>(g.n, g.npair, g.ldB, Jpart, nspin, splits, scale, out_kind, out);
 }
 
@@ -331,6 +338,7 @@ void launch_k_prepare_c(const Geom& g, const double* eigv, int64_t ld_eigv, int6
   const int64_t coff1 = round_up(nw[0], TS);
   const int64_t total = ldc * ocols;
   const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), 148 * 16));
+  count_launch();
   k_prepare_c<<<blocks, 256, 0, st>>>(g.n, eigv, ld_eigv, stride_eigv, occ, stride_occ, nw[0], nspin == 2 ? nw[1] : 0,
                                       coff1, nspin, ldc, ocols, Cw);
 }
@@ -347,6 +355,7 @@ __global__ void __launch_bounds__(256) k_pad_square(const double* __restrict__ s
 void launch_pad_square(const double* src, int64_t n, int64_t ldsrc, int64_t ldc, double* dst, cudaStream_t st) {
   const int64_t total = ldc * ldc;
   const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), 148 * 16));
+  count_launch();
   k_pad_square<<<blocks, 256, 0, st>>>(src, n, ldsrc, ldc, dst);
 }
 
@@ -396,6 +405,7 @@ void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t n
   cudaFuncSetAttribute(k_half_transform<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
   const int nrb = (int)(ldx / Cfg::BM);
   dim3 grid((unsigned)(np * nrb), (unsigned)(ncol / Cfg::BN));
+  count_launch();
   k_half_transform<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(B, g.ldB, p0, nrb, W, ldw, (int)g.nt, X, ldx,
                                                                       sxp, err);
 }
@@ -476,6 +486,7 @@ void launch_k_rank_update(const Geom& g, const double* X, int64_t ldx, int64_t s
   const int c0t = (int)(c0 / TS);
   const int ctiles = (int)cdiv(ncol, TS);
   dim3 grid((unsigned)pairs, (unsigned)splits);
+  count_launch();
   k_rank_update<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(X, ldx, sxp, np, c0t, ctiles, splits, full, nkb,
                                                                    pairs, Kpart, err);
 }
@@ -537,6 +548,7 @@ void launch_k_dm_update(const Geom& g, const double* T, int64_t ldt, int64_t stp
   const int64_t nkb = cdiv(g.n, KB);
   const int64_t pairs = k_block_pairs(g, full);
   dim3 grid((unsigned)pairs, (unsigned)splits);
+  count_launch();
   k_dm_update<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(T, ldt, stp, B, g.ldB, p0, np, (int)g.nt, splits,
                                                                  full, nkb, pairs, Kpart, err);
 }
@@ -570,8 +582,16 @@ void launch_k_finalize(const Geom& g, const double* Kpart, int splits, int full,
   const int64_t pairs = k_block_pairs(g, full);
   const int64_t total = out_kind == 0 ? g.npair : g.n * g.n;
   const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), 148 * 16));
+  count_launch();
   k_k_finalize<<<blocks, 256, 0, st>>>(g.n, g.npair, Kpart, splits, full, nkb, pairs, scale, accumulate, out_kind,
                                        out);
 }
 
+}  // namespace rijk
+
+#include <atomic>
+namespace rijk {
+static std::atomic<int64_t> g_launches{0};
+void count_launch(int64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 }  // namespace rijk

@@ -91,6 +91,7 @@ static void launch_dgemm_cfg(int64_t M, int64_t N, int64_t K, double alpha, cons
                              cudaStream_t st) {
   cudaFuncSetAttribute(k_dgemm<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
   dim3 grid((unsigned)cdiv_m(M, Cfg::BM), (unsigned)cdiv_m(N, Cfg::BN), (unsigned)batch);
+  count_launch();
   k_dgemm<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(M, N, K, alpha, A, lda, ta, B, ldb, tb, beta, C, ldc,
                                                             klim, lower_only, sa, sb, sc, err);
 }
@@ -157,6 +158,7 @@ __global__ void __launch_bounds__(1024) k_potrf_diag(double* A, int64_t lda, int
 void run_potrf(double* A, int64_t np, int64_t lda, double* Linvd, int* d_info, int* err, cudaStream_t st) {
   const int64_t nb = np / TS;
   for (int64_t j = 0; j < nb; ++j) {
+    count_launch();
     k_potrf_diag<<<1, 1024, 0, st>>>(A, lda, j, Linvd, d_info);
     const int64_t rem = np - (j + 1) * TS;
     if (rem <= 0) break;
@@ -194,6 +196,7 @@ __global__ void __launch_bounds__(256) k_zero_upper(double* L, int64_t np, int64
 void run_trtri(const double* L, int64_t np, int64_t ld, const double* Linvd, double* Linv, double* T, int* err,
                cudaStream_t st) {
   const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv_m(np * np, 256), 148 * 16));
+  count_launch();
   k_trtri_init<<<blocks, 256, 0, st>>>(Linvd, np, ld, Linv);
   for (int64_t h = TS; h < np; h *= 2) {
     const int64_t full_pairs = np / (2 * h);
@@ -231,6 +234,7 @@ __global__ void __launch_bounds__(256) k_pad_matrix(const double* __restrict__ s
 
 void launch_pad_matrix(const double* src, int64_t n, int64_t np, double* dst, cudaStream_t st) {
   const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv_m(np * np, 256), 148 * 16));
+  count_launch();
   k_pad_matrix<<<blocks, 256, 0, st>>>(src, n, np, dst);
 }
 
@@ -248,6 +252,7 @@ __global__ void __launch_bounds__(256) k_fit_copy_back(const double* __restrict_
 void launch_fit_copy_back(const double* out, int64_t kc, double* dB, int64_t ldB, int64_t k0, int64_t rows,
                           cudaStream_t st) {
   const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv_m(kc * rows, 256), 148 * 32));
+  count_launch();
   k_fit_copy_back<<<blocks, 256, 0, st>>>(out, kc, dB, ldB, k0, rows);
 }
 

@@ -98,6 +98,23 @@ class RIJK:
         self._check(lib().rijk_ctx_info(self._h, None, None, C.byref(b)))
         return b.value
 
+    PROF_CLASSES = ("j_pass1", "j_pass2", "j_other", "k_half", "k_rank", "k_dm", "k_other")
+
+    def profile(self, enable: bool = True):
+        self._check(lib().rijk_ctx_profile(self._h, int(bool(enable))))
+
+    def profile_read(self) -> dict:
+        """{class: (milliseconds, launches)} accumulated since the last read."""
+        k = len(self.PROF_CLASSES)
+        ms = (C.c_double * k)()
+        cnt = (C.c_int64 * k)()
+        self._check(lib().rijk_ctx_profile_read(self._h, ms, cnt))
+        return {name: (ms[i], cnt[i]) for i, name in enumerate(self.PROF_CLASSES)}
+
+    @staticmethod
+    def kernel_launches() -> int:
+        return int(lib().rijk_kernel_launches())
+
     def synchronize(self, stream: int = 0):
         self._check(lib().rijk_ctx_synchronize(self._h, C.c_void_p(stream or None)))
 
