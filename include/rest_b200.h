@@ -160,6 +160,25 @@ int rijk_vk_upper_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state
 int rijk_vk_upper_dm_dev(rijk_ctx* ctx, const double* d_dm, int spin_channel, double scaling_factor, double* d_vk,
                          void* stream);
 
+/* ---- J without any device allocation ----------------------------------------- */
+/* No counterpart in REST.  Same result as rijk_vj_upper_dev for callers that
+ * cannot let a library call cudaMalloc (their device memory is owned by another
+ * allocator or a fixed arena, or a cudaMalloc between builds would synchronise
+ * their pipeline).  Inputs and outputs are the caller's device pointers:
+ * d_tensor/row_stride as returned by rijk_ctx_tensor for a loaded tensor;
+ * d_dm, d_vj as in rijk_vj_upper_dev; the work is enqueued on `stream`.
+ * Scratch lives in one static device array of RIJK_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading the library holds until exit; sizes needing more
+ * (2 spin ldB + spin N doubles: n <= 2016 for spin 1 and n <= 1408 for
+ * spin 2 at N = 4n) return RIJK_ERR_TOO_LARGE.  The first call on a device
+ * looks the array's address up (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller. */
+#define RIJK_NOALLOC_SCRATCH_BYTES (32ull << 20)
+int rijk_vj_upper_noalloc(const double* d_tensor, int64_t row_stride, int64_t num_basis, int64_t num_auxbas,
+                          const double* d_dm, int spin_channel, double scaling_factor, int dm_mode, double* d_vj,
+                          void* stream);
+
 /* ---- SCF pieces around the build ------------------------------------------- */
 /* generate_density_matrix (src/scf_io/mod.rs:441-478): D = (C occ) C^T over the
  * first homo+1 columns, per spin; dm: spin_channel x (n x n). */

@@ -137,6 +137,13 @@ class RIJK:
         self._check(lib().rijk_set_ri3fn(self._h, _ptr(r), n, naux))
         self.num_basis, self.num_auxbas = n, naux
 
+    def tensor_ptr(self) -> tuple[int, int]:
+        """(device address, row stride in doubles) of the tile-packed tensor."""
+        p = C.c_void_p()
+        ld = C.c_int64()
+        self._check(lib().rijk_ctx_tensor(self._h, C.byref(p), C.byref(ld)))
+        return int(p.value), int(ld.value)
+
     def tensor_alloc(self, num_basis: int, num_auxbas: int):
         self._check(lib().rijk_tensor_alloc(self._h, num_basis, num_auxbas))
         self.num_basis, self.num_auxbas = num_basis, num_auxbas
