@@ -78,6 +78,13 @@ enum rijk_prof_class {
   RIJK_PROF_K_OTHER = 6,    /* operand preparation, reduction   */
   RIJK_PROF_NCLASS = 7
 };
+/* CTA shapes of the K kernels (results agree to rounding across them).  All
+ * are 64x64 tiles of 4 DMMA warps; for both the half-transform and the updates:
+ * 0: cp.async staging, 3 stages (2 CTAs/SM); 1: cp.async, 2 stages (3 CTAs/SM,
+ * the default); 2: cp.async, 4 stages (1 CTA/SM); 3: bulk copies issued by a
+ * producer warp, 3 stages.  RIJK_HT_CFG / RIJK_RK_CFG override the defaults
+ * at context creation. */
+int rijk_ctx_set_tiles(rijk_ctx* ctx, int half_transform_cfg, int update_cfg);
 int rijk_ctx_profile(rijk_ctx* ctx, int enable);
 int rijk_ctx_profile_read(rijk_ctx* ctx, double* ms, int64_t* launches);
 /* Wait for the work enqueued on `stream` (NULL = the context's stream) and

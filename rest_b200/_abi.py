@@ -52,6 +52,7 @@ SIGNATURES = {
     "rijk_ctx_synchronize": (C.c_int, [_ctxp, C.c_void_p]),
     "rijk_kernel_launches": (C.c_int64, []),
     "rijk_ctx_profile": (C.c_int, [_ctxp, C.c_int]),
+    "rijk_ctx_set_tiles": (C.c_int, [_ctxp, C.c_int, C.c_int]),
     "rijk_ctx_profile_read": (C.c_int, [_ctxp, _dp, _i64p]),
     "rijk_set_rimatr": (C.c_int, [_ctxp, C.c_void_p, C.c_int64, C.c_int64]),
     "rijk_set_ri3fn": (C.c_int, [_ctxp, C.c_void_p, C.c_int64, C.c_int64]),

@@ -40,6 +40,7 @@ struct rijk_ctx {
   int* d_info = nullptr;  // Cholesky failing pivot
   DevBuf stage, W, w, Jpart, Cw, X, Kpart, din, dout, docc, mV, mLinv, mT, mLinvd, mOut;
   size_t scratch_budget = (size_t)4 << 30;
+  int ht_cfg = 1, rk_cfg = 1;  // CTA shapes of the K kernels (fastest measured on B200)
   std::string last;
   // per-kernel-class event timers
   struct ProfRec {
@@ -186,6 +187,8 @@ int alloc_tensor(rijk_ctx* ctx, int64_t n, int64_t naux) {
                             ctx->stream));
   ctx->g = g;
   ctx->naux_pad = naux_pad;
+  ctx->g.ht_cfg = ctx->ht_cfg;
+  ctx->g.rk_cfg = ctx->rk_cfg;
   ctx->have = false;
   return RIJK_OK;
 }
@@ -291,7 +294,8 @@ int vk_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int
   }
   const int64_t ldx = round_up(g.n, 128);
   const int64_t coff[2] = {0, round_up(nw[0], rijk::TS)};
-  const int64_t ocols = round_up(spin == 2 ? coff[1] + nw[1] : nw[0], 64);
+  const int64_t ocols_valid = spin == 2 ? coff[1] + nw[1] : nw[0];
+  const int64_t ocols = round_up(ocols_valid, 128);  // a multiple of every half-transform CTA width
   RIJK_TRY(ensure(ctx, ctx->Cw, (size_t)ldx * ocols * 8));
   double* Cw = static_cast<double*>(ctx->Cw.p);
   {
@@ -309,7 +313,8 @@ int vk_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int
     const int64_t np = std::min(pchunk, g.naux - p0);
     {
       ProfScope ps(ctx, RIJK_PROF_K_HALF, st);
-      rijk::launch_half_transform(g, ctx->dB, p0, np, Cw, ldx, ocols, X, ldx, ldx * ocols, ctx->d_err, st);
+      rijk::launch_half_transform(g, ctx->dB, p0, np, Cw, ldx, ocols, ocols_valid, X, ldx, ldx * ocols, ctx->d_err,
+                                  st);
     }
     for (int s = 0; s < spin; ++s) {
       if (nw[s] == 0) continue;
@@ -348,7 +353,7 @@ int vk_dm_dev(rijk_ctx* ctx, const double* d_dm, int spin, double scale, int ful
       const int64_t np = std::min(pchunk, g.naux - p0);
       {
         ProfScope ps(ctx, RIJK_PROF_K_HALF, st);
-        rijk::launch_half_transform(g, ctx->dB, p0, np, Dp, ldx, ldx, T, ldx, ldx * ldx, ctx->d_err, st);
+        rijk::launch_half_transform(g, ctx->dB, p0, np, Dp, ldx, ldx, g.n, T, ldx, ldx * ldx, ctx->d_err, st);
       }
       const int splits = rijk::k_rank_splits(g, np, full);
       {
@@ -411,6 +416,8 @@ int rijk_ctx_create(int device, rijk_ctx** out) {
   if (cudaSetDevice(device) != cudaSuccess) return RIJK_ERR_CUDA;
   rijk_ctx* c = new rijk_ctx();
   c->device = device;
+  if (const char* s = getenv("RIJK_HT_CFG")) c->ht_cfg = std::max(0, std::min(3, atoi(s)));
+  if (const char* s = getenv("RIJK_RK_CFG")) c->rk_cfg = std::max(0, std::min(3, atoi(s)));
   if (const char* s = getenv("RIJK_SCRATCH_BYTES")) {
     const long long v = atoll(s);
     if (v > (1 << 20)) c->scratch_budget = (size_t)v;
@@ -459,6 +466,14 @@ int rijk_ctx_info(const rijk_ctx* ctx, int64_t* num_basis, int64_t* num_auxbas, 
 void* rijk_ctx_stream(rijk_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 int64_t rijk_kernel_launches(void) { return rijk::launch_count(); }
+
+int rijk_ctx_set_tiles(rijk_ctx* ctx, int half_transform_cfg, int update_cfg) {
+  if (!ctx || half_transform_cfg < 0 || half_transform_cfg > 3 || update_cfg < 0 || update_cfg > 3)
+    return set_err(ctx, RIJK_ERR_ARG, "tile configuration out of range");
+  ctx->ht_cfg = ctx->g.ht_cfg = half_transform_cfg;
+  ctx->rk_cfg = ctx->g.rk_cfg = update_cfg;
+  return RIJK_OK;
+}
 
 int rijk_ctx_profile(rijk_ctx* ctx, int enable) {
   if (!ctx) return RIJK_ERR_ARG;

@@ -1,5 +1,5 @@
 // CTA-level FP64 tensor-core (DMMA, mma.m8n8k4.f64) contraction over 32x32
-// operand slots staged by bulk copies.
+// operand slots staged by bulk copies, with a dedicated producer warp.
 //
 // A CTA computes a (MT*32) x (NT*32) block of  sum_kt  A_kt * B_kt  where each
 // k-step kt contributes MT A-slots (32 rows x 32 k) and NT B-slots (32 k x 32
@@ -10,11 +10,17 @@
 //   32 columns of 32 contiguous doubles).  For an A-slot, A[m][k] = S[m][k]
 //   when trans == 0 and S[k][m] when trans == 1; for a B-slot, B[k][n] = S[k][n]
 //   when trans == 0 and S[n][k] when trans == 1.  ptr == nullptr stages zeros.
+//   kvalid(kt) is the number of k columns of step kt that can be non-zero
+//   (the rest is padding and its k4 steps are skipped).
 //
-// Staging: warp 0 issues one 256-byte cp.async.bulk per slot column into a
-// slot with leading dimension 36 doubles (36 = 4 mod 16 makes the m8n8k4
-// fragment loads bank-conflict free in both orientations), all completing on
-// the stage's mbarrier.  STAGES stages are in flight; every wait is bounded.
+// Warp roles: warps 0 .. WM*WN-1 compute, the last warp produces.  The producer
+// waits until a stage is released (empty mbarrier, one arrival per consumer
+// warp), writes the stage's orientation flags, arms the full mbarrier with the
+// stage's byte count and issues one 256-byte cp.async.bulk per slot column (one
+// per lane) into a slot with leading dimension 36 doubles (36 = 4 mod 16 makes
+// the m8n8k4 fragment loads bank-conflict free in both orientations).
+// Consumers wait on full, run the DMMAs, and release the stage.  No CTA-wide
+// barrier runs inside the k-loop; every wait is bounded.
 #pragma once
 #include "rijk_common.cuh"
 
@@ -26,118 +32,346 @@ struct SlotSrc {
   int trans;
 };
 
-template <int MT_, int NT_, int WM_, int WN_, int STAGES_>
+template <int MT_, int NT_, int WM_, int WN_, int STAGES_, bool CPASYNC_ = false>
 struct DmmaCfg {
   static constexpr int MT = MT_, NT = NT_, WM = WM_, WN = WN_, STAGES = STAGES_;
+  static constexpr bool CPASYNC = CPASYNC_;  // cp.async staging instead of the bulk-copy producer
   static constexpr int BM = MT * TS, BN = NT * TS;
-  static constexpr int WARPS = WM * WN, THREADS = WARPS * 32;
-  static constexpr int WTM = BM / WM, WTN = BN / WN;  // warp tile
-  static constexpr int FM = WTM / 8, FN = WTN / 8;    // m8n8 fragments per warp
+  static constexpr int CWARPS = WM * WN;                  // consumer warps
+  static constexpr int THREADS = (CWARPS + (CPASYNC ? 0 : 1)) * 32;  // + producer warp
+  static constexpr int WTM = BM / WM, WTN = BN / WN;      // warp tile
+  static constexpr int FM = WTM / 8, FN = WTN / 8;        // m8n8 fragments per warp
   static constexpr int SLOTS = MT + NT;
   static constexpr int STAGE_DOUBLES = SLOTS * SLOT_DOUBLES;
   static constexpr uint32_t STAGE_BYTES = SLOTS * TS * TS * 8;  // bytes landed per stage
-  static constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_DOUBLES * 8 + 64;
+  // slots | full[STAGES] | empty[STAGES] | flags[STAGES][SLOTS]
+  static constexpr size_t BAR_OFFSET = (size_t)STAGES * STAGE_DOUBLES * 8;
+  static constexpr size_t FLAG_OFFSET = BAR_OFFSET + 2 * STAGES * 8;
+  static constexpr size_t SMEM_BYTES = FLAG_OFFSET + ((STAGES * SLOTS + 15) / 16) * 16;
   static_assert(BM % WM == 0 && BN % WN == 0, "warp grid");
   static_assert(WTM % 8 == 0 && WTN % 8 == 0, "warp tile");
   static_assert(TS % WTM == 0 || WTM % TS == 0, "warp rows vs slot");
   static_assert(TS % WTN == 0 || WTN % TS == 0, "warp cols vs slot");
 };
 
-template <class Cfg, class Sched>
-__device__ __forceinline__ void dmma_issue_stage(const Sched& sc, int kt, double* stage, uint64_t* bar) {
-  const int lane = threadIdx.x & 31;
-  if (lane == 0) mbar_arrive_expect_tx(bar, Cfg::STAGE_BYTES);
-  __syncwarp();
-#pragma unroll
-  for (int s = 0; s < Cfg::SLOTS; ++s) {
-    const SlotSrc src = (s < Cfg::MT) ? sc.a(kt, s) : sc.b(kt, s - Cfg::MT);
-    const double* g = src.ptr ? src.ptr + (int64_t)lane * src.ld : g_zero_tile + lane * TS;
-    bulk_g2s(stage + s * SLOT_DOUBLES + lane * SLD, g, TS * 8, bar);
+struct DefaultKValid {
+  __device__ int operator()(int) const { return TS; }
+};
+
+template <class Cfg>
+struct DmmaSmem {
+  double* slots;
+  uint64_t* full;
+  uint64_t* empty;
+  uint8_t* flags;
+  __device__ explicit DmmaSmem(void* base) {
+    char* b = static_cast<char*>(base);
+    slots = reinterpret_cast<double*>(b);
+    full = reinterpret_cast<uint64_t*>(b + Cfg::BAR_OFFSET);
+    empty = full + Cfg::STAGES;
+    flags = reinterpret_cast<uint8_t*>(b + Cfg::FLAG_OFFSET);
   }
+};
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Runs the k-loop of one CTA tile; acc[fm][fn][2] holds, for this thread, the
-// elements (m = warp_m0 + 8 fm + lane/4, n = warp_n0 + 8 fn + 2 (lane%4) + j).
-// Returns false if a stage wait timed out (the device error flag is then set).
+// Producer warp: stages every k-step.  Returns false on a timed-out wait.
 template <class Cfg, class Sched>
-__device__ __forceinline__ bool dmma_mainloop(const Sched& sc, int ktiles, double* smem, uint64_t* bars,
-                                              double (&acc)[Cfg::FM][Cfg::FN][2], int* err) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int warp_m0 = (warp / Cfg::WN) * Cfg::WTM;
-  const int warp_n0 = (warp % Cfg::WN) * Cfg::WTN;
-
-#pragma unroll
-  for (int i = 0; i < Cfg::FM; ++i)
-#pragma unroll
-    for (int j = 0; j < Cfg::FN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-  if (tid == 0) {
-    for (int s = 0; s < Cfg::STAGES; ++s) mbar_init(&bars[s], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-
-  if (warp == 0) {
-    for (int s = 0; s < Cfg::STAGES && s < ktiles; ++s)
-      dmma_issue_stage<Cfg>(sc, s, smem + s * Cfg::STAGE_DOUBLES, &bars[s]);
-  }
-
+__device__ __forceinline__ bool dmma_produce(const Sched& sc, int ktiles, DmmaSmem<Cfg>& sm, int* err) {
+  const int lane = threadIdx.x & 31;
   for (int kt = 0; kt < ktiles; ++kt) {
     const int st = kt % Cfg::STAGES;
-    const uint32_t parity = (uint32_t)((kt / Cfg::STAGES) & 1);
-    const bool ok = mbar_wait_bounded(&bars[st], parity, err);
-    if (!__syncthreads_and(ok)) {
-      // Give the copies still in flight (stages kt+1 .. kt+STAGES-1) a bounded
-      // time to land before the CTA's shared memory is released.
-      if (tid == 0)
-        for (int k2 = kt + 1; k2 < ktiles && k2 < kt + Cfg::STAGES; ++k2)
-          mbar_wait_bounded(&bars[k2 % Cfg::STAGES], (uint32_t)((k2 / Cfg::STAGES) & 1), nullptr);
-      __syncthreads();
-      return false;
+    if (kt >= Cfg::STAGES) {
+      const uint32_t parity = (uint32_t)(((kt / Cfg::STAGES) - 1) & 1);
+      if (!mbar_wait_bounded(&sm.empty[st], parity, err)) return false;
     }
-    const double* sbase = smem + st * Cfg::STAGE_DOUBLES;
-
-    // Per-fragment slot offsets and k strides for this k-step.
-    int aoff[Cfg::FM], ask[Cfg::FM], boff[Cfg::FN], bsk[Cfg::FN];
-#pragma unroll
-    for (int fm = 0; fm < Cfg::FM; ++fm) {
-      const int m = warp_m0 + fm * 8 + (lane >> 2);
-      const int slot = m / TS, r = m % TS;
-      const int tr = sc.a(kt, slot).trans;
-      const int sm = tr ? SLD : 1, sk = tr ? 1 : SLD;
-      aoff[fm] = slot * SLOT_DOUBLES + r * sm + (lane & 3) * sk;
-      ask[fm] = 4 * sk;
+    if (lane == 0) {
+#pragma unroll 1
+      for (int s = 0; s < Cfg::SLOTS; ++s) {
+        const SlotSrc src = (s < Cfg::MT) ? sc.a(kt, s) : sc.b(kt, s - Cfg::MT);
+        sm.flags[st * Cfg::SLOTS + s] = (uint8_t)src.trans;
+      }
+      mbar_arrive_expect_tx(&sm.full[st], Cfg::STAGE_BYTES);
     }
-#pragma unroll
-    for (int fn = 0; fn < Cfg::FN; ++fn) {
-      const int n = warp_n0 + fn * 8 + (lane >> 2);
-      const int slot = n / TS, c = n % TS;
-      const int tr = sc.b(kt, slot).trans;
-      const int sn = tr ? 1 : SLD, sk = tr ? SLD : 1;
-      boff[fn] = (Cfg::MT + slot) * SLOT_DOUBLES + c * sn + (lane & 3) * sk;
-      bsk[fn] = 4 * sk;
+    __syncwarp();
+    double* stage = sm.slots + st * Cfg::STAGE_DOUBLES;
+#pragma unroll 1
+    for (int s = 0; s < Cfg::SLOTS; ++s) {
+      const SlotSrc src = (s < Cfg::MT) ? sc.a(kt, s) : sc.b(kt, s - Cfg::MT);
+      const double* g = src.ptr ? src.ptr + (int64_t)lane * src.ld : g_zero_tile + lane * TS;
+      bulk_g2s(stage + s * SLOT_DOUBLES + lane * SLD, g, TS * 8, &sm.full[st]);
     }
-
-#pragma unroll
-    for (int kk = 0; kk < TS / 4; ++kk) {
-      double af[Cfg::FM], bf[Cfg::FN];
-#pragma unroll
-      for (int fm = 0; fm < Cfg::FM; ++fm) af[fm] = sbase[aoff[fm] + kk * ask[fm]];
-#pragma unroll
-      for (int fn = 0; fn < Cfg::FN; ++fn) bf[fn] = sbase[boff[fn] + kk * bsk[fn]];
-#pragma unroll
-      for (int fm = 0; fm < Cfg::FM; ++fm)
-#pragma unroll
-        for (int fn = 0; fn < Cfg::FN; ++fn) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], af[fm], bf[fn]);
-    }
-    __syncthreads();  // every warp is done reading stage st
-    if (warp == 0 && kt + Cfg::STAGES < ktiles)
-      dmma_issue_stage<Cfg>(sc, kt + Cfg::STAGES, smem + st * Cfg::STAGE_DOUBLES, &bars[st]);
   }
   return true;
 }
 
-// Visits every accumulator element of this thread with its CTA-local (m, n).
+// Consumer warps: acc[fm][fn][2] holds, for this thread, the elements
+// (m = warp_m0 + 8 fm + lane/4, n = warp_n0 + 8 fn + 2 (lane%4) + j).
+// Fragments at or beyond (mvalid, nvalid) (CTA-local) are known to be zero
+// and are skipped.  Returns false if a stage wait timed out.
+template <class Cfg, class KValid>
+__device__ __forceinline__ bool dmma_consume(int ktiles, DmmaSmem<Cfg>& sm, double (&acc)[Cfg::FM][Cfg::FN][2],
+                                             int mvalid, int nvalid, const KValid& kvalid, int* err) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int warp_m0 = (warp / Cfg::WN) * Cfg::WTM;
+  const int warp_n0 = (warp % Cfg::WN) * Cfg::WTN;
+  const int fm_lim = max(0, min(Cfg::FM, (mvalid - warp_m0 + 7) / 8));
+  const int fn_lim = max(0, min(Cfg::FN, (nvalid - warp_n0 + 7) / 8));
+  const bool idle = fm_lim == 0 || fn_lim == 0;
+  for (int kt = 0; kt < ktiles; ++kt) {
+    const int st = kt % Cfg::STAGES;
+    const uint32_t parity = (uint32_t)((kt / Cfg::STAGES) & 1);
+    if (!mbar_wait_bounded(&sm.full[st], parity, err)) return false;
+    if (!idle) {
+      const double* sbase = sm.slots + st * Cfg::STAGE_DOUBLES;
+      const uint8_t* fl = sm.flags + st * Cfg::SLOTS;
+      // One (base, m/n stride, k stride) per slot this warp touches: fragment
+      // fm lies in relative slot fm / FPS at row (fm % FPS) * 8 inside it.
+      constexpr int APS = Cfg::WTM >= TS ? Cfg::WTM / TS : 1;  // A slots per warp
+      constexpr int BPS = Cfg::WTN >= TS ? Cfg::WTN / TS : 1;  // B slots per warp
+      constexpr int FPA = Cfg::FM / APS, FPB = Cfg::FN / BPS;  // fragments per slot
+      int abase[APS], amst[APS], akst[APS], bbase[BPS], bnst[BPS], bkst[BPS];
+#pragma unroll
+      for (int j = 0; j < APS; ++j) {
+        const int m = warp_m0 + j * TS;
+        const int slot = m / TS, r = m % TS + (lane >> 2);
+        const int tr = fl[slot];
+        amst[j] = tr ? SLD : 1;
+        akst[j] = tr ? 1 : SLD;
+        abase[j] = slot * SLOT_DOUBLES + r * amst[j] + (lane & 3) * akst[j];
+      }
+#pragma unroll
+      for (int j = 0; j < BPS; ++j) {
+        const int c0 = warp_n0 + j * TS;
+        const int slot = c0 / TS, c = c0 % TS + (lane >> 2);
+        const int tr = fl[Cfg::MT + slot];
+        bnst[j] = tr ? 1 : SLD;
+        bkst[j] = tr ? SLD : 1;
+        bbase[j] = (Cfg::MT + slot) * SLOT_DOUBLES + c * bnst[j] + (lane & 3) * bkst[j];
+      }
+      const int kk_lim = (kvalid(kt) + 3) / 4;
+      if (kk_lim == TS / 4 && fm_lim == Cfg::FM && fn_lim == Cfg::FN) {
+        // Common case: straight-line code, so the compiler can load the
+        // fragments of step kk+1 while the DMMAs of step kk issue.
+#pragma unroll
+        for (int kk = 0; kk < TS / 4; ++kk) {
+          double af[Cfg::FM], bf[Cfg::FN];
+#pragma unroll
+          for (int fm = 0; fm < Cfg::FM; ++fm) {
+            const int j = fm / FPA, i = fm % FPA;
+            af[fm] = sbase[abase[j] + (i * 8) * amst[j] + (kk * 4) * akst[j]];
+          }
+#pragma unroll
+          for (int fn = 0; fn < Cfg::FN; ++fn) {
+            const int j = fn / FPB, i = fn % FPB;
+            bf[fn] = sbase[bbase[j] + (i * 8) * bnst[j] + (kk * 4) * bkst[j]];
+          }
+#pragma unroll
+          for (int fm = 0; fm < Cfg::FM; ++fm)
+#pragma unroll
+            for (int fn = 0; fn < Cfg::FN; ++fn) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], af[fm], bf[fn]);
+        }
+      } else {
+        // Edge tiles: skip the k4 steps and fragments that only hold padding.
+#pragma unroll 1
+        for (int kk = 0; kk < kk_lim; ++kk) {
+          double af[Cfg::FM], bf[Cfg::FN];
+#pragma unroll
+          for (int fm = 0; fm < Cfg::FM; ++fm) {
+            const int j = fm / FPA, i = fm % FPA;
+            af[fm] = fm < fm_lim ? sbase[abase[j] + (i * 8) * amst[j] + (kk * 4) * akst[j]] : 0.0;
+          }
+#pragma unroll
+          for (int fn = 0; fn < Cfg::FN; ++fn) {
+            const int j = fn / FPB, i = fn % FPB;
+            bf[fn] = fn < fn_lim ? sbase[bbase[j] + (i * 8) * bnst[j] + (kk * 4) * bkst[j]] : 0.0;
+          }
+#pragma unroll
+          for (int fm = 0; fm < Cfg::FM; ++fm)
+#pragma unroll
+            for (int fn = 0; fn < Cfg::FN; ++fn)
+              if (fm < fm_lim && fn < fn_lim) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], af[fm], bf[fn]);
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sm.empty[st]);
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Second staging scheme, selected per CTA shape (Cfg::STAGES < 0 never; the
+// template flag below): every thread copies 16-byte chunks with cp.async into
+// the same padded slots, cp.async groups track the stages, one CTA barrier per
+// k-step protects stage reuse.  No producer warp: all WM*WN warps compute, the
+// extra warp of Cfg::THREADS only helps copying.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <class Cfg, class Sched>
+__device__ __forceinline__ void cpa_issue_stage(const Sched& sc, int kt, double* stage, uint8_t* flags) {
+  // 512 16-byte chunks per slot: chunk = column c (0..31) x row pair r2 (0..15)
+  constexpr int CHUNKS = 512;
+#pragma unroll 1
+  for (int s = 0; s < Cfg::SLOTS; ++s) {
+    const SlotSrc src = (s < Cfg::MT) ? sc.a(kt, s) : sc.b(kt, s - Cfg::MT);
+    if (threadIdx.x == 0) flags[s] = (uint8_t)src.trans;
+    const double* base = src.ptr ? src.ptr : g_zero_tile;
+    const int64_t ld = src.ptr ? src.ld : TS;
+    double* dst = stage + s * SLOT_DOUBLES;
+    for (int ch = threadIdx.x; ch < CHUNKS; ch += Cfg::THREADS) {
+      const int c = ch >> 4, r = (ch & 15) * 2;
+      cp_async16(dst + c * SLD + r, base + (int64_t)c * ld + r);
+    }
+  }
+}
+
+template <class Cfg, class Sched, class KValid>
+__device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktiles, void* smem_base,
+                                                      double (&acc)[Cfg::FM][Cfg::FN][2], int mvalid, int nvalid,
+                                                      const KValid& kvalid) {
+  DmmaSmem<Cfg> sm(smem_base);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < Cfg::FM; ++i)
+#pragma unroll
+    for (int j = 0; j < Cfg::FN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  constexpr int S = Cfg::STAGES;
+#pragma unroll
+  for (int s = 0; s < S - 1; ++s) {
+    if (s < ktiles) cpa_issue_stage<Cfg>(sc, s, sm.slots + s * Cfg::STAGE_DOUBLES, sm.flags + s * Cfg::SLOTS);
+    cp_async_commit();
+  }
+  const bool compute = warp < Cfg::CWARPS;
+  const int warp_m0 = (warp / Cfg::WN) * Cfg::WTM;
+  const int warp_n0 = (warp % Cfg::WN) * Cfg::WTN;
+  const int fm_lim = compute ? max(0, min(Cfg::FM, (mvalid - warp_m0 + 7) / 8)) : 0;
+  const int fn_lim = compute ? max(0, min(Cfg::FN, (nvalid - warp_n0 + 7) / 8)) : 0;
+  const bool idle = fm_lim == 0 || fn_lim == 0;
+  constexpr int APS = Cfg::WTM >= TS ? Cfg::WTM / TS : 1;
+  constexpr int BPS = Cfg::WTN >= TS ? Cfg::WTN / TS : 1;
+  constexpr int FPA = Cfg::FM / APS, FPB = Cfg::FN / BPS;
+  for (int kt = 0; kt < ktiles; ++kt) {
+    cp_async_wait<S - 2>();
+    __syncthreads();  // stage kt landed for everyone; stage kt-1 is free
+    {
+      const int nk = kt + S - 1;
+      const int ns = nk % S;
+      if (nk < ktiles) cpa_issue_stage<Cfg>(sc, nk, sm.slots + ns * Cfg::STAGE_DOUBLES, sm.flags + ns * Cfg::SLOTS);
+      cp_async_commit();
+    }
+    if (idle) continue;
+    const int st = kt % S;
+    const double* sbase = sm.slots + st * Cfg::STAGE_DOUBLES;
+    const uint8_t* fl = sm.flags + st * Cfg::SLOTS;
+    int abase[APS], amst[APS], akst[APS], bbase[BPS], bnst[BPS], bkst[BPS];
+#pragma unroll
+    for (int j = 0; j < APS; ++j) {
+      const int m = warp_m0 + j * TS;
+      const int slot = m / TS, r = m % TS + (lane >> 2);
+      const int tr = fl[slot];
+      amst[j] = tr ? SLD : 1;
+      akst[j] = tr ? 1 : SLD;
+      abase[j] = slot * SLOT_DOUBLES + r * amst[j] + (lane & 3) * akst[j];
+    }
+#pragma unroll
+    for (int j = 0; j < BPS; ++j) {
+      const int c0 = warp_n0 + j * TS;
+      const int slot = c0 / TS, c = c0 % TS + (lane >> 2);
+      const int tr = fl[Cfg::MT + slot];
+      bnst[j] = tr ? 1 : SLD;
+      bkst[j] = tr ? SLD : 1;
+      bbase[j] = (Cfg::MT + slot) * SLOT_DOUBLES + c * bnst[j] + (lane & 3) * bkst[j];
+    }
+    const int kk_lim = (kvalid(kt) + 3) / 4;
+    if (kk_lim == TS / 4 && fm_lim == Cfg::FM && fn_lim == Cfg::FN) {
+#pragma unroll
+      for (int kk = 0; kk < TS / 4; ++kk) {
+        double af[Cfg::FM], bf[Cfg::FN];
+#pragma unroll
+        for (int fm = 0; fm < Cfg::FM; ++fm) {
+          const int j = fm / FPA, i = fm % FPA;
+          af[fm] = sbase[abase[j] + (i * 8) * amst[j] + (kk * 4) * akst[j]];
+        }
+#pragma unroll
+        for (int fn = 0; fn < Cfg::FN; ++fn) {
+          const int j = fn / FPB, i = fn % FPB;
+          bf[fn] = sbase[bbase[j] + (i * 8) * bnst[j] + (kk * 4) * bkst[j]];
+        }
+#pragma unroll
+        for (int fm = 0; fm < Cfg::FM; ++fm)
+#pragma unroll
+          for (int fn = 0; fn < Cfg::FN; ++fn) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], af[fm], bf[fn]);
+      }
+    } else {
+#pragma unroll 1
+      for (int kk = 0; kk < kk_lim; ++kk) {
+        double af[Cfg::FM], bf[Cfg::FN];
+#pragma unroll
+        for (int fm = 0; fm < Cfg::FM; ++fm) {
+          const int j = fm / FPA, i = fm % FPA;
+          af[fm] = fm < fm_lim ? sbase[abase[j] + (i * 8) * amst[j] + (kk * 4) * akst[j]] : 0.0;
+        }
+#pragma unroll
+        for (int fn = 0; fn < Cfg::FN; ++fn) {
+          const int j = fn / FPB, i = fn % FPB;
+          bf[fn] = fn < fn_lim ? sbase[bbase[j] + (i * 8) * bnst[j] + (kk * 4) * bkst[j]] : 0.0;
+        }
+#pragma unroll
+        for (int fm = 0; fm < Cfg::FM; ++fm)
+#pragma unroll
+          for (int fn = 0; fn < Cfg::FN; ++fn)
+            if (fm < fm_lim && fn < fn_lim) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], af[fm], bf[fn]);
+      }
+    }
+  }
+  cp_async_wait<0>();
+  return compute;
+}
+
+// Whole CTA: set up the barriers, split into producer and consumers.  Only
+// consumer threads return true (and hold results); the producer returns false.
+// Cfg::CPASYNC selects the cp.async staging above instead.
+template <class Cfg, class Sched, class KValid = DefaultKValid>
+__device__ __forceinline__ bool dmma_mainloop(const Sched& sc, int ktiles, void* smem_base,
+                                              double (&acc)[Cfg::FM][Cfg::FN][2], int* err, int mvalid = 1 << 30,
+                                              int nvalid = 1 << 30, const KValid& kvalid = KValid()) {
+  if constexpr (Cfg::CPASYNC) {
+    (void)err;
+    return dmma_mainloop_cpasync<Cfg>(sc, ktiles, smem_base, acc, mvalid, nvalid, kvalid);
+  }
+  DmmaSmem<Cfg> sm(smem_base);
+  const int warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < Cfg::FM; ++i)
+#pragma unroll
+    for (int j = 0; j < Cfg::FN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < Cfg::STAGES; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], Cfg::CWARPS);
+    }
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (warp == Cfg::CWARPS) {
+    dmma_produce<Cfg>(sc, ktiles, sm, err);
+    return false;
+  }
+  return dmma_consume<Cfg>(ktiles, sm, acc, mvalid, nvalid, kvalid, err);
+}
+
+// Visits every accumulator element of this consumer thread with its CTA-local (m, n).
 template <class Cfg, class F>
 __device__ __forceinline__ void dmma_for_each(const double (&acc)[Cfg::FM][Cfg::FN][2], F&& f) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

@@ -13,6 +13,8 @@ struct Geom {
   int64_t ntp = 0;    // nt (nt + 1) / 2
   int64_t ldB = 0;    // ntp * 1024 doubles per aux row
   int64_t npair = 0;  // n (n + 1) / 2
+  int ht_cfg = 1;     // CTA shape of the half-transform (0..3)
+  int rk_cfg = 1;     // CTA shape of the rank / dm updates (0..3)
 };
 Geom make_geom(int64_t n, int64_t naux);
 
@@ -54,8 +56,10 @@ void launch_pad_square(const double* src, int64_t n, int64_t ldsrc, int64_t ldc,
 
 // X[p] = B_{p0+p} * W for p in [0, np): W is ldw x ncol (ncol multiple of 64),
 // X[p] is ldx x ncol column-major with ldx = round_up(n, 128), stride sxp.
+// Columns at or beyond ncol_valid of W are zero and their fragments are skipped.
 void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
-                           int64_t ncol, double* X, int64_t ldx, int64_t sxp, int* err, cudaStream_t st);
+                           int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, int64_t sxp, int* err,
+                           cudaStream_t st);
 // Kpart[split][q] (128x128 blocks q over block pairs) = sum over p in split,
 // columns [c0, c0+ncol) of X:  X_p X_p^T.  full = 0: pairs Ib<=Jb; 1: all pairs.
 int k_rank_splits(const Geom& g, int64_t np, int full);

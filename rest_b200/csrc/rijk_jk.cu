@@ -360,7 +360,11 @@ void launch_pad_square(const double* src, int64_t n, int64_t ldsrc, int64_t ldc,
 }
 
 // ---- half-transform: X_p = B_p W ------------------------------------------
-using HtCfg = DmmaCfg<2, 2, 2, 2, 3>;  // 64 x 64 CTA tile, 4 warps of 32 x 32
+// CTA shapes (selected per context; rows x cols, compute warps, stages, staging):
+using HtCfg0 = DmmaCfg<2, 2, 2, 2, 3, true>;  // 64 x 64, 4 warps of 32 x 32, cp.async, 3 stages (2 CTAs/SM)
+using HtCfg1 = DmmaCfg<2, 2, 2, 2, 2, true>;  // 64 x 64, cp.async, 2 stages (3 CTAs/SM)
+using HtCfg2 = DmmaCfg<2, 2, 2, 2, 4, true>;  // 64 x 64, cp.async, 4 stages (1 CTA/SM)
+using HtCfg3 = DmmaCfg<2, 2, 2, 2, 3>;        // 64 x 64, bulk copies + producer warp, 3 stages
 
 struct HalfTransformSched {
   const double* Bp;  // row P of the tile-packed tensor
@@ -378,41 +382,74 @@ struct HalfTransformSched {
   }
 };
 
+// Only the rows of the last k tile below n can be non-zero.
+struct LastTileK {
+  int last, lastk;
+  __device__ int operator()(int kt) const { return kt == last ? lastk : TS; }
+};
+
+// Grid: blockIdx.x = cb + ncb * (rb + nrb * p), so that the column blocks of
+// one row block run back to back and share its B tiles in L2.
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::THREADS) k_half_transform(const double* __restrict__ B, int64_t ldB, int64_t p0,
-                                                                 int nrb, const double* __restrict__ W, int64_t ldw,
-                                                                 int nt, double* __restrict__ X, int64_t ldx,
-                                                                 int64_t sxp, int* err) {
+__global__ void __launch_bounds__(Cfg::THREADS, 1) k_half_transform(const double* __restrict__ B, int64_t ldB, int64_t p0,
+                                                                 int nrb, int ncb, const double* __restrict__ W,
+                                                                 int64_t ldw, int n, int nt, int ncol_valid,
+                                                                 double* __restrict__ X, int64_t ldx, int64_t sxp,
+                                                                 int* err) {
   extern __shared__ __align__(128) double smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_DOUBLES);
-  const int64_t rb = blockIdx.x;
-  const int64_t pl = rb / nrb;
-  const int I0 = (int)(rb % nrb) * Cfg::MT;
-  const int col0 = blockIdx.y * Cfg::BN;
+  const int64_t bid = blockIdx.x;
+  const int cb = (int)(bid % ncb);
+  const int64_t rest = bid / ncb;
+  const int64_t pl = rest / nrb;
+  const int I0 = (int)(rest % nrb) * Cfg::MT;
+  const int col0 = cb * Cfg::BN;
   HalfTransformSched sc{B + (p0 + pl) * ldB, W, ldw, nt, I0, col0};
   double acc[Cfg::FM][Cfg::FN][2];
-  if (!dmma_mainloop<Cfg>(sc, nt, smem, bars, acc, err)) return;
+  // Row blocks entirely below n hold zeros only: skip their k-loop.
+  const int ktiles = I0 < nt ? nt : 0;
+  const LastTileK kv{nt - 1, n - (nt - 1) * TS};
+  if (!dmma_mainloop<Cfg>(sc, ktiles, smem, acc, err, n - I0 * TS, ncol_valid - col0, kv)) return;
   double* Xp = X + pl * sxp + (int64_t)I0 * TS + (int64_t)col0 * ldx;
-  dmma_for_each<Cfg>(acc, [&](int m, int n, double v0, double v1) {
-    Xp[m + (int64_t)n * ldx] = v0;
-    Xp[m + (int64_t)(n + 1) * ldx] = v1;
+  dmma_for_each<Cfg>(acc, [&](int m, int c, double v0, double v1) {
+    Xp[m + (int64_t)c * ldx] = v0;
+    Xp[m + (int64_t)(c + 1) * ldx] = v1;
   });
 }
 
-void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
-                           int64_t ncol, double* X, int64_t ldx, int64_t sxp, int* err, cudaStream_t st) {
-  using Cfg = HtCfg;
+template <class Cfg>
+static void half_transform_cfg(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
+                               int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, int64_t sxp, int* err,
+                               cudaStream_t st) {
   cudaFuncSetAttribute(k_half_transform<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
   const int nrb = (int)(ldx / Cfg::BM);
-  dim3 grid((unsigned)(np * nrb), (unsigned)(ncol / Cfg::BN));
+  const int ncb = (int)(ncol / Cfg::BN);
   count_launch();
-  k_half_transform<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(B, g.ldB, p0, nrb, W, ldw, (int)g.nt, X, ldx,
-                                                                      sxp, err);
+  k_half_transform<Cfg><<<(unsigned)(np * nrb * ncb), Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(
+      B, g.ldB, p0, nrb, ncb, W, ldw, (int)g.n, (int)g.nt, (int)ncol_valid, X, ldx, sxp, err);
+}
+
+void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
+                           int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, int64_t sxp, int* err,
+                           cudaStream_t st) {
+  switch (g.ht_cfg) {
+    case 1: return half_transform_cfg<HtCfg1>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
+    case 2: return half_transform_cfg<HtCfg2>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
+    case 3: return half_transform_cfg<HtCfg3>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
+    default: return half_transform_cfg<HtCfg0>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
+  }
 }
 
 // ---- rank update: Kpart = sum_p X_p X_p^T ------------------------------------
-using RkCfg = DmmaCfg<4, 4, 2, 4, 3>;  // 128 x 128 CTA tile, 8 warps of 64 x 32
-constexpr int KB = RkCfg::BM;          // K block edge (128)
+// K is accumulated in 128 x 128 blocks; a CTA computes one (BM x BN) sub-block
+// of one block.  CTA shapes (selected per context):
+using RkCfg0 = DmmaCfg<2, 2, 2, 2, 3, true>;  // 64 x 64, 4 warps of 32 x 32, cp.async, 3 stages (2 CTAs/SM)
+using RkCfg1 = DmmaCfg<2, 2, 2, 2, 2, true>;  // 64 x 64, cp.async, 2 stages (3 CTAs/SM)
+using RkCfg2 = DmmaCfg<2, 2, 2, 2, 4, true>;  // 64 x 64, cp.async, 4 stages (1 CTA/SM)
+using RkCfg3 = DmmaCfg<2, 2, 2, 2, 3>;        // 64 x 64, bulk copies + producer warp, 3 stages
+constexpr int KB = 128;                       // K block edge
+
+static int rk_subs(int) { return 4; }
+static int rk_ctas_per_sm(int cfg) { return cfg == 1 ? 3 : cfg == 2 ? 1 : 2; }
 
 int64_t k_block_pairs(const Geom& g, int full) {
   const int64_t nkb = cdiv(g.n, KB);
@@ -430,10 +467,27 @@ __device__ __forceinline__ void block_pair(int64_t q, int full, int64_t nkb, int
 }
 
 int k_rank_splits(const Geom& g, int64_t np, int full) {
-  const int64_t pairs = k_block_pairs(g, full);
-  int64_t s = cdiv(2 * 148, pairs);
+  const int64_t ctas = k_block_pairs(g, full) * rk_subs(g.rk_cfg);
+  int64_t s = cdiv(2 * 148 * rk_ctas_per_sm(g.rk_cfg), ctas);
   s = std::max<int64_t>(1, std::min<int64_t>(s, np));
   return (int)s;
+}
+
+// Sub-block (hm, hn) of block pair q for CTA tile BM x BN; false when the
+// sub-block lies strictly below the diagonal of a diagonal block (never read).
+template <class Cfg>
+__device__ __forceinline__ bool sub_block(int64_t bq, int full, int64_t nkb, int64_t& q, int64_t& row0,
+                                          int64_t& col0, int64_t& off) {
+  constexpr int SM = KB / Cfg::BM, SN = KB / Cfg::BN;
+  q = bq / (SM * SN);
+  const int sub = (int)(bq % (SM * SN));
+  const int hm = sub % SM, hn = sub / SM;
+  int64_t Ib, Jb;
+  block_pair(q, full, nkb, Ib, Jb);
+  row0 = Ib * KB + hm * Cfg::BM;
+  col0 = Jb * KB + hn * Cfg::BN;
+  off = hm * Cfg::BM + (int64_t)KB * (hn * Cfg::BN);
+  return full || Ib != Jb || hm * Cfg::BM < (hn + 1) * Cfg::BN;
 }
 
 struct RankSched {
@@ -454,41 +508,58 @@ struct RankSched {
   }
 };
 
+// Valid occupied columns of the last column tile of every P.
+struct RankK {
+  int ctiles, lastk;
+  __device__ int operator()(int kt) const { return (kt % ctiles) == ctiles - 1 ? lastk : TS; }
+};
+
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::THREADS) k_rank_update(const double* __restrict__ X, int64_t ldx, int64_t sxp,
-                                                              int64_t np, int c0t, int ctiles, int splits, int full,
-                                                              int64_t nkb, int64_t pairs, double* __restrict__ Kpart,
-                                                              int* err) {
+__global__ void __launch_bounds__(Cfg::THREADS, 1) k_rank_update(const double* __restrict__ X, int64_t ldx, int64_t sxp,
+                                                              int64_t np, int c0t, int ctiles, int lastk, int n,
+                                                              int splits, int full, int64_t nkb, int64_t pairs,
+                                                              double* __restrict__ Kpart, int* err) {
   extern __shared__ __align__(128) double smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_DOUBLES);
-  const int64_t q = blockIdx.x;
   const int sp = blockIdx.y;
-  int64_t Ib, Jb;
-  block_pair(q, full, nkb, Ib, Jb);
+  int64_t q, row0, col0, off;
+  if (!sub_block<Cfg>(blockIdx.x, full, nkb, q, row0, col0, off)) return;
   const int64_t pa = np * sp / splits, pb = np * (sp + 1) / splits;
-  RankSched sc{X, ldx, sxp, pa, ctiles, c0t, Ib * Cfg::BM, Jb * Cfg::BN};
+  RankSched sc{X, ldx, sxp, pa, ctiles, c0t, row0, col0};
   double acc[Cfg::FM][Cfg::FN][2];
   const int ktiles = (int)((pb - pa) * ctiles);
-  if (!dmma_mainloop<Cfg>(sc, ktiles, smem, bars, acc, err)) return;
-  double* out = Kpart + ((int64_t)sp * pairs + q) * (Cfg::BM * Cfg::BN);
-  dmma_for_each<Cfg>(acc, [&](int m, int n, double v0, double v1) {
-    out[m + Cfg::BM * n] = v0;
-    out[m + Cfg::BM * (n + 1)] = v1;
+  if (!dmma_mainloop<Cfg>(sc, ktiles, smem, acc, err, n - (int)row0, n - (int)col0, RankK{ctiles, lastk}))
+    return;
+  double* out = Kpart + ((int64_t)sp * pairs + q) * (KB * KB) + off;
+  dmma_for_each<Cfg>(acc, [&](int m, int c, double v0, double v1) {
+    out[m + KB * c] = v0;
+    out[m + KB * (c + 1)] = v1;
   });
 }
 
-void launch_k_rank_update(const Geom& g, const double* X, int64_t ldx, int64_t sxp, int64_t np, int64_t c0,
-                          int64_t ncol, int splits, int full, double* Kpart, int* err, cudaStream_t st) {
-  using Cfg = RkCfg;
+template <class Cfg>
+static void rank_update_cfg(const Geom& g, const double* X, int64_t ldx, int64_t sxp, int64_t np, int64_t c0,
+                            int64_t ncol, int splits, int full, double* Kpart, int* err, cudaStream_t st) {
   cudaFuncSetAttribute(k_rank_update<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
   const int64_t nkb = cdiv(g.n, KB);
   const int64_t pairs = k_block_pairs(g, full);
   const int c0t = (int)(c0 / TS);
   const int ctiles = (int)cdiv(ncol, TS);
-  dim3 grid((unsigned)pairs, (unsigned)splits);
+  const int lastk = (int)(ncol - (ctiles - 1) * TS);
+  constexpr int subs = (KB / Cfg::BM) * (KB / Cfg::BN);
+  dim3 grid((unsigned)(pairs * subs), (unsigned)splits);
   count_launch();
-  k_rank_update<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(X, ldx, sxp, np, c0t, ctiles, splits, full, nkb,
-                                                                   pairs, Kpart, err);
+  k_rank_update<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(X, ldx, sxp, np, c0t, ctiles, lastk, (int)g.n,
+                                                                   splits, full, nkb, pairs, Kpart, err);
+}
+
+void launch_k_rank_update(const Geom& g, const double* X, int64_t ldx, int64_t sxp, int64_t np, int64_t c0,
+                          int64_t ncol, int splits, int full, double* Kpart, int* err, cudaStream_t st) {
+  switch (g.rk_cfg) {
+    case 1: return rank_update_cfg<RkCfg1>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
+    case 2: return rank_update_cfg<RkCfg2>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
+    case 3: return rank_update_cfg<RkCfg3>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
+    default: return rank_update_cfg<RkCfg0>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
+  }
 }
 
 // ---- dm form: Kpart = sum_p T_p B_p ------------------------------------------
@@ -519,38 +590,49 @@ struct KdmSched {
 };
 
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::THREADS) k_dm_update(const double* __restrict__ T, int64_t ldt, int64_t stp,
+__global__ void __launch_bounds__(Cfg::THREADS, 1) k_dm_update(const double* __restrict__ T, int64_t ldt, int64_t stp,
                                                             const double* __restrict__ B, int64_t ldB, int64_t pg0,
-                                                            int64_t np, int nt, int splits, int full, int64_t nkb,
-                                                            int64_t pairs, double* __restrict__ Kpart, int* err) {
+                                                            int64_t np, int n, int nt, int splits, int full,
+                                                            int64_t nkb, int64_t pairs, double* __restrict__ Kpart,
+                                                            int* err) {
   extern __shared__ __align__(128) double smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_DOUBLES);
-  const int64_t q = blockIdx.x;
   const int sp = blockIdx.y;
-  int64_t Ib, Jb;
-  block_pair(q, full, nkb, Ib, Jb);
+  int64_t q, row0, col0, off;
+  if (!sub_block<Cfg>(blockIdx.x, full, nkb, q, row0, col0, off)) return;
   const int64_t pa = np * sp / splits, pb = np * (sp + 1) / splits;
-  KdmSched sc{T, ldt, stp, B, ldB, pg0, pa, nt, Ib * Cfg::BM, (int)(Jb * Cfg::NT)};
+  KdmSched sc{T, ldt, stp, B, ldB, pg0, pa, nt, row0, (int)(col0 / TS)};
   double acc[Cfg::FM][Cfg::FN][2];
   const int ktiles = (int)((pb - pa) * nt);
-  if (!dmma_mainloop<Cfg>(sc, ktiles, smem, bars, acc, err)) return;
-  double* out = Kpart + ((int64_t)sp * pairs + q) * (Cfg::BM * Cfg::BN);
-  dmma_for_each<Cfg>(acc, [&](int m, int n, double v0, double v1) {
-    out[m + Cfg::BM * n] = v0;
-    out[m + Cfg::BM * (n + 1)] = v1;
+  if (!dmma_mainloop<Cfg>(sc, ktiles, smem, acc, err, n - (int)row0, n - (int)col0, RankK{nt, n - (nt - 1) * TS}))
+    return;
+  double* out = Kpart + ((int64_t)sp * pairs + q) * (KB * KB) + off;
+  dmma_for_each<Cfg>(acc, [&](int m, int c, double v0, double v1) {
+    out[m + KB * c] = v0;
+    out[m + KB * (c + 1)] = v1;
   });
+}
+
+template <class Cfg>
+static void dm_update_cfg(const Geom& g, const double* T, int64_t ldt, int64_t stp, const double* B, int64_t p0,
+                          int64_t np, int splits, int full, double* Kpart, int* err, cudaStream_t st) {
+  cudaFuncSetAttribute(k_dm_update<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+  const int64_t nkb = cdiv(g.n, KB);
+  const int64_t pairs = k_block_pairs(g, full);
+  constexpr int subs = (KB / Cfg::BM) * (KB / Cfg::BN);
+  dim3 grid((unsigned)(pairs * subs), (unsigned)splits);
+  count_launch();
+  k_dm_update<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(T, ldt, stp, B, g.ldB, p0, np, (int)g.n, (int)g.nt,
+                                                                 splits, full, nkb, pairs, Kpart, err);
 }
 
 void launch_k_dm_update(const Geom& g, const double* T, int64_t ldt, int64_t stp, const double* B, int64_t p0,
                         int64_t np, int splits, int full, double* Kpart, int* err, cudaStream_t st) {
-  using Cfg = RkCfg;
-  cudaFuncSetAttribute(k_dm_update<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
-  const int64_t nkb = cdiv(g.n, KB);
-  const int64_t pairs = k_block_pairs(g, full);
-  dim3 grid((unsigned)pairs, (unsigned)splits);
-  count_launch();
-  k_dm_update<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(T, ldt, stp, B, g.ldB, p0, np, (int)g.nt, splits,
-                                                                 full, nkb, pairs, Kpart, err);
+  switch (g.rk_cfg) {
+    case 1: return dm_update_cfg<RkCfg1>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
+    case 2: return dm_update_cfg<RkCfg2>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
+    case 3: return dm_update_cfg<RkCfg3>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
+    default: return dm_update_cfg<RkCfg0>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
+  }
 }
 
 __global__ void __launch_bounds__(256) k_k_finalize(int64_t n, int64_t npair, const double* __restrict__ Kpart,

@@ -45,13 +45,12 @@ struct GemmSched {
 };
 
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::THREADS) k_dgemm(int64_t M, int64_t N, int64_t K, double alpha,
+__global__ void __launch_bounds__(Cfg::THREADS, 1) k_dgemm(int64_t M, int64_t N, int64_t K, double alpha,
                                                         const double* A, int64_t lda, int ta, const double* B,
                                                         int64_t ldb, int tb, double beta, double* C, int64_t ldc,
                                                         int klim, int lower_only, int64_t sa, int64_t sb, int64_t sc_,
                                                         int* err) {
   extern __shared__ __align__(128) double smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_DOUBLES);
   const int64_t m0 = (int64_t)blockIdx.x * Cfg::BM, n0 = (int64_t)blockIdx.y * Cfg::BN;
   if (lower_only && n0 >= m0 + Cfg::BM) return;
   A += blockIdx.z * sa;
@@ -66,7 +65,9 @@ __global__ void __launch_bounds__(Cfg::THREADS) k_dgemm(int64_t M, int64_t N, in
   const int ktiles = ke > kb ? ke - kb : 0;
   GemmSched sc{A, lda, ta, B, ldb, tb, m0, n0, kb, M, N};
   double acc[Cfg::FM][Cfg::FN][2];
-  if (!dmma_mainloop<Cfg>(sc, ktiles, smem, bars, acc, err)) return;
+  if (!dmma_mainloop<Cfg>(sc, ktiles, smem, acc, err, (int)std::min<int64_t>(M - m0, 1 << 30),
+                          (int)std::min<int64_t>(N - n0, 1 << 30)))
+    return;
   dmma_for_each<Cfg>(acc, [&](int m, int n, double v0, double v1) {
     const int64_t gm = m0 + m, gn = n0 + n;
     if (gm >= M) return;
@@ -81,8 +82,10 @@ __global__ void __launch_bounds__(Cfg::THREADS) k_dgemm(int64_t M, int64_t N, in
   });
 }
 
-using GemmSmall = DmmaCfg<2, 2, 2, 2, 3>;  // 64 x 64
-using GemmLarge = DmmaCfg<4, 4, 2, 4, 3>;  // 128 x 128
+// 64 x 64 tiles of 4 DMMA warps with cp.async staging: 3 stages when the grid is
+// small (latency), 2 stages / 3 CTAs per SM when it fills the GPU (throughput).
+using GemmSmall = DmmaCfg<2, 2, 2, 2, 3, true>;
+using GemmLarge = DmmaCfg<2, 2, 2, 2, 2, true>;
 
 template <class Cfg>
 static void launch_dgemm_cfg(int64_t M, int64_t N, int64_t K, double alpha, const double* A, int64_t lda, int ta,
@@ -100,8 +103,8 @@ void launch_dgemm(int64_t M, int64_t N, int64_t K, double alpha, const double* A
                   const double* B, int64_t ldb, int tb, double beta, double* C, int64_t ldc, int klim, int lower_only,
                   int batch, int64_t sa, int64_t sb, int64_t sc, int* err, cudaStream_t st) {
   if (M <= 0 || N <= 0 || batch <= 0) return;
-  const int64_t big = cdiv_m(M, 128) * cdiv_m(N, 128) * batch;
-  if (big >= 2 * 148)
+  const int64_t ctas = cdiv_m(M, 64) * cdiv_m(N, 64) * batch;
+  if (ctas >= 3 * 148)
     launch_dgemm_cfg<GemmLarge>(M, N, K, alpha, A, lda, ta, B, ldb, tb, beta, C, ldc, klim, lower_only, batch, sa, sb,
                                 sc, err, st);
   else

@@ -100,6 +100,9 @@ class RIJK:
 
     PROF_CLASSES = ("j_pass1", "j_pass2", "j_other", "k_half", "k_rank", "k_dm", "k_other")
 
+    def set_tiles(self, half_transform_cfg: int, update_cfg: int):
+        self._check(lib().rijk_ctx_set_tiles(self._h, int(half_transform_cfg), int(update_cfg)))
+
     def profile(self, enable: bool = True):
         self._check(lib().rijk_ctx_profile(self._h, int(bool(enable))))
 

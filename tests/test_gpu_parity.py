@@ -270,3 +270,24 @@ def _n1200_body(ctx, n):
     assert float(e) > 0
     ek = 2.0 * torch.dot(d_up, k_occ) - torch.dot(d_up[dg], k_occ[dg])
     assert float(ek) < 0
+
+
+@pytest.mark.parametrize("ht,rk", [(0, 0), (1, 1), (2, 2), (3, 3), (2, 1), (1, 3)])
+def test_every_tile_shape_gives_the_same_k(ctx, ht, rk):
+    n, naux, nocc = 150, 300, 40
+    case = host_case(n, naux, nocc, seed=31)
+    ri3 = O.ri3fn_from_rimatr(case.rimatr, n)
+    ctx.set_rimatr(case.rimatr, n)
+    try:
+        ctx.set_tiles(ht, rk)
+        occ = np.full(nocc, 2.0)
+        k = ctx.vk_upper_with_ri_v([case.c_occ], [nocc - 1], [occ], 1, -0.5)[0]
+        assert _maxdiff(k, O.vk_upper_with_ri_v(ri3, [case.c_occ], [nocc - 1], [occ], 1, -0.5)[0]) <= TOL
+        kd = ctx.vk_upper_with_rimatr_use_dm_only([case.dm], 1, -1.0)[0]
+        assert _maxdiff(kd, O.vk_upper_with_rimatr_use_dm_only(case.rimatr, [case.dm], 1, -1.0)[0]) <= TOL
+        rng = np.random.default_rng(3)
+        d = np.asfortranarray(rng.standard_normal((n, n)) / n)
+        kf = ctx.vk_full_fromdm_with_ri_v([d], 1, 1.0)[0]
+        assert _maxdiff(kf, O.vk_full_fromdm_with_ri_v(ri3, [d], 1, 1.0)[0]) <= TOL
+    finally:
+        ctx.set_tiles(1, 1)
