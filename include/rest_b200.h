@@ -186,6 +186,35 @@ int rijk_vj_upper_noalloc(const double* d_tensor, int64_t row_stride, int64_t nu
                           const double* d_dm, int spin_channel, double scaling_factor, int dm_mode, double* d_vj,
                           void* stream);
 
+/* ---- integrals (host, OpenMP) ----------------------------------------------- */
+/* Contracted Gaussian shells in plain arrays.  Shell s has angular momentum
+ * l[s] (<= 6), nprim[s] primitives at exps/coefs[prim_off[s] ...], and centre
+ * centers[3s..3s+2] in bohr.  coefs multiply unnormalised Cartesian
+ * primitives x^i y^j z^k exp(-a r^2) and carry the caller's normalisation.
+ * Functions are real solid harmonics: c2s[l] is the (2l+1) x (l+1)(l+2)/2
+ * row-major transform for each l (Cartesian components ordered by descending
+ * x power, then descending y power). */
+typedef struct rijk_shells {
+  int64_t nshell;
+  const int32_t* l;
+  const int32_t* nprim;
+  const int64_t* prim_off;
+  const double* exps;
+  const double* coefs;
+  const double* centers;
+} rijk_shells;
+/* Replaces libcint's int1e_ovlp / int1e_kin / int1e_nuc (kind 0 / 1 / 2) as
+ * called by Molecule::int_ij_matrixupper (src/molecule_io/mod.rs:700-812).
+ * out: n x n column-major.  kind 2 sums -Z_A / |r - R_A| over natom atoms. */
+int rijk_int1e(const rijk_shells* bas, const double* const* c2s, int kind, int natom, const double* charges,
+               const double* coords, double* out);
+/* Replaces the cint_2c2e loop of int_ij_aux_columb_rayon (src/molecule_io/mod.rs:1072-1103):
+ * V = (P|Q), naux x naux column-major. */
+int rijk_int2c2e(const rijk_shells* aux, const double* const* c2s, double* out);
+/* Replaces the cint_3c2e loop of prepare_rimatr_for_ri_v_rayon_v02
+ * (src/molecule_io/mod.rs:1611-1660): (mu nu|P) in rimatr layout [npair, naux]. */
+int rijk_int3c2e(const rijk_shells* bas, const rijk_shells* aux, const double* const* c2s, double* out);
+
 /* ---- SCF pieces around the build ------------------------------------------- */
 /* generate_density_matrix (src/scf_io/mod.rs:441-478): D = (C occ) C^T over the
  * first homo+1 columns, per spin; dm: spin_channel x (n x n). */

