@@ -215,6 +215,15 @@ int rijk_int2c2e(const rijk_shells* aux, const double* const* c2s, double* out);
  * (src/molecule_io/mod.rs:1611-1660): (mu nu|P) in rimatr layout [npair, naux]. */
 int rijk_int3c2e(const rijk_shells* bas, const rijk_shells* aux, const double* const* c2s, double* out);
 
+/* ---- MO-basis three-centre tensor -------------------------------------------- */
+/* generate_ri3mo_rayon / ao2mo_rayon (src/scf_io/mod.rs:2331-2359, :3270-3307):
+ * ri3mo[P, a, i] = sum_{mu,nu} C[mu, a] B_P[mu, nu] C[nu, i] for a in
+ * [row_begin, row_end), i in [col_begin, col_end); output per spin is REST's
+ * RIFull[num_auxbas, nrow, ncol] (P fastest), spin after spin.  eigv:
+ * spin_channel x (n x num_state). */
+int rijk_ao2mo(rijk_ctx* ctx, const double* eigv, int64_t num_state, int64_t row_begin, int64_t row_end,
+               int64_t col_begin, int64_t col_end, int spin_channel, double* ri3mo);
+
 /* ---- SCF pieces around the build ------------------------------------------- */
 /* generate_density_matrix (src/scf_io/mod.rs:441-478): D = (C occ) C^T over the
  * first homo+1 columns, per spin; dm: spin_channel x (n x n). */

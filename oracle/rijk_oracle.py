@@ -291,6 +291,25 @@ def fit_rimatr_cholesky(int3c: np.ndarray, v: np.ndarray) -> np.ndarray:
 
 
 # ---------------------------------------------------------------------------
+# MO-basis three-centre tensor
+# ---------------------------------------------------------------------------
+def ao2mo(rimatr, eigv, row_range, col_range):
+    """``ao2mo_rayon`` (scf_io/mod.rs:3270-3307): per P, tmp = sym(B_P) C (dsymm
+    'L','U'), then tmp[:, rows]^T C[:, cols]; stored as RIFull[N, nrow, ncol]."""
+    npair, naux = rimatr.shape
+    n = int(round((np.sqrt(8 * npair + 1) - 1) / 2))
+    ii, jj = upper_pairs(n)
+    c = np.asarray(eigv, dtype=np.float64)
+    out = np.zeros((naux, len(row_range), len(col_range)), order="F")
+    for p in range(naux):
+        bu = np.zeros((n, n))
+        bu[ii, jj] = rimatr[:, p]
+        tmp = _symm_from_upper(bu) @ c
+        out[p] = tmp[:, row_range.start:row_range.stop].T @ c[:, col_range.start:col_range.stop]
+    return out
+
+
+# ---------------------------------------------------------------------------
 # density, energy, Fock assembly
 # ---------------------------------------------------------------------------
 def occupation_integer(num_state: int, num_elec_spin: float, occ_num: float):

@@ -102,6 +102,10 @@ SIGNATURES = {
         [_ctxp, C.c_void_p, C.c_int64, C.c_int64, _i64p, C.c_void_p, C.c_int, C.c_void_p],
     ),
     "rijk_energy_contraction": (C.c_double, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "rijk_ao2mo": (
+        C.c_int,
+        [_ctxp, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_void_p],
+    ),
     "rijk_int1e": (C.c_int, [C.POINTER(RijkShells), C.c_void_p, C.c_int, C.c_int, _dp, _dp, _dp]),
     "rijk_int2c2e": (C.c_int, [C.POINTER(RijkShells), C.c_void_p, _dp]),
     "rijk_int3c2e": (C.c_int, [C.POINTER(RijkShells), C.POINTER(RijkShells), C.c_void_p, _dp]),

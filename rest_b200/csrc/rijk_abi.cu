@@ -38,7 +38,7 @@ struct rijk_ctx {
   size_t dB_bytes = 0;
   int* d_err = nullptr;   // device-side wait timeouts
   int* d_info = nullptr;  // Cholesky failing pivot
-  DevBuf stage, W, w, Jpart, Cw, X, Kpart, din, dout, docc, mV, mLinv, mT, mLinvd, mOut;
+  DevBuf stage, W, w, Jpart, Cw, X, Kpart, din, dout, docc, mV, mLinv, mT, mLinvd, mOut, Cr, Y, Yp;
   size_t scratch_budget = (size_t)4 << 30;
   int ht_cfg = 1, rk_cfg = 1;  // CTA shapes of the K kernels (fastest measured on B200)
   std::string last;
@@ -744,6 +744,60 @@ int rijk_density_matrix(rijk_ctx* ctx, const double* eigv, int64_t num_basis, in
     RIJK_CK(cudaMemcpy2DAsync(dm + s * n * n, n * 8, dout + s * ld * ld, ld * 8, n * 8, n, cudaMemcpyDeviceToHost,
                               ctx->stream));
   return sync_and_check(ctx, ctx->stream);
+}
+
+int rijk_ao2mo(rijk_ctx* ctx, const double* eigv, int64_t num_state, int64_t row_begin, int64_t row_end,
+               int64_t col_begin, int64_t col_end, int spin_channel, double* ri3mo) {
+  RIJK_TRY(need_tensor(ctx));
+  RIJK_TRY(check_spin(ctx, spin_channel));
+  if (!eigv || !ri3mo || num_state <= 0 || row_begin < 0 || row_end <= row_begin || row_end > num_state ||
+      col_begin < 0 || col_end <= col_begin || col_end > num_state)
+    return set_err(ctx, RIJK_ERR_ARG, "bad argument");
+  const Geom& g = ctx->g;
+  cudaStream_t st = ctx->stream;
+  const int64_t n = g.n, nrow = row_end - row_begin, ncol = col_end - col_begin;
+  const int64_t ldx = round_up(n, 128);
+  const int64_t ocols = round_up(ncol, 128);
+  const int64_t nrp = round_up(nrow, 32);
+  const int64_t ldy = round_up(nrow, 2);
+  RIJK_TRY(ensure(ctx, ctx->din, (size_t)n * num_state * 8));
+  RIJK_TRY(ensure(ctx, ctx->Cw, (size_t)ldx * ocols * 8));
+  RIJK_TRY(ensure(ctx, ctx->Cr, (size_t)ldx * nrp * 8));
+  const int64_t per_p = ldx * ocols * 8 + ldy * ncol * 8 * 2;
+  const int64_t pchunk = std::max<int64_t>(1, std::min<int64_t>(g.naux, (int64_t)ctx->scratch_budget / per_p));
+  RIJK_TRY(ensure(ctx, ctx->X, (size_t)pchunk * ldx * ocols * 8));
+  RIJK_TRY(ensure(ctx, ctx->Y, (size_t)pchunk * ldy * ncol * 8));
+  RIJK_TRY(ensure(ctx, ctx->Yp, (size_t)pchunk * nrow * ncol * 8));
+  double* din = static_cast<double*>(ctx->din.p);
+  double* Cc = static_cast<double*>(ctx->Cw.p);
+  double* Cr = static_cast<double*>(ctx->Cr.p);
+  double* X = static_cast<double*>(ctx->X.p);
+  double* Y = static_cast<double*>(ctx->Y.p);
+  double* Yp = static_cast<double*>(ctx->Yp.p);
+  for (int s = 0; s < spin_channel; ++s) {
+    double* out = ri3mo + (size_t)s * g.naux * nrow * ncol;
+    RIJK_CK(cudaMemcpyAsync(din, eigv + (size_t)s * n * num_state, (size_t)n * num_state * 8, cudaMemcpyHostToDevice,
+                            st));
+    rijk::launch_gather_cols(din, n, n, col_begin, ncol, ldx, ocols, Cc, st);
+    rijk::launch_gather_cols(din, n, n, row_begin, nrow, ldx, nrp, Cr, st);
+    for (int64_t p0 = 0; p0 < g.naux; p0 += pchunk) {
+      const int64_t np = std::min(pchunk, g.naux - p0);
+      // X_p = B_p C[:, cols]  (FP64 DMMA half-transform)
+      rijk::launch_half_transform(g, ctx->dB, p0, np, Cc, ldx, ocols, ncol, X, ldx, ldx * ocols, ctx->d_err, st);
+      // Y_p = C[:, rows]^T X_p  (batched over p)
+      for (int64_t b0 = 0; b0 < np; b0 += 65535) {
+        const int64_t nb = std::min<int64_t>(65535, np - b0);
+        rijk::launch_dgemm(nrow, ncol, g.nt * rijk::TS, 1.0, Cr, ldx, 1, X + b0 * ldx * ocols, ldx, 0, 0.0,
+                           Y + b0 * ldy * ncol, ldy, 0, 0, (int)nb, 0, ldx * ocols, ldy * ncol, ctx->d_err, st);
+      }
+      rijk::launch_ri3mo_permute(Y, ldy, ldy * ncol, np, nrow, ncol, Yp, st);
+      RIJK_TRY(after_launch(ctx, "ao2mo"));
+      // chunk rows p0..p0+np of every (a, i) column of REST's RIFull[naux, nrow, ncol]
+      RIJK_CK(cudaMemcpy2DAsync(out + p0, (size_t)g.naux * 8, Yp, (size_t)np * 8, (size_t)np * 8,
+                                (size_t)nrow * ncol, cudaMemcpyDeviceToHost, st));
+    }
+  }
+  return sync_and_check(ctx, st);
 }
 
 double rijk_energy_contraction(const double* a, const double* b, int64_t npair) {

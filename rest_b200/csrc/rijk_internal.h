@@ -73,6 +73,14 @@ int64_t k_block_pairs(const Geom& g, int full);
 void launch_k_finalize(const Geom& g, const double* Kpart, int splits, int full, double scale, int accumulate,
                        int out_kind, double* out, cudaStream_t st);
 
+// --- ri3mo ---------------------------------------------------------------------
+// out (ldo x ncp, zero padded) = C[:, c0 : c0 + nc]
+void launch_gather_cols(const double* C, int64_t n, int64_t ldc_in, int64_t c0, int64_t nc, int64_t ldo, int64_t ncp,
+                        double* out, cudaStream_t st);
+// out[p + np (a + nrow i)] = Y[p * sy + a + ldy i]
+void launch_ri3mo_permute(const double* Y, int64_t ldy, int64_t sy, int64_t np, int64_t nrow, int64_t ncol,
+                          double* out, cudaStream_t st);
+
 // --- dense FP64 GEMM on the DMMA mainloop (metric step) -----------------------
 // C[MxN] = alpha op(A) op(B) + beta C, all column-major, M,N,K multiples of 32,
 // pointers 16-byte aligned, leading dimensions even.  klim: bit 0 = op(A)

@@ -677,3 +677,50 @@ static std::atomic<int64_t> g_launches{0};
 void count_launch(int64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 }  // namespace rijk
+
+// ============================================================================
+// ri3mo (ao2mo_rayon, src/scf_io/mod.rs:3270-3307)
+// ============================================================================
+namespace rijk {
+
+// out (ldo x ncp, zero padded) = C[:, c0 : c0 + nc]  (C column-major, ld = ldc_in)
+__global__ void __launch_bounds__(256) k_gather_cols(const double* __restrict__ C, int64_t n, int64_t ldc_in,
+                                                     int64_t c0, int64_t nc, int64_t ldo, int64_t ncp,
+                                                     double* __restrict__ out) {
+  const int64_t total = ldo * ncp;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e % ldo, c = e / ldo;
+    out[e] = (r < n && c < nc) ? C[r + ldc_in * (c0 + c)] : 0.0;
+  }
+}
+
+void launch_gather_cols(const double* C, int64_t n, int64_t ldc_in, int64_t c0, int64_t nc, int64_t ldo, int64_t ncp,
+                        double* out, cudaStream_t st) {
+  const int64_t total = ldo * ncp;
+  const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), 148 * 16));
+  count_launch();
+  k_gather_cols<<<blocks, 256, 0, st>>>(C, n, ldc_in, c0, nc, ldo, ncp, out);
+}
+
+// ri3mo[p + naux (a + nrow i)] = Y[p][a + ldy i] for the P chunk [p0, p0 + np)
+__global__ void __launch_bounds__(256) k_ri3mo_permute(const double* __restrict__ Y, int64_t ldy, int64_t sy,
+                                                       int64_t np, int64_t nrow, int64_t ncol,
+                                                       double* __restrict__ out) {
+  // out is the chunk buffer [np][nrow * ncol] with p fastest: out[p + np (a + nrow i)]
+  const int64_t total = np * nrow * ncol;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = e % np, ai = e / np;
+    const int64_t a = ai % nrow, i = ai / nrow;
+    out[e] = Y[p * sy + a + ldy * i];
+  }
+}
+
+void launch_ri3mo_permute(const double* Y, int64_t ldy, int64_t sy, int64_t np, int64_t nrow, int64_t ncol,
+                          double* out, cudaStream_t st) {
+  const int64_t total = np * nrow * ncol;
+  const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), 148 * 32));
+  count_launch();
+  k_ri3mo_permute<<<blocks, 256, 0, st>>>(Y, ldy, sy, np, nrow, ncol, out);
+}
+
+}  // namespace rijk

@@ -254,6 +254,21 @@ class RIJK:
         self._check(lib().rijk_vk_upper_dm_dev(self._h, C.c_void_p(d_dm), spin_channel, float(scaling_factor),
                                                C.c_void_p(d_vk), C.c_void_p(stream or None)))
 
+    # -- MO-basis tensor --------------------------------------------------
+    def ao2mo(self, eigv, row_range: range, col_range: range, spin_channel: int = 1):
+        """REST ``generate_ri3mo_rayon`` / ``ao2mo_rayon`` (scf_io/mod.rs:2331, :3270):
+        per spin an RIFull[N, nrow, ncol] array (Fortran order)."""
+        n = self.num_basis
+        num_state = np.asarray(eigv[0]).shape[1]
+        c = _stack_spin(eigv, spin_channel, (n, num_state))
+        nrow, ncol = len(row_range), len(col_range)
+        out = np.empty(spin_channel * self.num_auxbas * nrow * ncol)
+        self._check(lib().rijk_ao2mo(self._h, _ptr(c), num_state, row_range.start, row_range.stop, col_range.start,
+                                     col_range.stop, spin_channel, _ptr(out)))
+        per = self.num_auxbas * nrow * ncol
+        return [out[s * per:(s + 1) * per].reshape(self.num_auxbas, nrow, ncol, order="F")
+                for s in range(spin_channel)]
+
     # -- SCF pieces --------------------------------------------------------
     def density_matrix(self, eigv, homo, occupation, spin_channel: int):
         """REST ``generate_density_matrix`` (scf_io/mod.rs:441): list of n x n D."""

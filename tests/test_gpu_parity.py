@@ -272,6 +272,20 @@ def _n1200_body(ctx, n):
     assert float(ek) < 0
 
 
+@pytest.mark.parametrize("n,naux,rows,cols", [(7, 33, (2, 7), (0, 2)), (37, 150, (6, 37), (0, 6)),
+                                              (130, 300, (20, 130), (3, 20))])
+def test_ao2mo_ri3mo(ctx, n, naux, rows, cols):
+    case = host_case(n, naux, 2, seed=900 + n)
+    rng = np.random.default_rng(n)
+    c = np.asfortranarray(rng.standard_normal((n, n)) / np.sqrt(n))
+    ctx.set_rimatr(case.rimatr, n)
+    got = ctx.ao2mo([c, c[:, ::-1]], range(*rows), range(*cols), spin_channel=2)
+    for s, cs in enumerate([c, np.asfortranarray(c[:, ::-1])]):
+        ref = O.ao2mo(case.rimatr, cs, range(*rows), range(*cols))
+        assert got[s].shape == ref.shape
+        assert _maxdiff(got[s], ref) <= TOL
+
+
 @pytest.mark.parametrize("ht,rk", [(0, 0), (1, 1), (2, 2), (3, 3), (2, 1), (1, 3)])
 def test_every_tile_shape_gives_the_same_k(ctx, ht, rk):
     n, naux, nocc = 150, 300, 40
