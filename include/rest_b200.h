@@ -167,6 +167,23 @@ int rijk_vk_upper_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state
 int rijk_vk_upper_dm_dev(rijk_ctx* ctx, const double* d_dm, int spin_channel, double scaling_factor, double* d_vk,
                          void* stream);
 
+/* ---- split-precision exchange on the 5th-generation tensor cores -------------- */
+/* Same contraction as rijk_vk_upper_occ_dev (REST vk_upper_with_ri_v_sync,
+ * src/scf_io/mod.rs:2758-2834) with every FP64 operand split into two BF16
+ * parts and three tcgen05 products per pair accumulated in FP32 (relative
+ * error about 1e-5 of |K|).  The first call after a tensor change builds BF16
+ * copies of the tensor (4 bytes per element of the full n x n B_P). */
+int rijk_vk_upper_occ_split_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int64_t* homo,
+                                const double* d_occupation, int spin_channel, double scaling_factor, double* d_vk,
+                                void* stream);
+/* Low-rank form: d_vk (+)= scaling_factor * sum_P (B_P V) S (B_P V)^T with
+ * S = +1 on columns [0, npos) and -1 on [npos, ncols) of V (n x ncols,
+ * column-major, leading dimension ld_v even, 16-byte aligned).  With V the
+ * signed square-root factor of a density difference dD = V S V^T this is the
+ * exchange matrix of dD, whose split-precision error shrinks with |dD|. */
+int rijk_vk_upper_lowrank_split_dev(rijk_ctx* ctx, const double* d_V, int64_t ld_v, int64_t ncols, int64_t npos,
+                                    double scaling_factor, int accumulate, double* d_vk, void* stream);
+
 /* ---- J without any device allocation ----------------------------------------- */
 /* No counterpart in REST.  Same result as rijk_vj_upper_dev for callers that
  * cannot let a library call cudaMalloc (their device memory is owned by another

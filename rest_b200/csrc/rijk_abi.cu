@@ -39,6 +39,9 @@ struct rijk_ctx {
   int* d_err = nullptr;   // device-side wait timeouts
   int* d_info = nullptr;  // Cholesky failing pivot
   DevBuf stage, W, w, Jpart, Cw, X, Kpart, din, dout, docc, mV, mLinv, mT, mLinvd, mOut, Cr, Y, Yp;
+  // split-precision (tcgen05) state: BF16 hi/lo copies of the tensor, operands, partials
+  DevBuf tcBhi, tcBlo, tcVhi, tcVlo, tcXhi, tcXlo, tcPart;
+  int64_t tensor_version = 0, tc_version = -1;
   size_t scratch_budget = (size_t)4 << 30;
   int ht_cfg = 1, rk_cfg = 1;  // CTA shapes of the K kernels (fastest measured on B200)
   std::string last;
@@ -189,6 +192,7 @@ int alloc_tensor(rijk_ctx* ctx, int64_t n, int64_t naux) {
   ctx->naux_pad = naux_pad;
   ctx->g.ht_cfg = ctx->ht_cfg;
   ctx->g.rk_cfg = ctx->rk_cfg;
+  ctx->tensor_version++;
   ctx->have = false;
   return RIJK_OK;
 }
@@ -250,6 +254,7 @@ int fit_in_place(rijk_ctx* ctx, const double* dF, int64_t ldf, int tb, int klim)
     rijk::launch_fit_copy_back(out, kc, ctx->dB, g.ldB, k0, np, ctx->stream);
     RIJK_TRY(after_launch(ctx, "fit copy"));
   }
+  ctx->tensor_version++;
   return RIJK_OK;
 }
 
@@ -437,7 +442,9 @@ int rijk_ctx_destroy(rijk_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   DevBuf* bufs[] = {&ctx->stage, &ctx->W,   &ctx->w,    &ctx->Jpart, &ctx->Cw,    &ctx->X,      &ctx->Kpart, &ctx->din,
-                    &ctx->dout,  &ctx->docc, &ctx->mV, &ctx->mLinv, &ctx->mT, &ctx->mLinvd, &ctx->mOut};
+                    &ctx->dout,  &ctx->docc, &ctx->mV, &ctx->mLinv, &ctx->mT, &ctx->mLinvd, &ctx->mOut,
+                    &ctx->Cr,    &ctx->Y,    &ctx->Yp, &ctx->tcBhi, &ctx->tcBlo, &ctx->tcVhi, &ctx->tcVlo,
+                    &ctx->tcXhi, &ctx->tcXlo, &ctx->tcPart};
   for (DevBuf* b : bufs)
     if (b->p) cudaFree(b->p);
   for (auto& r : ctx->prof_pending) {
@@ -541,6 +548,7 @@ int rijk_tensor_load_rows_dev(rijk_ctx* ctx, const double* d_rows, int64_t p0, i
   RIJK_TRY(need_tensor(ctx));
   if (!d_rows || p0 < 0 || np <= 0 || p0 + np > ctx->g.naux || (layout != 0 && layout != 1))
     return set_err(ctx, RIJK_ERR_ARG, "bad row range or layout");
+  ctx->tensor_version++;
   if (layout == 0)
     rijk::launch_pack_rimatr(ctx->g, d_rows, np, ctx->dB + p0 * ctx->g.ldB, pick(ctx, stream));
   else
@@ -744,6 +752,100 @@ int rijk_density_matrix(rijk_ctx* ctx, const double* eigv, int64_t num_basis, in
     RIJK_CK(cudaMemcpy2DAsync(dm + s * n * n, n * 8, dout + s * ld * ld, ld * 8, n * 8, n, cudaMemcpyDeviceToHost,
                               ctx->stream));
   return sync_and_check(ctx, ctx->stream);
+}
+
+// ---- split-precision exchange (tcgen05) ----------------------------------------
+static int tc_prepare(rijk_ctx* ctx, cudaStream_t st) {
+  if (ctx->tc_version == ctx->tensor_version) return RIJK_OK;
+  const Geom& g = ctx->g;
+  const size_t bytes = (size_t)rijk::tc_tensor_elems(g) * 2;
+  RIJK_TRY(ensure(ctx, ctx->tcBhi, bytes));
+  RIJK_TRY(ensure(ctx, ctx->tcBlo, bytes));
+  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(g.naux, 1024));
+  for (int64_t p0 = 0; p0 < g.naux; p0 += chunk)
+    rijk::launch_split_tensor(g, ctx->dB, p0, std::min(chunk, g.naux - p0), ctx->tcBhi.p, ctx->tcBlo.p, st);
+  RIJK_TRY(after_launch(ctx, "split tensor"));
+  ctx->tc_version = ctx->tensor_version;
+  return RIJK_OK;
+}
+
+// out (+)= scale sum_P (B_P V)(S)(B_P V)^T for the columns [c0, c0 + nc) of V, all of sign `sgn`
+static int tc_lowrank_group(rijk_ctx* ctx, const double* d_V, int64_t ldv, int c0, int nc, int sgn, double scale,
+                            int accumulate, double* d_out, cudaStream_t st) {
+  const Geom& g = ctx->g;
+  const rijk::TcGeom t = rijk::make_tc_geom(g, nc);
+  const size_t vbytes = (size_t)t.npad * 64 * t.nkb * 2;
+  RIJK_TRY(ensure(ctx, ctx->tcVhi, vbytes));
+  RIJK_TRY(ensure(ctx, ctx->tcVlo, vbytes));
+  rijk::launch_split_cols(g, t, d_V + (int64_t)c0 * ldv, ldv, nc, ctx->tcVhi.p, ctx->tcVlo.p, st);
+  const int64_t xper = (int64_t)t.nmb * t.nib * t.block_elems * 2;  // bytes per P per plane
+  const int64_t pchunk = std::max<int64_t>(1, std::min<int64_t>(g.naux, (int64_t)ctx->scratch_budget / (2 * xper)));
+  RIJK_TRY(ensure(ctx, ctx->tcXhi, (size_t)pchunk * xper));
+  RIJK_TRY(ensure(ctx, ctx->tcXlo, (size_t)pchunk * xper));
+  const int64_t pairs = (int64_t)t.nmb * (t.nmb + 1) / 2;
+  const int splits_max = rijk::tc_rank_splits(t, pchunk);
+  RIJK_TRY(ensure(ctx, ctx->tcPart, (size_t)splits_max * pairs * 128 * 128 * 4));
+  for (int64_t p0 = 0; p0 < g.naux; p0 += pchunk) {
+    const int64_t np = std::min(pchunk, g.naux - p0);
+    {
+      ProfScope ps(ctx, RIJK_PROF_K_HALF, st);
+      rijk::launch_half_tc(g, t, ctx->tcBhi.p, ctx->tcBlo.p, p0, np, ctx->tcVhi.p, ctx->tcVlo.p, ctx->tcXhi.p,
+                           ctx->tcXlo.p, ctx->d_err, st);
+    }
+    const int splits = rijk::tc_rank_splits(t, np);
+    {
+      ProfScope ps(ctx, RIJK_PROF_K_RANK, st);
+      rijk::launch_rank_tc(g, t, ctx->tcXhi.p, ctx->tcXlo.p, np, sgn > 0 ? t.nib : 0, splits,
+                           static_cast<float*>(ctx->tcPart.p), ctx->d_err, st);
+    }
+    ProfScope ps(ctx, RIJK_PROF_K_OTHER, st);
+    rijk::launch_rank_tc_finalize(g, t, static_cast<float*>(ctx->tcPart.p), splits, scale,
+                                  (accumulate || p0 > 0) ? 1 : 0, d_out, st);
+  }
+  return after_launch(ctx, "split exchange");
+}
+
+int rijk_vk_upper_lowrank_split_dev(rijk_ctx* ctx, const double* d_V, int64_t ld_v, int64_t ncols, int64_t npos,
+                                    double scaling_factor, int accumulate, double* d_vk, void* stream) {
+  RIJK_TRY(need_tensor(ctx));
+  if (!d_V || !d_vk || ncols < 0 || npos < 0 || npos > ncols || ld_v < ctx->g.n || (ld_v & 1) ||
+      (reinterpret_cast<uintptr_t>(d_V) & 15))
+    return set_err(ctx, RIJK_ERR_ARG, "bad argument");
+  cudaStream_t st = pick(ctx, stream);
+  RIJK_TRY(tc_prepare(ctx, st));
+  bool first = !accumulate;
+  if (ncols == 0 && first) RIJK_CK(cudaMemsetAsync(d_vk, 0, (size_t)ctx->g.npair * 8, st));
+  for (int64_t c0 = 0; c0 < ncols;) {
+    const int64_t end = c0 < npos ? npos : ncols;
+    const int nc = (int)std::min<int64_t>(256, end - c0);
+    RIJK_TRY(tc_lowrank_group(ctx, d_V, ld_v, (int)c0, nc, c0 < npos ? 1 : -1, scaling_factor, first ? 0 : 1, d_vk,
+                              st));
+    first = false;
+    c0 += nc;
+  }
+  return RIJK_OK;
+}
+
+int rijk_vk_upper_occ_split_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int64_t* homo,
+                                const double* d_occupation, int spin_channel, double scaling_factor, double* d_vk,
+                                void* stream) {
+  RIJK_TRY(need_tensor(ctx));
+  RIJK_TRY(check_spin(ctx, spin_channel));
+  if (!d_eigv || !homo || !d_occupation || !d_vk || num_state <= 0) return set_err(ctx, RIJK_ERR_ARG, "bad argument");
+  const Geom& g = ctx->g;
+  cudaStream_t st = pick(ctx, stream);
+  const int64_t ldx = round_up(g.n, 128);
+  for (int s = 0; s < spin_channel; ++s) {
+    const int64_t nw[2] = {homo[s] + 1, 0};
+    if (homo[s] < 0 || nw[0] > num_state) return set_err(ctx, RIJK_ERR_ARG, "homo out of range");
+    const int64_t oc = round_up(nw[0], 64);
+    RIJK_TRY(ensure(ctx, ctx->Cw, (size_t)ldx * oc * 8));
+    double* Cw = static_cast<double*>(ctx->Cw.p);
+    rijk::launch_k_prepare_c(g, d_eigv + (size_t)s * g.n * num_state, g.n, 0, d_occupation + (size_t)s * num_state, 0,
+                             nw, 1, ldx, oc, Cw, st);
+    RIJK_TRY(rijk_vk_upper_lowrank_split_dev(ctx, Cw, ldx, nw[0], nw[0], scaling_factor, 0, d_vk + s * g.npair, st));
+  }
+  return RIJK_OK;
 }
 
 int rijk_ao2mo(rijk_ctx* ctx, const double* eigv, int64_t num_state, int64_t row_begin, int64_t row_end,

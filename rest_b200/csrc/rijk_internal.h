@@ -73,6 +73,30 @@ int64_t k_block_pairs(const Geom& g, int full);
 void launch_k_finalize(const Geom& g, const double* Kpart, int splits, int full, double scale, int accumulate,
                        int out_kind, double* out, cudaStream_t st);
 
+// --- split-precision exchange on tcgen05 (rijk_tc.cu) --------------------------
+struct TcGeom {
+  int nmb = 0;   // 128-row blocks of n
+  int nkb = 0;   // 64-wide K blocks of n
+  int npad = 0;  // column count padded to 64 / 128 / 256
+  int nib = 0;   // npad / 64
+  int64_t block_elems = 0;
+};
+TcGeom make_tc_geom(const Geom& g, int ncols);
+// BF16 elements of one plane (hi or lo) of the split tensor
+int64_t tc_tensor_elems(const Geom& g);
+void launch_split_tensor(const Geom& g, const double* B, int64_t p0, int64_t np, void* hi, void* lo, cudaStream_t st);
+void launch_split_cols(const Geom& g, const TcGeom& t, const double* V, int64_t ldv, int ncols, void* hi, void* lo,
+                       cudaStream_t st);
+// X (np x nmb x nib blocks, hi/lo) = B_{p0..p0+np} V
+void launch_half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
+                    const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st);
+int tc_rank_splits(const TcGeom& t, int64_t np);
+// part[split][pair][128x128] = sum_p X_p S X_p^T (S = -1 on blocks >= npos_blocks)
+void launch_rank_tc(const Geom& g, const TcGeom& t, const void* Xhi, const void* Xlo, int64_t np, int npos_blocks,
+                    int splits, float* part, int* err, cudaStream_t st);
+void launch_rank_tc_finalize(const Geom& g, const TcGeom& t, const float* part, int splits, double scale,
+                             int accumulate, double* out, cudaStream_t st);
+
 // --- ri3mo ---------------------------------------------------------------------
 // out (ldo x ncp, zero padded) = C[:, c0 : c0 + nc]
 void launch_gather_cols(const double* C, int64_t n, int64_t ldc_in, int64_t c0, int64_t nc, int64_t ldo, int64_t ncp,

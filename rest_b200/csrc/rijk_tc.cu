@@ -1,0 +1,512 @@
+// Split-precision exchange build on the 5th-generation tensor cores (tcgen05).
+//
+// Every FP64 operand x is carried as two BF16 numbers, hi = bf16(x) and
+// lo = bf16(x - hi), so that x = hi + lo to about 2^-17 relative.  A product
+// a b is formed as a_hi b_hi + a_hi b_lo + a_lo b_hi (three tcgen05.mma of kind
+// f16 accumulating into one FP32 accumulator in tensor memory); the dropped
+// a_lo b_lo term is below 2^-16 relative.  The two contractions of the
+// exchange build in the occupied-orbital form of REST's vk_upper_with_ri_v_sync
+// (src/scf_io/mod.rs:2758-2834),
+//     X_P = B_P V          (half-transform)
+//     K   = sum_P X_P S X_P^T  (rank update, S = diag(+1.. , -1..))
+// run this way; with V the occupied orbitals scaled by sqrt(occ) it is the
+// plain exchange matrix, and with V the signed square-root factor of a
+// density difference it is the exchange matrix of that difference (the
+// incremental builds of the mixed-precision SCF).
+//
+// Operands live in HBM in the canonical K-major layout of tcgen05 without
+// swizzle: 8-row x 16-byte "core matrices" (8 x 8 BF16), core matrix (r8, k8)
+// of a (R x 64) block at byte offset (k8 * R/8 + r8) * 128, row r%8 of it at
+// (r%8) * 16.  The descriptor's stride between core matrices along the rows is
+// then 128 bytes (SBO) and along K is R/8 * 128 bytes (LBO).  Each pipeline
+// stage is a handful of large contiguous bulk copies (TMA engine, no multicast).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "rijk_common.cuh"
+#include "rijk_internal.h"
+
+namespace rijk {
+
+namespace {
+
+constexpr int TC_M = 128;   // rows per UMMA / per operand block
+constexpr int TC_KB = 64;   // K per pipeline stage (4 UMMA k-steps of 16)
+constexpr int BLOCK_ELEMS = TC_M * TC_KB;          // 8192 BF16 = 16 KB
+constexpr uint32_t BLOCK_BYTES = BLOCK_ELEMS * 2;  // 16384
+
+inline int64_t cdiv_t(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// element offset of (r, k) inside an (R x 64) K-major core-matrix block
+__host__ __device__ __forceinline__ int core_off(int r, int k, int R) {
+  return ((k >> 3) * (R >> 3) + (r >> 3)) * 64 + (r & 7) * 8 + (k & 7);
+}
+
+// ---- tcgen05 helpers -------------------------------------------------------
+__device__ __forceinline__ uint64_t smem_desc(const void* p, uint32_t lbo, uint32_t sbo) {
+  const uint64_t a = smem_u32(p);
+  uint64_t d = 0;
+  d |= (a >> 4) & 0x3FFFull;                   // start address
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;  // leading (K-direction) byte offset
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;  // stride (row-direction) byte offset
+  d |= 1ull << 46;                             // descriptor version for tcgen05
+  // base offset 0, lbo mode 0, layout type 0 (no swizzle)
+  return d;
+}
+
+// kind::f16 instruction descriptor: BF16 A and B, FP32 D, both K-major.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool neg_b) {
+  return (1u << 4)                    // D format F32
+         | (1u << 7)                  // A format BF16
+         | (1u << 10)                 // B format BF16
+         | ((neg_b ? 1u : 0u) << 14)  // negate B
+         | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_alloc(uint32_t* dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// 32 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __double2bfloat16(x);
+  lo = __double2bfloat16(x - (double)__bfloat162float(hi));
+}
+
+// ---- layout producers --------------------------------------------------------
+// Bs[P][mb][kb] (hi and lo planes): the full symmetric B_P (n_pad x n_pad, rows
+// mu, K = kappa) from the FP64 tile-packed tensor.
+__global__ void __launch_bounds__(256) k_split_tensor(const double* __restrict__ B, int64_t ldB, int64_t n, int nt,
+                                                      int nmb, int nkb, int64_t p0, int64_t np,
+                                                      __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+  const int64_t per_p = (int64_t)nmb * nkb * BLOCK_ELEMS;
+  const int64_t total = np * per_p;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pl = e / per_p;
+    const int64_t rem = e - pl * per_p;
+    const int64_t blk = rem / BLOCK_ELEMS;
+    const int o = (int)(rem - blk * BLOCK_ELEMS);
+    const int mb = (int)(blk / nkb), kb = (int)(blk % nkb);
+    // invert core_off for R = 128
+    const int within = o & 63, core = o >> 6;
+    const int r = ((core % (TC_M / 8)) << 3) | (within >> 3);
+    const int k = ((core / (TC_M / 8)) << 3) | (within & 7);
+    const int64_t mu = (int64_t)mb * TC_M + r, ka = (int64_t)kb * TC_KB + k;
+    double x = 0.0;
+    if (mu < n && ka < n) {
+      const int64_t I = mu / TS, J = ka / TS;
+      const double* Bp = B + (p0 + pl) * ldB;
+      x = I <= J ? Bp[tile_pair_index(I, J) * TILE_ELEMS + (mu % TS) + TS * (ka % TS)]
+                 : Bp[tile_pair_index(J, I) * TILE_ELEMS + (ka % TS) + TS * (mu % TS)];
+    }
+    __nv_bfloat16 h, l;
+    split_bf16(x, h, l);
+    hi[e] = h;
+    lo[e] = l;
+  }
+  (void)nt;
+}
+
+// Vs[kb] (hi, lo): columns of V (n x ncols, column-major, ld) as the B operand
+// of the half-transform, N = npad rows (columns of V), K = kappa.
+__global__ void __launch_bounds__(256) k_split_cols(const double* __restrict__ V, int64_t ldv, int64_t n,
+                                                    int ncols, int npad, int nkb, __nv_bfloat16* __restrict__ hi,
+                                                    __nv_bfloat16* __restrict__ lo) {
+  const int64_t per_kb = (int64_t)npad * TC_KB;
+  const int64_t total = per_kb * nkb;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int kb = (int)(e / per_kb);
+    const int o = (int)(e - kb * per_kb);
+    const int within = o & 63, core = o >> 6;
+    const int i = ((core % (npad / 8)) << 3) | (within >> 3);
+    const int k = ((core / (npad / 8)) << 3) | (within & 7);
+    const int64_t ka = (int64_t)kb * TC_KB + k;
+    const double x = (i < ncols && ka < n) ? V[ka + ldv * i] : 0.0;
+    __nv_bfloat16 h, l;
+    split_bf16(x, h, l);
+    hi[e] = h;
+    lo[e] = l;
+  }
+}
+
+// ---- half-transform on tcgen05 -------------------------------------------------
+// One CTA per (P, 128-row block).  Warp 0: producer; warp 1 lane 0: MMA
+// issuer; warps 0..3: epilogue.  smem: STAGES x [A_hi | A_lo | V_hi | V_lo].
+template <int NPAD>
+struct HalfTc {
+  static constexpr int STAGES = 2;
+  static constexpr uint32_t V_BYTES = NPAD * TC_KB * 2;
+  static constexpr uint32_t STAGE_BYTES = 2 * BLOCK_BYTES + 2 * V_BYTES;
+  static constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 + 128;
+};
+
+template <int NPAD>
+__global__ void __launch_bounds__(128, 1)
+    k_half_tc(const __nv_bfloat16* __restrict__ Bhi, const __nv_bfloat16* __restrict__ Blo, int nmb, int nkb,
+              const __nv_bfloat16* __restrict__ Vhi, const __nv_bfloat16* __restrict__ Vlo, int nib,
+              __nv_bfloat16* __restrict__ Xhi, __nv_bfloat16* __restrict__ Xlo, int* err) {
+  using C = HalfTc<NPAD>;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
+  uint64_t* empty = full + C::STAGES;
+  uint64_t* accf = empty + C::STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t blk = blockIdx.x;  // = pl * nmb + mb
+  const int64_t pl = blk / nmb;
+  const int mb = (int)(blk % nmb);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accf, 1);
+    mbar_fence_init();
+  }
+  if (warp == 0) tc_alloc(tmem_slot, NPAD);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool ok = true;
+
+  if (warp == 0 && lane == 0) {
+    // producer
+    for (int kb = 0; kb < nkb && ok; ++kb) {
+      const int s = kb % C::STAGES;
+      if (kb >= C::STAGES) ok = mbar_wait_bounded(&empty[s], (uint32_t)(((kb / C::STAGES) - 1) & 1), err);
+      if (!ok) break;
+      uint8_t* st = smem + s * C::STAGE_BYTES;
+      mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
+      const int64_t boff = ((pl * nmb + mb) * (int64_t)nkb + kb) * BLOCK_ELEMS;
+      bulk_g2s(st, Bhi + boff, BLOCK_BYTES, &full[s]);
+      bulk_g2s(st + BLOCK_BYTES, Blo + boff, BLOCK_BYTES, &full[s]);
+      const int64_t voff = (int64_t)kb * NPAD * TC_KB;
+      bulk_g2s(st + 2 * BLOCK_BYTES, Vhi + voff, C::V_BYTES, &full[s]);
+      bulk_g2s(st + 2 * BLOCK_BYTES + C::V_BYTES, Vlo + voff, C::V_BYTES, &full[s]);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    constexpr uint32_t idesc = idesc_bf16(TC_M, NPAD, false);
+    for (int kb = 0; kb < nkb && ok; ++kb) {
+      const int s = kb % C::STAGES;
+      ok = mbar_wait_bounded(&full[s], (uint32_t)((kb / C::STAGES) & 1), err);
+      if (!ok) break;
+      tc_fence_after();
+      const uint8_t* st = smem + s * C::STAGE_BYTES;
+      const uint8_t* ahi = st;
+      const uint8_t* alo = st + BLOCK_BYTES;
+      const uint8_t* vhi = st + 2 * BLOCK_BYTES;
+      const uint8_t* vlo = st + 2 * BLOCK_BYTES + C::V_BYTES;
+#pragma unroll
+      for (int ks = 0; ks < TC_KB / 16; ++ks) {
+        // K step ks covers core-matrix columns 2ks, 2ks+1
+        const uint32_t ak = 2 * ks * (TC_M / 8) * 128, vk = 2 * ks * (NPAD / 8) * 128;
+        const uint64_t dah = smem_desc(ahi + ak, (TC_M / 8) * 128, 128);
+        const uint64_t dal = smem_desc(alo + ak, (TC_M / 8) * 128, 128);
+        const uint64_t dvh = smem_desc(vhi + vk, (NPAD / 8) * 128, 128);
+        const uint64_t dvl = smem_desc(vlo + vk, (NPAD / 8) * 128, 128);
+        const uint32_t acc0 = (kb > 0 || ks > 0) ? 1u : 0u;
+        tc_mma(tmem, dah, dvh, idesc, acc0);
+        tc_mma(tmem, dah, dvl, idesc, 1u);
+        tc_mma(tmem, dal, dvh, idesc, 1u);
+      }
+      tc_commit(&empty[s]);  // stage s is free once these MMAs have read it
+    }
+    tc_commit(accf);
+  }
+  __syncwarp();
+  // epilogue: warps 0..3, one TMEM lane (= row) per thread
+  const bool acc_ok = __syncthreads_and(ok) && mbar_wait_bounded(accf, 0, err);
+  tc_fence_after();
+  if (acc_ok) {
+    const int m = warp * 32 + lane;
+    const int64_t xbase = ((pl * nmb + mb) * (int64_t)nib) * BLOCK_ELEMS;
+#pragma unroll 1
+    for (int c0 = 0; c0 < NPAD; c0 += 32) {
+      float v[32];
+      tc_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      const int ib = c0 / TC_KB;
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {  // 8 columns -> one 16-byte core-matrix row
+        __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) split_bf16((double)v[g * 8 + j], h[j], l[j]);
+        const int k = (c0 % TC_KB) + g * 8;
+        const int64_t off = xbase + (int64_t)ib * BLOCK_ELEMS + core_off(m, k, TC_M);
+        *reinterpret_cast<uint4*>(Xhi + off) = *reinterpret_cast<const uint4*>(h);
+        *reinterpret_cast<uint4*>(Xlo + off) = *reinterpret_cast<const uint4*>(l);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc_dealloc(tmem, NPAD);
+}
+
+// ---- rank update on tcgen05 --------------------------------------------------------
+// CTA per (upper block pair q, P split): K[Ib][Jb] (128 x 128) = sum_p sum_ib
+// X_p[Ib, ib] S X_p[Jb, ib]^T, FP32 in TMEM, written as an FP32 partial.
+struct RankTc {
+  static constexpr int STAGES = 3;
+  static constexpr uint32_t STAGE_BYTES = 4 * BLOCK_BYTES;  // A hi, A lo, B hi, B lo
+  // The whole per-CTA shared memory is reserved (one CTA per SM either way),
+  // so descriptor strides never point outside the allocation.
+  static constexpr size_t SMEM = 232448;
+  static_assert((size_t)STAGES * STAGE_BYTES + 1024 + 128 <= SMEM, "rank stage budget");
+};
+
+__device__ __forceinline__ int64_t tri_root_tc(int64_t t) {
+  int64_t j = (int64_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while (j * (j + 1) / 2 > t) --j;
+  while ((j + 1) * (j + 2) / 2 <= t) ++j;
+  return j;
+}
+
+__global__ void __launch_bounds__(128, 1)
+    k_rank_tc(const __nv_bfloat16* __restrict__ Xhi, const __nv_bfloat16* __restrict__ Xlo, int nmb, int nib,
+              int npos_blocks, int64_t np, int splits, float* __restrict__ part, int* err) {
+  using C = RankTc;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
+  uint64_t* empty = full + C::STAGES;
+  uint64_t* accf = empty + C::STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t q = blockIdx.x;
+  const int sp = blockIdx.y;
+  const int64_t Jb = tri_root_tc(q), Ib = q - Jb * (Jb + 1) / 2;
+  const int64_t pa = np * sp / splits, pb = np * (sp + 1) / splits;
+  const int64_t nsteps = (pb - pa) * nib;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accf, 1);
+    mbar_fence_init();
+  }
+  if (warp == 0) tc_alloc(tmem_slot, 128);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool ok = true;
+
+  if (warp == 0 && lane == 0) {
+    for (int64_t t = 0; t < nsteps && ok; ++t) {
+      const int s = (int)(t % C::STAGES);
+      if (t >= C::STAGES) ok = mbar_wait_bounded(&empty[s], (uint32_t)(((t / C::STAGES) - 1) & 1), err);
+      if (!ok) break;
+      const int64_t p = pa + t / nib;
+      const int ib = (int)(t % nib);
+      uint8_t* st = smem + s * C::STAGE_BYTES;
+      mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
+      const int64_t ao = ((p * nmb + Ib) * (int64_t)nib + ib) * BLOCK_ELEMS;
+      const int64_t bo = ((p * nmb + Jb) * (int64_t)nib + ib) * BLOCK_ELEMS;
+      bulk_g2s(st, Xhi + ao, BLOCK_BYTES, &full[s]);
+      bulk_g2s(st + BLOCK_BYTES, Xlo + ao, BLOCK_BYTES, &full[s]);
+      bulk_g2s(st + 2 * BLOCK_BYTES, Xhi + bo, BLOCK_BYTES, &full[s]);
+      bulk_g2s(st + 3 * BLOCK_BYTES, Xlo + bo, BLOCK_BYTES, &full[s]);
+    }
+  } else if (warp == 1 && lane == 0) {
+    constexpr uint32_t id_pos = idesc_bf16(TC_M, TC_M, false);
+    constexpr uint32_t id_neg = idesc_bf16(TC_M, TC_M, true);
+    for (int64_t t = 0; t < nsteps && ok; ++t) {
+      const int s = (int)(t % C::STAGES);
+      ok = mbar_wait_bounded(&full[s], (uint32_t)((t / C::STAGES) & 1), err);
+      if (!ok) break;
+      tc_fence_after();
+      const int ib = (int)(t % nib);
+      const uint32_t idesc = ib < npos_blocks ? id_pos : id_neg;
+      const uint8_t* st = smem + s * C::STAGE_BYTES;
+#pragma unroll
+      for (int ks = 0; ks < TC_KB / 16; ++ks) {
+        const uint32_t kof = 2 * ks * (TC_M / 8) * 128;
+        const uint64_t dah = smem_desc(st + kof, (TC_M / 8) * 128, 128);
+        const uint64_t dal = smem_desc(st + BLOCK_BYTES + kof, (TC_M / 8) * 128, 128);
+        const uint64_t dbh = smem_desc(st + 2 * BLOCK_BYTES + kof, (TC_M / 8) * 128, 128);
+        const uint64_t dbl = smem_desc(st + 3 * BLOCK_BYTES + kof, (TC_M / 8) * 128, 128);
+        const uint32_t acc0 = (t > 0 || ks > 0) ? 1u : 0u;
+        tc_mma(tmem, dah, dbh, idesc, acc0);
+        tc_mma(tmem, dah, dbl, idesc, 1u);
+        tc_mma(tmem, dal, dbh, idesc, 1u);
+      }
+      tc_commit(&empty[s]);
+    }
+    tc_commit(accf);
+  }
+  __syncwarp();
+  const bool acc_ok = __syncthreads_and(ok) && nsteps > 0 && mbar_wait_bounded(accf, 0, err);
+  tc_fence_after();
+  const int m = warp * 32 + lane;
+  float* out = part + ((int64_t)sp * gridDim.x + q) * (TC_M * TC_M);
+#pragma unroll 1
+  for (int c0 = 0; c0 < TC_M; c0 += 32) {
+    float v[32];
+    if (acc_ok) {
+      tc_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 32; ++i) v[i] = 0.0f;
+    }
+#pragma unroll
+    for (int i = 0; i < 32; ++i) out[m + TC_M * (c0 + i)] = v[i];
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc_dealloc(tmem, 128);
+}
+
+// FP32 partials -> packed upper K (FP64), out (+)= scale * sum_splits.
+__global__ void __launch_bounds__(256) k_rank_tc_finalize(int64_t n, int64_t npair, const float* __restrict__ part,
+                                                          int splits, int64_t pairs, double scale, int accumulate,
+                                                          double* __restrict__ out) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < npair; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = tri_root_tc(e), i = e - j * (j + 1) / 2;
+    const int64_t Ib = i / TC_M, Jb = j / TC_M;
+    const int64_t q = Jb * (Jb + 1) / 2 + Ib;
+    const int64_t off = (i % TC_M) + (int64_t)TC_M * (j % TC_M);
+    double v = 0.0;
+    for (int s = 0; s < splits; ++s) v += (double)part[((int64_t)s * pairs + q) * (TC_M * TC_M) + off];
+    v *= scale;
+    out[e] = accumulate ? out[e] + v : v;
+  }
+}
+
+}  // namespace
+
+// ============================================================================
+// host launchers
+// ============================================================================
+TcGeom make_tc_geom(const Geom& g, int ncols) {
+  TcGeom t;
+  t.nmb = (int)cdiv_t(g.n, TC_M);
+  t.nkb = (int)cdiv_t(g.n, TC_KB);
+  t.npad = ncols <= 64 ? 64 : ncols <= 128 ? 128 : 256;
+  t.nib = t.npad / TC_KB;
+  t.block_elems = BLOCK_ELEMS;
+  return t;
+}
+
+int64_t tc_tensor_elems(const Geom& g) {
+  return g.naux * (int64_t)cdiv_t(g.n, TC_M) * cdiv_t(g.n, TC_KB) * BLOCK_ELEMS;
+}
+
+void launch_split_tensor(const Geom& g, const double* B, int64_t p0, int64_t np, void* hi, void* lo,
+                         cudaStream_t st) {
+  const int nmb = (int)cdiv_t(g.n, TC_M), nkb = (int)cdiv_t(g.n, TC_KB);
+  const int64_t per_p = (int64_t)nmb * nkb * BLOCK_ELEMS;
+  auto* h = static_cast<__nv_bfloat16*>(hi) + p0 * per_p;
+  auto* l = static_cast<__nv_bfloat16*>(lo) + p0 * per_p;
+  const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv_t(np * per_p, 256), 148 * 32));
+  count_launch();
+  k_split_tensor<<<blocks, 256, 0, st>>>(B, g.ldB, g.n, (int)g.nt, nmb, nkb, p0, np, h, l);
+}
+
+void launch_split_cols(const Geom& g, const TcGeom& t, const double* V, int64_t ldv, int ncols, void* hi, void* lo,
+                       cudaStream_t st) {
+  const int64_t total = (int64_t)t.npad * TC_KB * t.nkb;
+  const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv_t(total, 256), 148 * 8));
+  count_launch();
+  k_split_cols<<<blocks, 256, 0, st>>>(V, ldv, g.n, ncols, t.npad, t.nkb, static_cast<__nv_bfloat16*>(hi),
+                                       static_cast<__nv_bfloat16*>(lo));
+}
+
+template <int NPAD>
+static void half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
+                    const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st) {
+  using C = HalfTc<NPAD>;
+  cudaFuncSetAttribute(k_half_tc<NPAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+  const int64_t per_p = (int64_t)t.nmb * t.nkb * BLOCK_ELEMS;
+  count_launch();
+  k_half_tc<NPAD><<<(unsigned)(np * t.nmb), 128, C::SMEM, st>>>(
+      static_cast<const __nv_bfloat16*>(Bhi) + p0 * per_p, static_cast<const __nv_bfloat16*>(Blo) + p0 * per_p,
+      t.nmb, t.nkb, static_cast<const __nv_bfloat16*>(Vhi), static_cast<const __nv_bfloat16*>(Vlo), t.nib,
+      static_cast<__nv_bfloat16*>(Xhi), static_cast<__nv_bfloat16*>(Xlo), err);
+}
+
+void launch_half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
+                    const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st) {
+  if (t.npad == 64)
+    half_tc<64>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
+  else if (t.npad == 128)
+    half_tc<128>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
+  else
+    half_tc<256>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
+}
+
+int tc_rank_splits(const TcGeom& t, int64_t np) {
+  const int64_t pairs = (int64_t)t.nmb * (t.nmb + 1) / 2;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(np, cdiv_t(2 * 148, pairs)));
+}
+
+void launch_rank_tc(const Geom& g, const TcGeom& t, const void* Xhi, const void* Xlo, int64_t np, int npos_blocks,
+                    int splits, float* part, int* err, cudaStream_t st) {
+  const int64_t pairs = (int64_t)t.nmb * (t.nmb + 1) / 2;
+  cudaFuncSetAttribute(k_rank_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RankTc::SMEM);
+  dim3 grid((unsigned)pairs, (unsigned)splits);
+  count_launch();
+  k_rank_tc<<<grid, 128, RankTc::SMEM, st>>>(static_cast<const __nv_bfloat16*>(Xhi),
+                                             static_cast<const __nv_bfloat16*>(Xlo), t.nmb, t.nib, npos_blocks, np,
+                                             splits, part, err);
+  (void)g;
+}
+
+void launch_rank_tc_finalize(const Geom& g, const TcGeom& t, const float* part, int splits, double scale,
+                             int accumulate, double* out, cudaStream_t st) {
+  const int64_t pairs = (int64_t)t.nmb * (t.nmb + 1) / 2;
+  const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv_t(g.npair, 256), 148 * 16));
+  count_launch();
+  k_rank_tc_finalize<<<blocks, 256, 0, st>>>(g.n, g.npair, part, splits, pairs, scale, accumulate, out);
+}
+
+}  // namespace rijk

@@ -269,6 +269,20 @@ class RIJK:
         return [out[s * per:(s + 1) * per].reshape(self.num_auxbas, nrow, ncol, order="F")
                 for s in range(spin_channel)]
 
+    # -- split precision (tcgen05) ------------------------------------------
+    def vk_upper_occ_split_dev(self, d_eigv: int, num_state: int, homo, d_occ: int, spin_channel: int,
+                               scaling_factor: float, d_vk: int, stream: int = 0):
+        hm = (C.c_int64 * 2)(*[int(homo[s]) if s < spin_channel else 0 for s in range(2)])
+        self._check(lib().rijk_vk_upper_occ_split_dev(self._h, C.c_void_p(d_eigv), num_state, hm, C.c_void_p(d_occ),
+                                                      spin_channel, float(scaling_factor), C.c_void_p(d_vk),
+                                                      C.c_void_p(stream or None)))
+
+    def vk_upper_lowrank_split_dev(self, d_v: int, ld_v: int, ncols: int, npos: int, scaling_factor: float,
+                                   accumulate: bool, d_vk: int, stream: int = 0):
+        self._check(lib().rijk_vk_upper_lowrank_split_dev(self._h, C.c_void_p(d_v), ld_v, ncols, npos,
+                                                          float(scaling_factor), int(bool(accumulate)),
+                                                          C.c_void_p(d_vk), C.c_void_p(stream or None)))
+
     # -- SCF pieces --------------------------------------------------------
     def density_matrix(self, eigv, homo, occupation, spin_channel: int):
         """REST ``generate_density_matrix`` (scf_io/mod.rs:441): list of n x n D."""
