@@ -484,9 +484,12 @@ void launch_half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void*
     half_tc<256>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
 }
 
+// Each split accumulates at most ~64 aux rows in FP32 in tensor memory (the
+// splits are then summed in FP64), and there are enough CTAs to fill the GPU.
 int tc_rank_splits(const TcGeom& t, int64_t np) {
   const int64_t pairs = (int64_t)t.nmb * (t.nmb + 1) / 2;
-  return (int)std::max<int64_t>(1, std::min<int64_t>(np, cdiv_t(2 * 148, pairs)));
+  const int64_t s = std::max<int64_t>(cdiv_t(2 * 148, pairs), cdiv_t(np, 64));
+  return (int)std::max<int64_t>(1, std::min<int64_t>(np, s));
 }
 
 void launch_rank_tc(const Geom& g, const TcGeom& t, const void* Xhi, const void* Xlo, int64_t np, int npos_blocks,

@@ -75,6 +75,14 @@ class ScfOptions:
     metric: str = "inv_sqrt"  # inv_sqrt (REST's live path) | cholesky
     start_check_oscillation: int = 20
     print_level: int = 0
+    # precision of the exchange build: "fp64" (plain) or "mixed": incremental
+    # split-precision (3 x BF16 on tcgen05) builds K_k = K_{k-1} + K(D_k - D_{k-1})
+    # until |dE| <= mixed_switch_etot and dDM <= mixed_switch_rho, then full FP64
+    # builds to convergence (the converged energy is an FP64 energy).
+    precision: str = "fp64"
+    mixed_switch_etot: float = 1.0e-5
+    mixed_switch_rho: float = 1.0e-4
+    mixed_rebuild_every: int = 8  # full FP64 rebuild of K every this many split steps
 
 
 @dataclass
@@ -131,6 +139,13 @@ class SCF:
             self.occ_num = 1.0
         self.k_scale = -0.5 if self.spin_channel == 1 else -1.0
         self.h_upper = _upper(self.h_core)
+        # mixed-precision state: reference exchange matrix and the density terms it belongs to
+        self._kref = None
+        self._kref_terms = None
+        self._fp64_now = self.opts.precision != "mixed"
+        self._split_steps = 0
+        self.split_builds = 0
+        self.fp64_builds = 0
 
     # -- pieces of the loop ---------------------------------------------------
     def occupation(self):
@@ -157,18 +172,89 @@ class SCF:
     def density(self, eigv, occ, homo):
         return self.ctx.density_matrix(eigv, homo, occ, self.spin_channel)
 
-    def hamiltonian(self, dm, eigv=None, occ=None, homo=None):
+    # -- mixed precision: exchange of a density difference ---------------------
+    def terms_of(self, eigv, occ, homo):
+        """Factor terms of a density: D_s = sum coef Y Y^T with Y = C[:, :nw] sqrt(occ)."""
+        return [[(1.0, np.asarray(eigv[s])[:, :homo[s] + 1] * np.sqrt(np.asarray(occ[s])[:homo[s] + 1]))]
+                for s in range(self.spin_channel)]
+
+    @staticmethod
+    def mix_terms(t0, t1, alpha):
+        return [[(c * (1.0 - alpha), y) for c, y in a] + [(c * alpha, y) for c, y in b] for a, b in zip(t0, t1)]
+
+    def delta_factor(self, terms_new, terms_ref):
+        """dD = sum_new - sum_ref as V S V^T with V = Q U |lam|^1/2 (thin QR of the
+        stacked factors, eigendecomposition of the small core), positive columns first."""
+        cols, sg = [], []
+        for sign, terms in ((1.0, terms_new), (-1.0, terms_ref)):
+            for c, y in terms:
+                cc = sign * c
+                if cc == 0.0 or y.shape[1] == 0:
+                    continue
+                cols.append(np.sqrt(abs(cc)) * y)
+                sg.append(np.full(y.shape[1], np.sign(cc)))
+        if not cols:
+            return np.zeros((self.n, 0)), 0
+        w = np.hstack(cols)
+        s = np.concatenate(sg)
+        q, r = np.linalg.qr(w)
+        lam, u = np.linalg.eigh((r * s) @ r.T)
+        big = np.max(np.abs(lam)) if lam.size else 0.0
+        keep = np.abs(lam) > 1e-14 * max(big, 1e-300)
+        lam, u = lam[keep], u[:, keep]
+        order = np.argsort(-lam)  # positive eigenvalues first
+        lam, u = lam[order], u[:, order]
+        v = (q @ u) * np.sqrt(np.abs(lam))
+        return v, int(np.sum(lam > 0))
+
+    def k_split_delta(self, terms_new, terms_ref):
+        """K_s(D_new - D_ref) for each spin by the split-precision tcgen05 build."""
+        import torch
+
+        out = []
+        n, ld = self.n, self.n + (self.n & 1)
+        st = self.ctx.stream
+        with torch.cuda.stream(torch.cuda.ExternalStream(st)):
+            for s in range(self.spin_channel):
+                v, npos = self.delta_factor(terms_new[s], terms_ref[s])
+                dk = torch.zeros(self.n * (self.n + 1) // 2, dtype=torch.float64, device="cuda")
+                if v.shape[1] > 0:
+                    buf = np.zeros((v.shape[1], ld))
+                    buf[:, :n] = v.T
+                    dv = torch.tensor(buf, dtype=torch.float64, device="cuda")
+                    self.ctx.vk_upper_lowrank_split_dev(dv.data_ptr(), ld, v.shape[1], npos, self.k_scale, False,
+                                                        dk.data_ptr(), st)
+                self.ctx.synchronize(st)
+                out.append(dk.cpu().numpy())
+        return out
+
+    def hamiltonian(self, dm, eigv=None, occ=None, homo=None, terms=None):
         """generate_hf_hamiltonian_ri_v + the energy of generate_hf_hamiltonian."""
         sc = self.spin_channel
-        if self.opts.use_ri_symm:
+        o = self.opts
+        incremental = (o.precision == "mixed" and terms is not None and getattr(self, "_kref", None) is not None
+                       and not self._fp64_now and self._split_steps < o.mixed_rebuild_every)
+        if o.use_ri_symm:
             vj = self.ctx.vj_upper_with_rimatr_v(dm, sc, 1.0)
-            vk = self.ctx.vk_upper_with_rimatr_use_dm_only(dm, sc, self.k_scale)
         else:
             vj = self.ctx.vj_upper_with_ri_v(dm, sc, 1.0)
-            if self.opts.use_dm_only or eigv is None:
+        if incremental:
+            dk = self.k_split_delta(terms, self._kref_terms)
+            vk = [self._kref[s] + dk[s] for s in range(sc)] + [np.zeros(1)] * (2 - sc)
+            self._split_steps += 1
+            self.split_builds += 1
+        else:
+            if o.use_ri_symm:
+                vk = self.ctx.vk_upper_with_rimatr_use_dm_only(dm, sc, self.k_scale)
+            elif o.use_dm_only or eigv is None:
                 vk = self.ctx.vk_upper_with_ri_v_use_dm_only(dm, sc, self.k_scale)
             else:
                 vk = self.ctx.vk_upper_with_ri_v(eigv, homo, occ, sc, self.k_scale)
+            self._split_steps = 0
+            self.fp64_builds += 1
+        if o.precision == "mixed" and terms is not None:
+            self._kref = [vk[s].copy() for s in range(sc)]
+            self._kref_terms = terms
         fock = []
         for s in range(sc):
             f = self.h_upper.copy()
@@ -198,12 +284,15 @@ class SCF:
         t0 = time.perf_counter()
         n, sc = self.n, self.spin_channel
         dm, eigv, occ, homo = self.initial_density()
-        fock, energy = self.hamiltonian(dm, eigv, occ, homo)
+        terms0 = self.terms_of(eigv, occ, homo)
+        fock, energy = self.hamiltonian(dm, eigv, occ, homo, terms=terms0)
         vals, eigv = self.diagonalize(fock)
         occ, homo = self.occupation()
         dm_new = self.density(eigv, occ, homo)
         # ScfTraceRecord: density_matrix = [previous, current input]
         rec_dm = [dm, dm_new]
+        rec_terms = [terms0, self.terms_of(eigv, occ, homo)]
+        fp64_streak = 0
         rec_energy, rec_vals = energy, vals
         num_iter = 1
         start_diis = o.start_diis_cycle
@@ -214,13 +303,15 @@ class SCF:
         while True:
             # prepare_next_input
             dm_in = rec_dm[1]
+            fp64_before = self.fp64_builds
             if o.mixer == "direct":
-                fock, energy = self.hamiltonian(dm_in, eigv, occ, homo)
+                fock, energy = self.hamiltonian(dm_in, eigv, occ, homo, terms=rec_terms[1])
             elif o.mixer == "linear" or (o.mixer == "diis" and num_iter < start_diis):
                 dm_in = [rec_dm[0][s] + o.mix_param * (rec_dm[1][s] - rec_dm[0][s]) for s in range(sc)]
-                fock, energy = self.hamiltonian(dm_in, eigv, occ, homo)
+                fock, energy = self.hamiltonian(dm_in, eigv, occ, homo,
+                                                terms=self.mix_terms(rec_terms[0], rec_terms[1], o.mix_param))
             else:
-                fock, energy = self.hamiltonian(dm_in, eigv, occ, homo)
+                fock, energy = self.hamiltonian(dm_in, eigv, occ, homo, terms=rec_terms[1])
                 energies.append(energy)
                 osc = len(energies) >= 2 and len(energies) > o.start_check_oscillation and energies[-1] > energies[-2]
                 if len(targets) == o.num_max_diis:
@@ -251,12 +342,15 @@ class SCF:
                     prev_fock = fock
                 except np.linalg.LinAlgError:
                     dm_in = [rec_dm[0][s] + o.mix_param * (rec_dm[1][s] - rec_dm[0][s]) for s in range(sc)]
-                    fock, energy = self.hamiltonian(dm_in, eigv, occ, homo)
+                    fock, energy = self.hamiltonian(dm_in, eigv, occ, homo,
+                                                    terms=self.mix_terms(rec_terms[0], rec_terms[1], o.mix_param))
                     start_diis = num_iter + 8
                     err_vecs, targets = [], []
+            fp64_streak = fp64_streak + 1 if self.fp64_builds > fp64_before else 0
             vals, eigv = self.diagonalize(fock)
             occ, homo = self.occupation()
             dm_new = self.density(eigv, occ, homo)
+            terms_new = self.terms_of(eigv, occ, homo)
             # check_scf_convergence against the record
             de = energy - rec_energy
             eev = float(np.sqrt(sum(np.sum((vals[s] - rec_vals[s]) ** 2) for s in range(sc))))
@@ -266,8 +360,15 @@ class SCF:
                 print(f"Energy: {energy:18.10f} Ha after {num_iter:4d} iterations; "
                       f"dDM {max(ddm):.3e} deev {eev:.3e} dE {de:.3e}")
             conv = num_iter >= 2 and abs(de) <= o.scf_acc_etot and max(ddm) <= o.scf_acc_rho and eev <= o.scf_acc_eev
+            if o.precision == "mixed":
+                # converged only on consecutive full FP64 builds; leave the split
+                # builds once the SCF is loosely converged
+                conv = conv and fp64_streak >= 2
+                if not self._fp64_now and abs(de) <= o.mixed_switch_etot and max(ddm) <= o.mixed_switch_rho:
+                    self._fp64_now = True
             # update
             rec_dm = [rec_dm[1], dm_new]
+            rec_terms = [rec_terms[1], terms_new]
             rec_energy, rec_vals = energy, vals
             num_iter += 1
             if conv:
@@ -276,6 +377,8 @@ class SCF:
             if num_iter > o.max_scf_cycle:
                 break
         self.timings["scf_s"] = time.perf_counter() - t0
+        self.timings["fp64_k_builds"] = self.fp64_builds
+        self.timings["split_k_builds"] = self.split_builds
         return ScfResult(energy, converged, num_iter - 1, vals, eigv, rec_dm[1], self.nuc_energy, n, self.naux,
                          dict(self.timings), history)
 

@@ -55,6 +55,21 @@ def test_pen_energy_matches_rest(ctx):
     assert abs(rc.energy - r.energy) < 2e-8
 
 
+@pytest.mark.parametrize("name,tol", [("water_rihf.json", 1e-9), ("pen_rihf.json", 3e-8)])
+def test_mixed_precision_scf_reaches_the_fp64_energy(ctx, name, tol):
+    """Incremental split-precision (tcgen05) exchange builds, then FP64 builds to
+    convergence: the energy is the FP64 one (water: oracle within 1e-9 Eh;
+    pentacene: REST's published energy within the metric's noise floor)."""
+    g, mol = _golden(name)
+    ref = g.get("oracle_energy", g.get("rest_energy"))
+    opts = ScfOptions(precision="mixed", scf_acc_etot=1e-10, scf_acc_rho=1e-7, scf_acc_eev=1e-7,
+                      max_scf_cycle=150)
+    r = SCF(mol, g["basis"], g["auxbas"], opts, ctx=ctx).run()
+    assert r.converged
+    assert r.timings["split_k_builds"] > 0
+    assert abs(r.energy - ref) < tol
+
+
 def test_uhf_radical_matches_oracle(ctx):
     from oracle.scf_ctx import OracleRIJK
 

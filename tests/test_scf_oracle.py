@@ -96,3 +96,27 @@ def test_pen_rihf_energy_matches_rest():
     assert abs(r.energy - g["rest_energy"]) < 1e-8
     # PySCF uses a different Bohr radius (0.52917721092): its energy differs by ~6e-8
     assert abs(r.energy - g["pyscf_energy"]) < 2e-7
+
+
+def test_density_difference_factor_is_exact():
+    """The signed low-rank factor dD = V S V^T the mixed-precision SCF feeds to
+    the split exchange build reproduces the density difference."""
+    from rest_b200.scf import SCF
+
+    rng = np.random.default_rng(4)
+    n, o = 30, 6
+    c1 = np.linalg.qr(rng.standard_normal((n, n)))[0]
+    c2 = np.linalg.qr(c1 + 0.05 * rng.standard_normal((n, n)))[0]
+    occ = np.zeros(n)
+    occ[:o] = 2.0
+    stub = SCF.__new__(SCF)
+    stub.spin_channel, stub.n = 1, n
+    t1 = stub.terms_of([c1], [occ], [o - 1])
+    t2 = stub.terms_of([c2], [occ], [o - 1])
+    for new, ref in ((t2, t1), (SCF.mix_terms(t1, t2, 0.6), t1)):
+        d_new = sum(c * y @ y.T for c, y in new[0])
+        d_ref = sum(c * y @ y.T for c, y in ref[0])
+        v, npos = stub.delta_factor(new[0], ref[0])
+        s = np.concatenate([np.ones(npos), -np.ones(v.shape[1] - npos)])
+        assert np.max(np.abs((v * s) @ v.T - (d_new - d_ref))) < 1e-12
+        assert v.shape[1] <= 4 * o
