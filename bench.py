@@ -303,6 +303,55 @@ def run_ours(args, w):
         if cls_time.get(k):
             j_rates[k] = w["j_pass_bytes"] / cls_time[k] / 1e9
 
+    # split-precision exchange (3 x BF16 on tcgen05) on the same workload: the
+    # first call builds the BF16 copies of the tensor (once per geometry)
+    split = None
+    if not args.no_split:
+        vk_split = torch.empty(npair, dtype=torch.float64, device="cuda")
+
+        def k_split():
+            ctx.vk_upper_occ_split_dev(c_cm.data_ptr(), nocc, [nocc - 1], occ.data_ptr(), 1, -1.0,
+                                       vk_split.data_ptr(), st)
+
+        t_prep0 = time.perf_counter()
+        k_split()
+        ctx.synchronize(st)
+        t_prep = time.perf_counter() - t_prep0
+        for _ in range(2):
+            k_split()
+        ctx.synchronize(st)
+        ctx.profile(True)
+        ctx.profile_read()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(args.steps):
+            ctx.vj_upper_dev(dm.data_ptr(), 1, 1.0, 1, vj.data_ptr(), st)
+            k_split()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        sp = ctx.profile_read()
+        ctx.profile(False)
+        t_mixed = s0.elapsed_time(s1) / 1e3 / args.steps
+        rel = float((vk_split - vk).abs().max() / vk.abs().max())
+        half_ms = sp["k_half"][0] / args.steps
+        rank_ms = sp["k_rank"][0] / args.steps
+        bf16_peak = peaks.get("bf16_tflops", 1590.0)
+        half_tc = 3 * w["half_flops"] / (half_ms / 1e3) / 1e12  # BF16 tensor flops actually issued (3 products)
+        split = {
+            "what": "J in FP64 + K as 3 x BF16 split products on tcgen05 (FP32 accumulation in TMEM)",
+            "fock_build_ms": t_mixed * 1e3,
+            "value_tflops_alg": world * flops / t_mixed / 1e12,
+            "speedup_vs_fp64_build": t_step / t_mixed,
+            "k_rel_err_vs_fp64": rel,
+            "k_half_ms": half_ms,
+            "k_rank_ms": rank_ms,
+            "half_roofline": {"bound": "tensor", "achieved": half_tc, "peak": bf16_peak, "unit": "TFLOP/s",
+                              "frac": half_tc / bf16_peak,
+                              "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if "bf16_tflops" in peaks
+                              else "fallback 1.59 PFLOP/s"},
+            "split_tensor_build_s": t_prep,
+        }
+
     # e2e through the host C ABI, pinned host buffers
     e2e = None
     if not args.no_e2e:
@@ -340,6 +389,32 @@ def run_ours(args, w):
                "d2h_bytes_per_step": d2h, "ms_per_step": te / args.steps * 1e3,
                "how": "rijk_vj_upper_with_rimatr_v + rijk_vk_upper_with_ri_v on pinned host buffers, wall clock"}
 
+    # RI-HF SCF on the water molecule of the plain config (def2-SVP / def2-SVP-JKFIT):
+    # FP64 GPU path and mixed-precision path, same converged energy
+    scf = None
+    if rank == 0 and not args.no_scf:
+        from rest_b200.basis import Molecule
+        from rest_b200.scf import SCF, ScfOptions
+
+        water = Molecule.from_angstrom(["O", "H", "H"], [[0.0, 0.0, 0.0], [0.757, 0.587, 0.0], [-0.757, 0.587, 0.0]])
+        tight = dict(scf_acc_etot=1e-8, scf_acc_rho=1e-6, scf_acc_eev=1e-6, max_scf_cycle=100)
+        res = {}
+        sctx = RIJK(local)
+        for prec in ("fp64", "mixed"):
+            t0 = time.perf_counter()
+            runner = SCF(water, "def2-SVP", "def2-SVP-JKFIT", ScfOptions(precision=prec, **tight), ctx=sctx)
+            r = runner.run()
+            res[prec] = {"wall_s": time.perf_counter() - t0, "iterations": r.iterations, "energy": r.energy,
+                         "converged": r.converged, "scf_s": r.timings["scf_s"],
+                         "setup_s": r.timings["one_electron_s"] + r.timings["ri_integrals_s"] + r.timings["fit_s"],
+                         "split_k_builds": r.timings["split_k_builds"]}
+        sctx.close()
+        scf = {"molecule": "H2O def2-SVP/def2-SVP-JKFIT (24 AO, 113 aux), RHF, 1e-8 Eh",
+               "fp64": res["fp64"], "mixed": res["mixed"],
+               "mixed_minus_fp64_energy": res["mixed"]["energy"] - res["fp64"]["energy"],
+               "molecules_per_s_fp64": 1.0 / res["fp64"]["wall_s"],
+               "molecules_per_s_mixed": 1.0 / res["mixed"]["wall_s"]}
+
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         stepf, cflops, threads, sample = cpu_sample_run(w, target_s=6.0)
@@ -370,6 +445,8 @@ def run_ours(args, w):
             "gpu_launches": int(launches),
             "e2e": e2e,
             "cpu_baseline": cpu_base,
+            "split_precision": split,
+            "scf_water": scf,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -392,6 +469,8 @@ def main():
     ap.add_argument("--n", type=int, default=1200, help="num_basis of the sweep workload")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-split", action="store_true", help="skip the split-precision (tcgen05) measurement")
+    ap.add_argument("--no-scf", action="store_true", help="skip the water SCF timing")
     args = ap.parse_args()
     w = workload(args.n)
     if args.impl == "reference":
