@@ -81,6 +81,10 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
                : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
@@ -173,121 +177,153 @@ __global__ void __launch_bounds__(256) k_split_cols(const double* __restrict__ V
   }
 }
 
-// ---- half-transform on tcgen05 -------------------------------------------------
-// One CTA per (P, 128-row block).  Warp 0: producer; warp 1 lane 0: MMA
-// issuer; warps 0..3: epilogue.  smem: STAGES x [A_hi | A_lo | V_hi | V_lo].
+// ---- persistent half-transform ---------------------------------------------------
+// One CTA per SM walks tiles (P, 128-row block) with stride gridDim.x.  Two FP32
+// accumulators in tensor memory (2 x NPAD columns) alternate between tiles, so
+// the epilogue of tile i (4 warps, TMEM -> BF16 split -> HBM) overlaps the MMAs
+// of tile i+1.  Warp 0: producer, warp 1: MMA issuer, warps 2..5: epilogue
+// (warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31).
 template <int NPAD>
-struct HalfTc {
-  static constexpr int STAGES = 2;
+struct HalfTcP {
+  static constexpr int STAGES = NPAD == 256 ? 2 : NPAD == 128 ? 3 : 4;
   static constexpr uint32_t V_BYTES = NPAD * TC_KB * 2;
   static constexpr uint32_t STAGE_BYTES = 2 * BLOCK_BYTES + 2 * V_BYTES;
-  static constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 + 128;
+  static constexpr size_t SMEM = 232448;  // whole per-CTA budget (one CTA per SM)
+  static_assert((size_t)STAGES * STAGE_BYTES + 1024 + 256 <= SMEM, "stage budget");
 };
 
 template <int NPAD>
-__global__ void __launch_bounds__(128, 1)
-    k_half_tc(const __nv_bfloat16* __restrict__ Bhi, const __nv_bfloat16* __restrict__ Blo, int nmb, int nkb,
-              const __nv_bfloat16* __restrict__ Vhi, const __nv_bfloat16* __restrict__ Vlo, int nib,
-              __nv_bfloat16* __restrict__ Xhi, __nv_bfloat16* __restrict__ Xlo, int* err) {
-  using C = HalfTc<NPAD>;
+__global__ void __launch_bounds__(192, 1)
+    k_half_tc_persistent(const __nv_bfloat16* __restrict__ Bhi, const __nv_bfloat16* __restrict__ Blo, int nmb,
+                         int nkb, const __nv_bfloat16* __restrict__ Vhi, const __nv_bfloat16* __restrict__ Vlo,
+                         int nib, int64_t ntiles, __nv_bfloat16* __restrict__ Xhi, __nv_bfloat16* __restrict__ Xlo,
+                         int* err) {
+  using C = HalfTcP<NPAD>;
+  constexpr int S = C::STAGES;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
-  uint64_t* empty = full + C::STAGES;
-  uint64_t* accf = empty + C::STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_BYTES);
+  uint64_t* empty = full + S;
+  uint64_t* acc_full = empty + S;    // [2]
+  uint64_t* acc_empty = acc_full + 2;  // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t blk = blockIdx.x;  // = pl * nmb + mb
-  const int64_t pl = blk / nmb;
-  const int mb = (int)(blk % nmb);
+  const int64_t G = gridDim.x;
+  const int64_t my_tiles = ntiles > blockIdx.x ? (ntiles - blockIdx.x + G - 1) / G : 0;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < C::STAGES; ++s) {
+    for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accf, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 4);
+    }
     mbar_fence_init();
   }
-  if (warp == 0) tc_alloc(tmem_slot, NPAD);
+  if (warp == 0) tc_alloc(tmem_slot, 2 * NPAD);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   bool ok = true;
 
-  if (warp == 0 && lane == 0) {
-    // producer
-    for (int kb = 0; kb < nkb && ok; ++kb) {
-      const int s = kb % C::STAGES;
-      if (kb >= C::STAGES) ok = mbar_wait_bounded(&empty[s], (uint32_t)(((kb / C::STAGES) - 1) & 1), err);
-      if (!ok) break;
-      uint8_t* st = smem + s * C::STAGE_BYTES;
-      mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
-      const int64_t boff = ((pl * nmb + mb) * (int64_t)nkb + kb) * BLOCK_ELEMS;
-      bulk_g2s(st, Bhi + boff, BLOCK_BYTES, &full[s]);
-      bulk_g2s(st + BLOCK_BYTES, Blo + boff, BLOCK_BYTES, &full[s]);
-      const int64_t voff = (int64_t)kb * NPAD * TC_KB;
-      bulk_g2s(st + 2 * BLOCK_BYTES, Vhi + voff, C::V_BYTES, &full[s]);
-      bulk_g2s(st + 2 * BLOCK_BYTES + C::V_BYTES, Vlo + voff, C::V_BYTES, &full[s]);
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int64_t lt = 0; lt < my_tiles && ok; ++lt) {
+        const int64_t tile = blockIdx.x + lt * G;
+        const int64_t pl = tile / nmb;
+        const int mb = (int)(tile % nmb);
+        for (int kb = 0; kb < nkb && ok; ++kb) {
+          const int64_t g = lt * nkb + kb;
+          const int s = (int)(g % S);
+          if (g >= S) ok = mbar_wait_bounded(&empty[s], (uint32_t)(((g / S) - 1) & 1), err);
+          if (!ok) break;
+          uint8_t* st = smem + s * C::STAGE_BYTES;
+          mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
+          const int64_t boff = ((pl * nmb + mb) * (int64_t)nkb + kb) * BLOCK_ELEMS;
+          bulk_g2s(st, Bhi + boff, BLOCK_BYTES, &full[s]);
+          bulk_g2s(st + BLOCK_BYTES, Blo + boff, BLOCK_BYTES, &full[s]);
+          const int64_t voff = (int64_t)kb * NPAD * TC_KB;
+          bulk_g2s(st + 2 * BLOCK_BYTES, Vhi + voff, C::V_BYTES, &full[s]);
+          bulk_g2s(st + 2 * BLOCK_BYTES + C::V_BYTES, Vlo + voff, C::V_BYTES, &full[s]);
+        }
+      }
     }
-  } else if (warp == 1 && lane == 0) {
-    // MMA issuer
-    constexpr uint32_t idesc = idesc_bf16(TC_M, NPAD, false);
-    for (int kb = 0; kb < nkb && ok; ++kb) {
-      const int s = kb % C::STAGES;
-      ok = mbar_wait_bounded(&full[s], (uint32_t)((kb / C::STAGES) & 1), err);
-      if (!ok) break;
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_bf16(TC_M, NPAD, false);
+      for (int64_t lt = 0; lt < my_tiles && ok; ++lt) {
+        const int b = (int)(lt & 1);
+        if (lt >= 2) ok = mbar_wait_bounded(&acc_empty[b], (uint32_t)(((lt / 2) - 1) & 1), err);
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(b * NPAD);
+        for (int kb = 0; kb < nkb && ok; ++kb) {
+          const int64_t g = lt * nkb + kb;
+          const int s = (int)(g % S);
+          ok = mbar_wait_bounded(&full[s], (uint32_t)((g / S) & 1), err);
+          if (!ok) break;
+          tc_fence_after();
+          const uint8_t* st = smem + s * C::STAGE_BYTES;
+#pragma unroll
+          for (int ks = 0; ks < TC_KB / 16; ++ks) {
+            const uint32_t ak = 2 * ks * (TC_M / 8) * 128, vk = 2 * ks * (NPAD / 8) * 128;
+            const uint64_t dah = smem_desc(st + ak, (TC_M / 8) * 128, 128);
+            const uint64_t dal = smem_desc(st + BLOCK_BYTES + ak, (TC_M / 8) * 128, 128);
+            const uint64_t dvh = smem_desc(st + 2 * BLOCK_BYTES + vk, (NPAD / 8) * 128, 128);
+            const uint64_t dvl = smem_desc(st + 2 * BLOCK_BYTES + C::V_BYTES + vk, (NPAD / 8) * 128, 128);
+            const uint32_t acc0 = (kb > 0 || ks > 0) ? 1u : 0u;
+            tc_mma(d, dah, dvh, idesc, acc0);
+            tc_mma(d, dah, dvl, idesc, 1u);
+            tc_mma(d, dal, dvh, idesc, 1u);
+          }
+          tc_commit(&empty[s]);
+        }
+        tc_commit(&acc_full[b]);
+      }
+    }
+  } else {
+    // epilogue warps 2..5
+    const int quad = warp & 3;
+    const int m = quad * 32 + lane;
+    for (int64_t lt = 0; lt < my_tiles; ++lt) {
+      const int b = (int)(lt & 1);
+      const bool got = mbar_wait_bounded(&acc_full[b], (uint32_t)((lt / 2) & 1), err);
+      if (!__all_sync(0xffffffffu, got)) {
+        ok = false;
+        break;
+      }
       tc_fence_after();
-      const uint8_t* st = smem + s * C::STAGE_BYTES;
-      const uint8_t* ahi = st;
-      const uint8_t* alo = st + BLOCK_BYTES;
-      const uint8_t* vhi = st + 2 * BLOCK_BYTES;
-      const uint8_t* vlo = st + 2 * BLOCK_BYTES + C::V_BYTES;
-#pragma unroll
-      for (int ks = 0; ks < TC_KB / 16; ++ks) {
-        // K step ks covers core-matrix columns 2ks, 2ks+1
-        const uint32_t ak = 2 * ks * (TC_M / 8) * 128, vk = 2 * ks * (NPAD / 8) * 128;
-        const uint64_t dah = smem_desc(ahi + ak, (TC_M / 8) * 128, 128);
-        const uint64_t dal = smem_desc(alo + ak, (TC_M / 8) * 128, 128);
-        const uint64_t dvh = smem_desc(vhi + vk, (NPAD / 8) * 128, 128);
-        const uint64_t dvl = smem_desc(vlo + vk, (NPAD / 8) * 128, 128);
-        const uint32_t acc0 = (kb > 0 || ks > 0) ? 1u : 0u;
-        tc_mma(tmem, dah, dvh, idesc, acc0);
-        tc_mma(tmem, dah, dvl, idesc, 1u);
-        tc_mma(tmem, dal, dvh, idesc, 1u);
-      }
-      tc_commit(&empty[s]);  // stage s is free once these MMAs have read it
-    }
-    tc_commit(accf);
-  }
-  __syncwarp();
-  // epilogue: warps 0..3, one TMEM lane (= row) per thread
-  const bool acc_ok = __syncthreads_and(ok) && mbar_wait_bounded(accf, 0, err);
-  tc_fence_after();
-  if (acc_ok) {
-    const int m = warp * 32 + lane;
-    const int64_t xbase = ((pl * nmb + mb) * (int64_t)nib) * BLOCK_ELEMS;
+      const int64_t tile = blockIdx.x + lt * G;
+      const int64_t pl = tile / nmb;
+      const int mb = (int)(tile % nmb);
+      const int64_t xbase = ((pl * nmb + mb) * (int64_t)nib) * BLOCK_ELEMS;
 #pragma unroll 1
-    for (int c0 = 0; c0 < NPAD; c0 += 32) {
-      float v[32];
-      tc_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-      const int ib = c0 / TC_KB;
+      for (int c0 = 0; c0 < NPAD; c0 += 32) {
+        float v[32];
+        tc_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * NPAD + c0), v);
+        const int ib = c0 / TC_KB;
 #pragma unroll
-      for (int g = 0; g < 4; ++g) {  // 8 columns -> one 16-byte core-matrix row
-        __align__(16) __nv_bfloat16 h[8], l[8];
+        for (int gq = 0; gq < 4; ++gq) {
+          __align__(16) __nv_bfloat16 h[8], l[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) split_bf16((double)v[g * 8 + j], h[j], l[j]);
-        const int k = (c0 % TC_KB) + g * 8;
-        const int64_t off = xbase + (int64_t)ib * BLOCK_ELEMS + core_off(m, k, TC_M);
-        *reinterpret_cast<uint4*>(Xhi + off) = *reinterpret_cast<const uint4*>(h);
-        *reinterpret_cast<uint4*>(Xlo + off) = *reinterpret_cast<const uint4*>(l);
+          for (int j = 0; j < 8; ++j) split_bf16((double)v[gq * 8 + j], h[j], l[j]);
+          const int k = (c0 % TC_KB) + gq * 8;
+          const int64_t off = xbase + (int64_t)ib * BLOCK_ELEMS + core_off(m, k, TC_M);
+          *reinterpret_cast<uint4*>(Xhi + off) = *reinterpret_cast<const uint4*>(h);
+          *reinterpret_cast<uint4*>(Xlo + off) = *reinterpret_cast<const uint4*>(l);
+        }
       }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[b]);
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tc_dealloc(tmem, NPAD);
+  if (warp == 0) tc_dealloc(tmem, 2 * NPAD);
 }
 
 // ---- rank update on tcgen05 --------------------------------------------------------
@@ -461,17 +497,30 @@ void launch_split_cols(const Geom& g, const TcGeom& t, const double* V, int64_t 
                                        static_cast<__nv_bfloat16*>(lo));
 }
 
+static int sm_count() {
+  int dev = 0, n = 148;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    n = 148;
+  }
+  return n;
+}
+
 template <int NPAD>
 static void half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
                     const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st) {
-  using C = HalfTc<NPAD>;
-  cudaFuncSetAttribute(k_half_tc<NPAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+  using C = HalfTcP<NPAD>;
+  cudaFuncSetAttribute(k_half_tc_persistent<NPAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
   const int64_t per_p = (int64_t)t.nmb * t.nkb * BLOCK_ELEMS;
+  const int64_t ntiles = np * t.nmb;
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, sm_count()));
   count_launch();
-  k_half_tc<NPAD><<<(unsigned)(np * t.nmb), 128, C::SMEM, st>>>(
+  k_half_tc_persistent<NPAD><<<grid, 192, C::SMEM, st>>>(
       static_cast<const __nv_bfloat16*>(Bhi) + p0 * per_p, static_cast<const __nv_bfloat16*>(Blo) + p0 * per_p,
-      t.nmb, t.nkb, static_cast<const __nv_bfloat16*>(Vhi), static_cast<const __nv_bfloat16*>(Vlo), t.nib,
+      t.nmb, t.nkb, static_cast<const __nv_bfloat16*>(Vhi), static_cast<const __nv_bfloat16*>(Vlo), t.nib, ntiles,
       static_cast<__nv_bfloat16*>(Xhi), static_cast<__nv_bfloat16*>(Xlo), err);
+  (void)g;
 }
 
 void launch_half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
