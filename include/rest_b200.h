@@ -85,6 +85,12 @@ enum rijk_prof_class {
  * producer warp, 3 stages.  RIJK_HT_CFG / RIJK_RK_CFG override the defaults
  * at context creation. */
 int rijk_ctx_set_tiles(rijk_ctx* ctx, int half_transform_cfg, int update_cfg);
+/* Autotuner: times every CTA shape of the half-transform and of the rank
+ * update on sample_rows aux rows (<= 0: 512) of the loaded tensor with ncols
+ * occupied columns, keeps the fastest of each and returns them; ms (if
+ * non-NULL, 8 doubles) receives {half, update} milliseconds per shape. */
+int rijk_ctx_autotune(rijk_ctx* ctx, int64_t ncols, int64_t sample_rows, int* best_half, int* best_update,
+                      double* ms);
 int rijk_ctx_profile(rijk_ctx* ctx, int enable);
 int rijk_ctx_profile_read(rijk_ctx* ctx, double* ms, int64_t* launches);
 /* Wait for the work enqueued on `stream` (NULL = the context's stream) and

@@ -482,6 +482,71 @@ int rijk_ctx_set_tiles(rijk_ctx* ctx, int half_transform_cfg, int update_cfg) {
   return RIJK_OK;
 }
 
+int rijk_ctx_autotune(rijk_ctx* ctx, int64_t ncols, int64_t sample_rows, int* best_half, int* best_update,
+                      double* ms_out) {
+  RIJK_TRY(need_tensor(ctx));
+  if (ncols <= 0) return set_err(ctx, RIJK_ERR_ARG, "ncols must be positive");
+  Geom g = ctx->g;
+  cudaStream_t st = ctx->stream;
+  const int64_t np = std::max<int64_t>(1, std::min<int64_t>(g.naux, sample_rows > 0 ? sample_rows : 512));
+  const int64_t ldx = round_up(g.n, 128);
+  const int64_t ocols = round_up(ncols, 128);
+  RIJK_TRY(ensure(ctx, ctx->Cw, (size_t)ldx * ocols * 8));
+  RIJK_TRY(ensure(ctx, ctx->X, (size_t)np * ldx * ocols * 8));
+  // any non-zero operand times the same as the real one: fill C with a constant
+  std::vector<double> ones((size_t)ldx * ocols, 0.0);
+  for (int64_t c = 0; c < ncols; ++c)
+    for (int64_t r = 0; r < g.n; ++r) ones[r + ldx * c] = 1.0 / (1.0 + (double)((r + c) % 7));
+  RIJK_CK(cudaMemcpyAsync(ctx->Cw.p, ones.data(), ones.size() * 8, cudaMemcpyHostToDevice, st));
+  cudaEvent_t a, b;
+  RIJK_CK(cudaEventCreate(&a));
+  RIJK_CK(cudaEventCreate(&b));
+  double best_ht_ms = 1e30, best_rk_ms = 1e30;
+  int bh = ctx->ht_cfg, br = ctx->rk_cfg;
+  for (int cfg = 0; cfg < 4; ++cfg) {
+    g.ht_cfg = cfg;
+    g.rk_cfg = cfg;
+    const int splits = rijk::k_rank_splits(g, np, 0);
+    RIJK_TRY(ensure(ctx, ctx->Kpart, (size_t)splits * rijk::k_block_pairs(g, 0) * 128 * 128 * 8));
+    float t_ht = 0.f, t_rk = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {  // first repetition warms up
+      RIJK_CK(cudaEventRecord(a, st));
+      rijk::launch_half_transform(g, ctx->dB, 0, np, static_cast<double*>(ctx->Cw.p), ldx, ocols, ncols,
+                                  static_cast<double*>(ctx->X.p), ldx, ldx * ocols, ctx->d_err, st);
+      RIJK_CK(cudaEventRecord(b, st));
+      RIJK_CK(cudaEventSynchronize(b));
+      RIJK_CK(cudaEventElapsedTime(&t_ht, a, b));
+      RIJK_CK(cudaEventRecord(a, st));
+      rijk::launch_k_rank_update(g, static_cast<double*>(ctx->X.p), ldx, ldx * ocols, np, 0, ncols, splits, 0,
+                                 static_cast<double*>(ctx->Kpart.p), ctx->d_err, st);
+      RIJK_CK(cudaEventRecord(b, st));
+      RIJK_CK(cudaEventSynchronize(b));
+      RIJK_CK(cudaEventElapsedTime(&t_rk, a, b));
+    }
+    RIJK_TRY(after_launch(ctx, "autotune"));
+    if (ms_out) {
+      ms_out[2 * cfg] = t_ht;
+      ms_out[2 * cfg + 1] = t_rk;
+    }
+    if (t_ht < best_ht_ms) {
+      best_ht_ms = t_ht;
+      bh = cfg;
+    }
+    if (t_rk < best_rk_ms) {
+      best_rk_ms = t_rk;
+      br = cfg;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  RIJK_TRY(sync_and_check(ctx, st));
+  ctx->ht_cfg = ctx->g.ht_cfg = bh;
+  ctx->rk_cfg = ctx->g.rk_cfg = br;
+  if (best_half) *best_half = bh;
+  if (best_update) *best_update = br;
+  return RIJK_OK;
+}
+
 int rijk_ctx_profile(rijk_ctx* ctx, int enable) {
   if (!ctx) return RIJK_ERR_ARG;
   ctx->prof = enable != 0;

@@ -103,6 +103,14 @@ class RIJK:
     def set_tiles(self, half_transform_cfg: int, update_cfg: int):
         self._check(lib().rijk_ctx_set_tiles(self._h, int(half_transform_cfg), int(update_cfg)))
 
+    def autotune(self, ncols: int, sample_rows: int = 0):
+        """Time every CTA shape on this tensor, keep the fastest; returns
+        (half_cfg, update_cfg, {cfg: (half_ms, update_ms)})."""
+        bh, br = C.c_int(), C.c_int()
+        ms = (C.c_double * 8)()
+        self._check(lib().rijk_ctx_autotune(self._h, int(ncols), int(sample_rows), C.byref(bh), C.byref(br), ms))
+        return bh.value, br.value, {c: (ms[2 * c], ms[2 * c + 1]) for c in range(4)}
+
     def profile(self, enable: bool = True):
         self._check(lib().rijk_ctx_profile(self._h, int(bool(enable))))
 

@@ -272,6 +272,23 @@ def _n1200_body(ctx, n):
     assert float(ek) < 0
 
 
+def test_autotuner_picks_a_shape_and_keeps_results(ctx):
+    n, naux, nocc = 200, 800, 33
+    case = host_case(n, naux, nocc, seed=77)
+    ctx.set_rimatr(case.rimatr, n)
+    try:
+        bh, br, ms = ctx.autotune(nocc, 256)
+        assert 0 <= bh <= 3 and 0 <= br <= 3
+        assert all(v[0] > 0 and v[1] > 0 for v in ms.values())
+        assert ms[bh][0] == min(v[0] for v in ms.values())
+        occ = np.full(nocc, 2.0)
+        ri3 = O.ri3fn_from_rimatr(case.rimatr, n)
+        k = ctx.vk_upper_with_ri_v([case.c_occ], [nocc - 1], [occ], 1, -0.5)[0]
+        assert _maxdiff(k, O.vk_upper_with_ri_v(ri3, [case.c_occ], [nocc - 1], [occ], 1, -0.5)[0]) <= TOL
+    finally:
+        ctx.set_tiles(1, 1)
+
+
 @pytest.mark.parametrize("n,naux,rows,cols", [(7, 33, (2, 7), (0, 2)), (37, 150, (6, 37), (0, 6)),
                                               (130, 300, (20, 130), (3, 20))])
 def test_ao2mo_ri3mo(ctx, n, naux, rows, cols):
