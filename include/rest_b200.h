@@ -238,6 +238,26 @@ int rijk_int2c2e(const rijk_shells* aux, const double* const* c2s, double* out);
  * (src/molecule_io/mod.rs:1611-1660): (mu nu|P) in rimatr layout [npair, naux]. */
 int rijk_int3c2e(const rijk_shells* bas, const rijk_shells* aux, const double* const* c2s, double* out);
 
+/* ---- integrals (device) -------------------------------------------------------- */
+/* The same integrals computed on the current CUDA device into device memory,
+ * for AO shells with l <= 2 and auxiliary shells with l <= 4
+ * (RIJK_ERR_TOO_LARGE otherwise); c2s must hold the matrices for l = 0..4.
+ * They replace the libcint loops of int_ij_aux_columb (src/molecule_io/mod.rs:1038)
+ * and prepare_rimatr_for_ri_v_rayon_v02 (src/molecule_io/mod.rs:1604-1660).
+ * Both return after the results are complete on `stream` (NULL: legacy default
+ * stream).  Calls from several host threads at once must be serialised. */
+int rijk_int2c2e_dev(const rijk_shells* aux, const double* const* c2s, double* d_out, void* stream);
+int rijk_int3c2e_dev(const rijk_shells* bas, const rijk_shells* aux, const double* const* c2s, double* d_out,
+                     void* stream);
+/* prepare_rimatr_for_ri_v_rayon_v02 (src/molecule_io/mod.rs:1563-1721) with
+ * every step on the device: (P|Q) and (mu nu|P) from the device integral
+ * engine (limits above), then the metric step.  metric_factor NULL: Cholesky
+ * fit as in rijk_build_rimatr_cholesky (failed_pivot as there); otherwise the
+ * host num_auxbas^2 factor M is applied, B = (mu nu|P) M, as rijk_fit_rimatr
+ * does with REST's V^-1/2.  The tensor is left loaded in the context. */
+int rijk_build_rimatr_from_shells(rijk_ctx* ctx, const rijk_shells* bas, const rijk_shells* aux,
+                                  const double* const* c2s, const double* metric_factor, int64_t* failed_pivot);
+
 /* ---- MO-basis three-centre tensor -------------------------------------------- */
 /* generate_ri3mo_rayon / ao2mo_rayon (src/scf_io/mod.rs:2331-2359, :3270-3307):
  * ri3mo[P, a, i] = sum_{mu,nu} C[mu, a] B_P[mu, nu] C[nu, i] for a in

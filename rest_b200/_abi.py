@@ -121,6 +121,15 @@ SIGNATURES = {
     "rijk_int1e": (C.c_int, [C.POINTER(RijkShells), C.c_void_p, C.c_int, C.c_int, _dp, _dp, _dp]),
     "rijk_int2c2e": (C.c_int, [C.POINTER(RijkShells), C.c_void_p, _dp]),
     "rijk_int3c2e": (C.c_int, [C.POINTER(RijkShells), C.POINTER(RijkShells), C.c_void_p, _dp]),
+    "rijk_int2c2e_dev": (C.c_int, [C.POINTER(RijkShells), C.c_void_p, C.c_void_p, C.c_void_p]),
+    "rijk_int3c2e_dev": (
+        C.c_int,
+        [C.POINTER(RijkShells), C.POINTER(RijkShells), C.c_void_p, C.c_void_p, C.c_void_p],
+    ),
+    "rijk_build_rimatr_from_shells": (
+        C.c_int,
+        [_ctxp, C.POINTER(RijkShells), C.POINTER(RijkShells), C.c_void_p, C.c_void_p, _i64p],
+    ),
 }
 
 

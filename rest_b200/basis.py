@@ -236,3 +236,34 @@ def int3c2e(bas: ShellSet, aux: ShellSet) -> np.ndarray:
     _check(lib().rijk_int3c2e(C.byref(bas.cstruct()), C.byref(aux.cstruct()), _C2S_PTRS,
                               out.ctypes.data_as(C.POINTER(C.c_double))), "int3c2e")
     return out
+
+
+# angular-momentum limits of the device integral engine (rijk_int*_dev)
+DEVICE_MAX_L_AO = 2
+DEVICE_MAX_L_AUX = 4
+
+
+def int2c2e_dev(aux: ShellSet, stream=None):
+    """(P|Q) computed on the current CUDA device: a torch float64 tensor
+    (naux, naux) whose storage is column-major (it is symmetric)."""
+    import torch
+
+    n = aux.nfun
+    out = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    _check(lib().rijk_int2c2e_dev(C.byref(aux.cstruct()), _C2S_PTRS, C.c_void_p(out.data_ptr()), C.c_void_p(st)),
+           "int2c2e_dev")
+    return out
+
+
+def int3c2e_dev(bas: ShellSet, aux: ShellSet, stream=None):
+    """(mu nu|P) computed on the current CUDA device in rimatr layout: a torch
+    float64 tensor of shape (naux, npair), row P = packed upper triangle of (..|P)."""
+    import torch
+
+    n, naux = bas.nfun, aux.nfun
+    out = torch.empty((naux, n * (n + 1) // 2), dtype=torch.float64, device="cuda")
+    st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    _check(lib().rijk_int3c2e_dev(C.byref(bas.cstruct()), C.byref(aux.cstruct()), _C2S_PTRS,
+                                  C.c_void_p(out.data_ptr()), C.c_void_p(st)), "int3c2e_dev")
+    return out

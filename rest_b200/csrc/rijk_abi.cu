@@ -638,14 +638,12 @@ int rijk_get_rimatr(rijk_ctx* ctx, double* rimatr) {
   return sync_and_check(ctx, ctx->stream);
 }
 
-int rijk_build_rimatr_cholesky(rijk_ctx* ctx, const double* aux_v, const double* int3c, int64_t num_basis,
-                               int64_t num_auxbas, int64_t* failed_pivot) {
-  if (failed_pivot) *failed_pivot = 0;
-  if (!ctx || !aux_v || !int3c) return set_err(ctx, RIJK_ERR_ARG, "null argument");
-  RIJK_TRY(upload_tensor(ctx, int3c, num_basis, num_auxbas, 0));
-  ctx->have = false;
+namespace {
+
+// The padded metric V is in ctx->mV and the three-centre rows in the tensor:
+// factor V = L L^T, invert L and fit B = int3c L^-T in place.
+int cholesky_fit(rijk_ctx* ctx, int64_t* failed_pivot) {
   const int64_t np = ctx->naux_pad;
-  RIJK_TRY(upload_square_padded(ctx, aux_v, num_auxbas, np, ctx->mV));
   RIJK_TRY(ensure(ctx, ctx->mLinvd, (size_t)np * rijk::TS * 8));
   RIJK_TRY(ensure(ctx, ctx->mLinv, (size_t)np * np * 8));
   RIJK_TRY(ensure(ctx, ctx->mT, (size_t)np * np * 8));
@@ -670,6 +668,104 @@ int rijk_build_rimatr_cholesky(rijk_ctx* ctx, const double* aux_v, const double*
   RIJK_TRY(sync_and_check(ctx, ctx->stream));
   ctx->have = true;
   return RIJK_OK;
+}
+
+struct PlanGuard {
+  rijk::RiIntPlan* p = nullptr;
+  ~PlanGuard() {
+    if (p) rijk::ri_plan_destroy(p);
+  }
+};
+
+const char* plan_error(int rc) {
+  return rc == RIJK_ERR_TOO_LARGE ? "device integrals take AO shells with l <= 2 and auxiliary shells with l <= 4"
+                                  : "invalid shell data or c2s table";
+}
+
+}  // namespace
+
+int rijk_build_rimatr_cholesky(rijk_ctx* ctx, const double* aux_v, const double* int3c, int64_t num_basis,
+                               int64_t num_auxbas, int64_t* failed_pivot) {
+  if (failed_pivot) *failed_pivot = 0;
+  if (!ctx || !aux_v || !int3c) return set_err(ctx, RIJK_ERR_ARG, "null argument");
+  RIJK_TRY(upload_tensor(ctx, int3c, num_basis, num_auxbas, 0));
+  ctx->have = false;
+  RIJK_TRY(upload_square_padded(ctx, aux_v, num_auxbas, ctx->naux_pad, ctx->mV));
+  return cholesky_fit(ctx, failed_pivot);
+}
+
+int rijk_int2c2e_dev(const rijk_shells* aux, const double* const* c2s, double* d_out, void* stream) {
+  if (!aux || !c2s || !d_out) return RIJK_ERR_ARG;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  PlanGuard pg;
+  const int rc = rijk::ri_plan_create(nullptr, aux, c2s, st, &pg.p);
+  if (rc != RIJK_OK) return rc;
+  rijk::launch_int2c2e(pg.p, d_out, rijk::ri_plan_naux(pg.p), st);
+  if (cudaGetLastError() != cudaSuccess) return RIJK_ERR_CUDA;
+  return cudaStreamSynchronize(st) == cudaSuccess ? RIJK_OK : RIJK_ERR_CUDA;
+}
+
+int rijk_int3c2e_dev(const rijk_shells* bas, const rijk_shells* aux, const double* const* c2s, double* d_out,
+                     void* stream) {
+  if (!bas || !aux || !c2s || !d_out) return RIJK_ERR_ARG;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  PlanGuard pg;
+  const int rc = rijk::ri_plan_create(bas, aux, c2s, st, &pg.p);
+  if (rc != RIJK_OK) return rc;
+  const int64_t n = rijk::ri_plan_nbas(pg.p), npair = n * (n + 1) / 2;
+  const int nsh = rijk::ri_plan_aux_shells(pg.p);
+  for (int k0 = 0; k0 < nsh; k0 += 64) {
+    const int k1 = std::min(nsh, k0 + 64);
+    rijk::launch_int3c2e(pg.p, k0, k1, d_out + rijk::ri_plan_aux_offset(pg.p, k0) * npair, st);
+    if (cudaGetLastError() != cudaSuccess) return RIJK_ERR_CUDA;
+  }
+  return cudaStreamSynchronize(st) == cudaSuccess ? RIJK_OK : RIJK_ERR_CUDA;
+}
+
+int rijk_build_rimatr_from_shells(rijk_ctx* ctx, const rijk_shells* bas, const rijk_shells* aux,
+                                  const double* const* c2s, const double* metric_factor, int64_t* failed_pivot) {
+  if (failed_pivot) *failed_pivot = 0;
+  if (!ctx || !bas || !aux || !c2s) return set_err(ctx, RIJK_ERR_ARG, "null argument");
+  RIJK_CK(cudaSetDevice(ctx->device));
+  PlanGuard pg;
+  const int rc = rijk::ri_plan_create(bas, aux, c2s, ctx->stream, &pg.p);
+  if (rc != RIJK_OK) return set_err(ctx, rc, plan_error(rc));
+  const int64_t n = rijk::ri_plan_nbas(pg.p), naux = rijk::ri_plan_naux(pg.p);
+  RIJK_TRY(alloc_tensor(ctx, n, naux));
+  const Geom& g = ctx->g;
+  // three-centre rows, a run of auxiliary shells at a time, packed as they come
+  const size_t chunk_bytes = std::max<size_t>((size_t)256 << 20, (size_t)9 * g.npair * 8);
+  RIJK_TRY(ensure(ctx, ctx->stage, std::max<size_t>(chunk_bytes, (size_t)naux * naux * 8)));
+  double* st = static_cast<double*>(ctx->stage.p);
+  const int nsh = rijk::ri_plan_aux_shells(pg.p);
+  for (int k0 = 0; k0 < nsh;) {
+    int k1 = k0 + 1;
+    while (k1 < nsh &&
+           (size_t)(rijk::ri_plan_aux_offset(pg.p, k1 + 1) - rijk::ri_plan_aux_offset(pg.p, k0)) * g.npair * 8 <=
+               chunk_bytes)
+      ++k1;
+    const int64_t p0 = rijk::ri_plan_aux_offset(pg.p, k0), np = rijk::ri_plan_aux_offset(pg.p, k1) - p0;
+    rijk::launch_int3c2e(pg.p, k0, k1, st, ctx->stream);
+    RIJK_TRY(after_launch(ctx, "int3c2e"));
+    rijk::launch_pack_rimatr(g, st, np, ctx->dB + p0 * g.ldB, ctx->stream);
+    RIJK_TRY(after_launch(ctx, "pack tensor"));
+    k0 = k1;
+  }
+  ctx->tensor_version++;
+  const int64_t npad = ctx->naux_pad;
+  if (metric_factor) {
+    RIJK_TRY(upload_square_padded(ctx, metric_factor, naux, npad, ctx->mV));
+    RIJK_TRY(fit_in_place(ctx, static_cast<double*>(ctx->mV.p), npad, 0, 0));
+    RIJK_TRY(sync_and_check(ctx, ctx->stream));
+    ctx->have = true;
+    return RIJK_OK;
+  }
+  RIJK_TRY(ensure(ctx, ctx->mV, (size_t)npad * npad * 8));
+  rijk::launch_int2c2e(pg.p, st, naux, ctx->stream);
+  RIJK_TRY(after_launch(ctx, "int2c2e"));
+  rijk::launch_pad_matrix(st, naux, npad, static_cast<double*>(ctx->mV.p), ctx->stream);
+  RIJK_TRY(after_launch(ctx, "pad metric"));
+  return cholesky_fit(ctx, failed_pivot);
 }
 
 int rijk_fit_rimatr(rijk_ctx* ctx, const double* metric_factor, const double* int3c, int64_t num_basis,

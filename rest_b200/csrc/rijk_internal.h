@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/rest_b200.h"
+
 namespace rijk {
 
 // Geometry of the tile-packed tensor held by a context.
@@ -125,5 +127,21 @@ void run_trtri(const double* L, int64_t np, int64_t ld, const double* Linvd, dou
                cudaStream_t st);
 // Copy a dense n x n (ld n) matrix into a zero-padded np x np (ld np) buffer.
 void launch_pad_matrix(const double* src, int64_t n, int64_t np, double* dst, cudaStream_t st);
+
+// --- device integral engine (rijk_ints_gpu.cu) ------------------------------------
+// A plan holds the device copy of an AO shell set (may be null: metric only)
+// and an auxiliary shell set, and loads the c2s table after `st` drains.
+struct RiIntPlan;
+int ri_plan_create(const rijk_shells* bas, const rijk_shells* aux, const double* const* c2s, cudaStream_t st,
+                   RiIntPlan** out);
+void ri_plan_destroy(RiIntPlan* p);
+int64_t ri_plan_nbas(const RiIntPlan* p);
+int64_t ri_plan_naux(const RiIntPlan* p);
+int ri_plan_aux_shells(const RiIntPlan* p);
+int64_t ri_plan_aux_offset(const RiIntPlan* p, int k);  // first function of auxiliary shell k (k <= nshell)
+// (P|Q) into dV (naux x naux, column-major, leading dimension ldv)
+void launch_int2c2e(const RiIntPlan* p, double* dV, int64_t ldv, cudaStream_t st);
+// (mu nu|P) for the auxiliary shells [k0, k1): rimatr rows starting at the first function of k0
+void launch_int3c2e(const RiIntPlan* p, int k0, int k1, double* out, cudaStream_t st);
 
 }  // namespace rijk

@@ -184,6 +184,20 @@ class RIJK:
         self._check(lib().rijk_fit_rimatr(self._h, _ptr(f), _ptr(m), num_basis, m.shape[1]))
         self.num_basis, self.num_auxbas = num_basis, m.shape[1]
 
+    def build_rimatr_from_shells(self, bas, aux, metric_factor: np.ndarray | None = None):
+        """Integrals, metric and fit all on the device (REST's
+        prepare_rimatr_for_ri_v_rayon_v02): Cholesky fit when ``metric_factor``
+        is None, else B = (mu nu|P) M with the given factor (e.g. V^-1/2).
+        ``bas`` and ``aux`` are ``basis.ShellSet`` objects."""
+        from .basis import _C2S_PTRS
+
+        piv = C.c_int64(0)
+        f = None if metric_factor is None else np.asfortranarray(_f64(metric_factor))
+        st = lib().rijk_build_rimatr_from_shells(self._h, C.byref(bas.cstruct()), C.byref(aux.cstruct()),
+                                                 _C2S_PTRS, None if f is None else _ptr(f), C.byref(piv))
+        self._check(st, piv.value)
+        self.num_basis, self.num_auxbas = bas.nfun, aux.nfun
+
     # -- J -------------------------------------------------------------------
     def _vj(self, fn, dm, spin_channel, scaling_factor, full=False):
         n = self.num_basis

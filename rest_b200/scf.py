@@ -25,7 +25,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import scipy.linalg as sla
 
-from .basis import Molecule, int1e, int2c2e, int3c2e
+from .basis import DEVICE_MAX_L_AO, DEVICE_MAX_L_AUX, Molecule, int1e, int2c2e, int2c2e_dev, int3c2e
 from .rijk import RIJK
 
 AUXBAS_THRESHOLD = 1.0e-8  # src/constants/mod.rs:81
@@ -73,6 +73,10 @@ class ScfOptions:
     scf_acc_etot: float = 1.0e-8
     initial_guess: str = "hcore"
     metric: str = "inv_sqrt"  # inv_sqrt (REST's live path) | cholesky
+    # where (P|Q) and (mu nu|P) are computed: "device" (CUDA integral engine,
+    # AO l <= 2 and auxiliary l <= 4), "host" (OpenMP engine) or "auto" (device
+    # when the shells are within its limits)
+    integrals: str = "auto"
     start_check_oscillation: int = 20
     print_level: int = 0
     # precision of the exchange build: "fp64" (plain) or "mixed": incremental
@@ -116,15 +120,24 @@ class SCF:
             raise ValueError(f"overlap matrix is singular (lowest eigenvalue {lam[0]:.3e})")
         self.ovlp_lowest_eig = float(lam[0])
         t1 = time.perf_counter()
-        v2 = int2c2e(self.aux)
-        i3 = int3c2e(self.bas, self.aux)
-        t2 = time.perf_counter()
-        if self.opts.metric == "inv_sqrt":
-            self.ctx.fit_rimatr(metric_inv_sqrt(v2), i3, self.n)
-        elif self.opts.metric == "cholesky":
-            self.ctx.build_rimatr_cholesky(v2, i3, self.n)
-        else:
+        if self.opts.metric not in ("inv_sqrt", "cholesky"):
             raise ValueError(f"unknown metric {self.opts.metric!r}")
+        self.integrals_on = self._integral_engine()
+        if self.integrals_on == "device":
+            # integrals, metric and fit on the device; V^-1/2 needs V on the host
+            factor = None
+            if self.opts.metric == "inv_sqrt":
+                factor = metric_inv_sqrt(int2c2e_dev(self.aux).cpu().numpy())
+            t2 = time.perf_counter()
+            self.ctx.build_rimatr_from_shells(self.bas, self.aux, factor)
+        else:
+            v2 = int2c2e(self.aux)
+            i3 = int3c2e(self.bas, self.aux)
+            t2 = time.perf_counter()
+            if self.opts.metric == "inv_sqrt":
+                self.ctx.fit_rimatr(metric_inv_sqrt(v2), i3, self.n)
+            else:
+                self.ctx.build_rimatr_cholesky(v2, i3, self.n)
         t3 = time.perf_counter()
         self.timings = {"one_electron_s": t1 - t0, "ri_integrals_s": t2 - t1, "fit_s": t3 - t2}
         # occupations (generate_occupation_integer, :364-440)
@@ -146,6 +159,16 @@ class SCF:
         self._split_steps = 0
         self.split_builds = 0
         self.fp64_builds = 0
+
+    def _integral_engine(self) -> str:
+        mode = self.opts.integrals
+        if mode not in ("auto", "device", "host"):
+            raise ValueError(f"unknown integrals engine {mode!r}")
+        if mode == "auto":
+            # a context without the device builder (a CPU stand-in) takes host integrals
+            fits = int(self.bas.l.max()) <= DEVICE_MAX_L_AO and int(self.aux.l.max()) <= DEVICE_MAX_L_AUX
+            return "device" if fits and hasattr(self.ctx, "build_rimatr_from_shells") else "host"
+        return mode
 
     # -- pieces of the loop ---------------------------------------------------
     def occupation(self):
