@@ -53,8 +53,19 @@ def _stale(lib: Path) -> bool:
     return any(p.stat().st_mtime > t for p in deps)
 
 
-def _compile(src: Path, extra: list[str]) -> Path:
+def _obj_stale(src: Path, obj: Path) -> bool:
+    """An object is rebuilt when its source or any header is newer."""
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))
+    return any(p.stat().st_mtime > t for p in [src] + headers)
+
+
+def _compile(src: Path, extra: list[str], force: bool = False) -> Path:
     obj = BUILD / (src.stem + ".o")
+    if not force and not extra and not _obj_stale(src, obj):
+        return obj
     if src.suffix == ".cpp":  # host-only code: g++ with OpenMP
         cmd = ["g++", "-c", str(src), "-o", str(obj), "-O3", "-fPIC", "-fopenmp", "-std=c++17", "-I" + str(INCLUDE)]
     else:
@@ -75,7 +86,9 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     if verbose_ptxas:
         os.environ["RIJK_PTXAS_VERBOSE"] = "1"
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, extra), sources()))
+        # longest compiles first so that they overlap the short ones
+        srcs = sorted(sources(), key=lambda p: p.stat().st_size, reverse=True)
+        objs = list(ex.map(lambda s: _compile(s, extra, force), srcs))
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", str(tmp)] + [str(o) for o in objs] + ["-lgomp"]
     r = subprocess.run(cmd, capture_output=True, text=True)

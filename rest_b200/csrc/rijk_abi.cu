@@ -733,8 +733,9 @@ int rijk_build_rimatr_from_shells(rijk_ctx* ctx, const rijk_shells* bas, const r
   const int64_t n = rijk::ri_plan_nbas(pg.p), naux = rijk::ri_plan_naux(pg.p);
   RIJK_TRY(alloc_tensor(ctx, n, naux));
   const Geom& g = ctx->g;
-  // three-centre rows, a run of auxiliary shells at a time, packed as they come
-  const size_t chunk_bytes = std::max<size_t>((size_t)256 << 20, (size_t)9 * g.npair * 8);
+  // three-centre rows, a run of auxiliary shells at a time, packed as they come;
+  // large runs keep every class kernel's grid wide
+  const size_t chunk_bytes = std::max<size_t>(ctx->scratch_budget / 2, (size_t)9 * g.npair * 8);
   RIJK_TRY(ensure(ctx, ctx->stage, std::max<size_t>(chunk_bytes, (size_t)naux * naux * 8)));
   double* st = static_cast<double*>(ctx->stage.p);
   const int nsh = rijk::ri_plan_aux_shells(pg.p);

@@ -1,16 +1,13 @@
-// Two- and three-centre Coulomb integrals on the GPU (McMurchie-Davidson),
-// the device counterpart of rijk_ints.cpp.  REST computes (P|Q)
-// (int_ij_aux_columb, src/molecule_io/mod.rs:1038, called at :1577) and the
-// (mu nu|P) blocks of prepare_rimatr_for_ri_v_rayon_v02 (:1604-1660) with
-// libcint on the host before its metric step; here both are produced in HBM,
-// so the fitted tensor is built without a host round trip.  One thread
-// evaluates one (AO shell pair, auxiliary shell) block: Hermite expansion
-// coefficients of the bra pair and of the single-centre ket, Hermite Coulomb
-// integrals R_tuv from the Boys function (tetrahedral storage, two ping-pong
-// levels), the Cartesian block, then the transform to real solid harmonics
-// with the caller's c2s matrices (constant memory), ket index first.
-// Supported: AO shells l <= 2, auxiliary shells l <= 4 (the bra of (P|Q) is
-// one auxiliary shell).
+// Two- and three-centre Coulomb integrals on the GPU, the device counterpart of
+// rijk_ints.cpp.  REST computes (P|Q) (int_ij_aux_columb,
+// src/molecule_io/mod.rs:1038, called at :1577) and the (mu nu|P) blocks of
+// prepare_rimatr_for_ri_v_rayon_v02 (:1604-1660) with libcint on the host
+// before its metric step; here both are produced in HBM, so the fitted tensor
+// is built without a host round trip.  Three-centre blocks: one thread per
+// (AO shell pair, auxiliary shell), one kernel per angular class
+// (rijk_ints_dev.cuh) over shell pairs sorted by class and primitive count, so
+// that a warp runs one code path.  Two-centre blocks: one thread per auxiliary
+// shell pair with run-time angular loops (a small share of the work).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -20,71 +17,14 @@
 #include <vector>
 
 #include "../../include/rest_b200.h"
+#include "rijk_ints_dev.cuh"
 #include "rijk_internal.h"
 
 namespace rijk {
 
+using namespace intsdev;
+
 namespace {
-
-constexpr int GLA = 2;                                    // max AO l
-constexpr int GLC = 4;                                    // max auxiliary l
-constexpr int GL = 2 * GLA + GLC;                         // max total l of (ab|c) and (c|d)
-constexpr int NTET = (GL + 1) * (GL + 2) * (GL + 3) / 6;  // R_tuv with t+u+v <= GL
-constexpr int C2S_TOTAL = 1 * 1 + 3 * 3 + 5 * 6 + 7 * 10 + 9 * 15;
-constexpr int MAXCART = 6 * 6 * 15;  // (dd|g) Cartesian block
-__constant__ double c_c2s[C2S_TOTAL];
-__constant__ int c_c2s_off[GLC + 1];
-
-struct DShells {
-  int nshell;
-  const int* l;
-  const int* nprim;
-  const int64_t* prim_off;
-  const double* exps;
-  const double* coefs;
-  const double* centers;
-  const int64_t* fun_off;
-};
-
-__device__ __forceinline__ int ncart_d(int l) { return (l + 1) * (l + 2) / 2; }
-__device__ __forceinline__ int tet(int t, int u, int v) {
-  const int s = t + u + v, w = u + v;
-  return s * (s + 1) * (s + 2) / 6 + w * (w + 1) / 2 + v;
-}
-// Cartesian component c of l, ordered by descending x power, then descending y:
-// component c lies in row r (x power l - r) with r(r+1)/2 <= c < (r+1)(r+2)/2.
-__device__ __forceinline__ void cart_ijk(int l, int c, int& i, int& j, int& k) {
-  int r = 0;
-  while ((r + 1) * (r + 2) / 2 <= c) ++r;
-  i = l - r;
-  j = r - (c - r * (r + 1) / 2);
-  k = l - i - j;
-}
-__device__ __forceinline__ double c2s_at(int l, int m, int c) { return c_c2s[c_c2s_off[l] + m * ncart_d(l) + c]; }
-
-// Boys function F_n(T), n = 0..nmax: series at the top order with downward
-// recursion, or the asymptotic F_0 with upward recursion for T > 40.
-__device__ void boys_d(int nmax, double T, double* F) {
-  if (T < 1e-14) {
-    for (int n = 0; n <= nmax; ++n) F[n] = 1.0 / (2 * n + 1);
-    return;
-  }
-  if (T > 40.0) {
-    F[0] = 0.5 * sqrt(3.14159265358979323846 / T);
-    const double e = exp(-T);
-    for (int n = 0; n < nmax; ++n) F[n + 1] = ((2 * n + 1) * F[n] - e) / (2 * T);
-    return;
-  }
-  const double e = exp(-T);
-  double term = 1.0 / (2 * nmax + 1), sum = term;
-  for (int k = 1; k < 400; ++k) {
-    term *= 2 * T / (2 * nmax + 2 * k + 1);
-    sum += term;
-    if (term < 1e-17 * sum) break;
-  }
-  F[nmax] = e * sum;
-  for (int m = nmax; m > 0; --m) F[m - 1] = (2 * T * F[m] + e) / (2 * m - 1);
-}
 
 // 1D Hermite coefficients e[i][j][t] (t <= i + j) of a Gaussian product with
 // exponents a, b and AB = A - B.  i <= GLC covers a lone auxiliary bra shell (j = 0).
@@ -248,43 +188,6 @@ __device__ void ket_to_sph(int nab, int lc, double* cart) {
   }
 }
 
-// 3c2e: task = k_local * npairs + q (shell pair q, auxiliary shell k0 + k_local).
-// out[(P - P0) * npair_fun + nu (nu+1)/2 + mu] for mu <= nu, P0 = first function of shell k0.
-__global__ void __launch_bounds__(64) k_int3c2e(DShells A, DShells Cs, const int* __restrict__ pi,
-                                                const int* __restrict__ pj, int npairs, int64_t npair_fun, int k0,
-                                                int nk, double* __restrict__ out) {
-  const int64_t task = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (task >= (int64_t)npairs * nk) return;
-  const int q = (int)(task % npairs), k = k0 + (int)(task / npairs);
-  const int i = pi[q], j = pj[q];
-  const int la = A.l[i], lb = A.l[j], lc = Cs.l[k];
-  const int na = ncart_d(la), nb = ncart_d(lb), nc = ncart_d(lc);
-  double cart[MAXCART];
-  triple_d(A, i, j, true, Cs, k, cart);
-  ket_to_sph(na * nb, lc, cart);
-  const int sa = 2 * la + 1, sb = 2 * lb + 1, sc = 2 * lc + 1;
-  const int64_t P0 = Cs.fun_off[k0];
-  for (int mc = 0; mc < sc; ++mc) {
-    double* row = out + (Cs.fun_off[k] + mc - P0) * npair_fun;
-    for (int ma = 0; ma < sa; ++ma) {
-      double half[6];  // sum_ca c2s_la[ma][ca] cart[ca][cb][mc]
-      for (int cb = 0; cb < nb; ++cb) {
-        double v = 0.0;
-        for (int ca = 0; ca < na; ++ca) v += c2s_at(la, ma, ca) * cart[(ca * nb + cb) * nc + mc];
-        half[cb] = v;
-      }
-      const int64_t mu = A.fun_off[i] + ma;
-      for (int mb = 0; mb < sb; ++mb) {
-        const int64_t nu = A.fun_off[j] + mb;
-        if (mu > nu) continue;
-        double v = 0.0;
-        for (int cb = 0; cb < nb; ++cb) v += c2s_at(lb, mb, cb) * half[cb];
-        row[nu * (nu + 1) / 2 + mu] = v;
-      }
-    }
-  }
-}
-
 // 2c2e over auxiliary shell pairs k1 <= k2: V (naux x naux, column-major, leading dim ldv).
 __global__ void __launch_bounds__(64) k_int2c2e(DShells Cs, int nshell, int64_t ldv, double* __restrict__ V) {
   const int64_t task = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -315,9 +218,13 @@ struct RiIntPlan {
   DShells A{}, C{};
   std::vector<int64_t> offA, offC;
   int64_t nA = 0, nC = 0;
-  const int* dpi = nullptr;
+  const int* dpi = nullptr;  // shell pairs sorted by (l_i, l_j, primitive count)
   const int* dpj = nullptr;
   int npairs = 0;
+  int pair_cls[10] = {};  // pairs of class la * 3 + lb are [pair_cls[c], pair_cls[c + 1])
+  std::vector<int> aux_sorted;  // auxiliary shells sorted by (l, index)
+  int aux_l_begin[GLC + 2] = {};
+  const int* daux = nullptr;
   ~RiIntPlan() {
     for (void* p : bufs) cudaFree(p);
   }
@@ -373,8 +280,10 @@ int upload_c2s(const double* const* c2s, cudaStream_t st) {
   }
   // earlier launches on this stream may still read the table: order after them
   if (cudaStreamSynchronize(st) != cudaSuccess) return RIJK_ERR_CUDA;
-  if (cudaMemcpyToSymbol(c_c2s, flat.data(), flat.size() * sizeof(double)) != cudaSuccess) return RIJK_ERR_CUDA;
-  if (cudaMemcpyToSymbol(c_c2s_off, off, sizeof(off)) != cudaSuccess) return RIJK_ERR_CUDA;
+  // every translation unit with integral kernels holds its own copy of the table
+  if (upload_tables(flat.data(), off) || int3c_tables_la0(flat.data(), off) || int3c_tables_la1(flat.data(), off) ||
+      int3c_tables_la2(flat.data(), off))
+    return RIJK_ERR_CUDA;
   return RIJK_OK;
 }
 
@@ -387,6 +296,16 @@ int ri_plan_create(const rijk_shells* bas, const rijk_shells* aux, const double*
   RiIntPlan* p = new RiIntPlan();
   int rc = upload_c2s(c2s, st);
   if (rc == RIJK_OK) rc = p->load(aux, GLC, p->C, p->offC, p->nC);
+  if (rc == RIJK_OK) {
+    for (int k = 0; k < p->C.nshell; ++k) p->aux_sorted.push_back(k);
+    std::stable_sort(p->aux_sorted.begin(), p->aux_sorted.end(), [&](int x, int y) { return aux->l[x] < aux->l[y]; });
+    for (int l = 0, t = 0; l <= GLC + 1; ++l) {
+      while (t < p->C.nshell && aux->l[p->aux_sorted[t]] < l) ++t;
+      p->aux_l_begin[l] = t;
+    }
+    p->daux = p->up(p->aux_sorted.data(), p->aux_sorted.size());
+    if (!p->daux) rc = RIJK_ERR_NOMEM;
+  }
   if (rc == RIJK_OK && bas) {
     rc = p->load(bas, GLA, p->A, p->offA, p->nA);
     if (rc == RIJK_OK && (int64_t)p->A.nshell * (p->A.nshell + 1) / 2 > (1ll << 30)) rc = RIJK_ERR_TOO_LARGE;
@@ -397,17 +316,22 @@ int ri_plan_create(const rijk_shells* bas, const rijk_shells* aux, const double*
           pi.push_back(i);
           pj.push_back(j);
         }
+      auto key = [&](int x) {
+        return (int64_t)(bas->l[pi[x]] * 3 + bas->l[pj[x]]) * 4096 + bas->nprim[pi[x]] * bas->nprim[pj[x]];
+      };
       std::vector<int> order(pi.size());
       std::iota(order.begin(), order.end(), 0);
-      std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        return bas->l[pi[x]] * 8 + bas->l[pj[x]] < bas->l[pi[y]] * 8 + bas->l[pj[y]];
-      });
+      std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key(x) < key(y); });
       std::vector<int> si(pi.size()), sj(pi.size());
       for (size_t t = 0; t < order.size(); ++t) {
         si[t] = pi[order[t]];
         sj[t] = pj[order[t]];
       }
       p->npairs = (int)si.size();
+      for (int c = 0, t = 0; c <= 9; ++c) {
+        while (t < p->npairs && bas->l[si[t]] * 3 + bas->l[sj[t]] < c) ++t;
+        p->pair_cls[c] = t;
+      }
       p->dpi = p->up(si.data(), si.size());
       p->dpj = p->up(sj.data(), sj.size());
       if (!p->dpi || !p->dpj) rc = RIJK_ERR_NOMEM;
@@ -435,10 +359,28 @@ void launch_int2c2e(const RiIntPlan* p, double* dV, int64_t ldv, cudaStream_t st
 
 void launch_int3c2e(const RiIntPlan* p, int k0, int k1, double* out, cudaStream_t st) {
   const int64_t npair_fun = p->nA * (p->nA + 1) / 2;
-  const int64_t tasks = (int64_t)p->npairs * (k1 - k0);
-  count_launch();
-  k_int3c2e<<<(unsigned)((tasks + 63) / 64), 64, 0, st>>>(p->A, p->C, p->dpi, p->dpj, p->npairs, npair_fun, k0,
-                                                          k1 - k0, out);
+  const int64_t P0 = p->offC[k0];
+  for (int lc = 0; lc <= GLC; ++lc) {
+    // the shells of [k0, k1) with l = lc are contiguous in the sorted list
+    const int* b = p->aux_sorted.data() + p->aux_l_begin[lc];
+    const int* e = p->aux_sorted.data() + p->aux_l_begin[lc + 1];
+    const int* lo = std::lower_bound(b, e, k0);
+    const int* hi = std::lower_bound(lo, e, k1);
+    const int nkc = (int)(hi - lo);
+    if (nkc == 0) continue;
+    const int* dkc = p->daux + (lo - p->aux_sorted.data());
+    for (int c = 0; c < 9; ++c) {
+      const int npc = p->pair_cls[c + 1] - p->pair_cls[c];
+      if (npc == 0) continue;
+      const int64_t tasks = (int64_t)npc * nkc;
+      count_launch();
+      const Int3cKernel kern = c < 3 ? int3c_kernel_la0(c % 3, lc)
+                               : c < 6 ? int3c_kernel_la1(c % 3, lc)
+                                       : int3c_kernel_la2(c % 3, lc);
+      kern<<<(unsigned)((tasks + 127) / 128), 128, 0, st>>>(
+          p->A, p->C, p->dpi + p->pair_cls[c], p->dpj + p->pair_cls[c], npc, dkc, nkc, npair_fun, P0, out);
+    }
+  }
 }
 
 }  // namespace rijk
