@@ -3,20 +3,34 @@
 Every molecule keeps its fitted tensor in its own device context (its own CUDA
 stream), and the SCF iterations of the whole set advance together:
 
+  integrals    (P|Q), (mu nu|P), metric and fit on the device per molecule
+               (rijk_build_rimatr_from_shells) when the shells fit the device
+               engine, else the host engine;
   J / K        per molecule through the device entry points (rijk_vj_upper_dev,
-               rijk_vk_upper_occ_dev or the split-precision tcgen05 form), the
+               rijk_vk_upper_occ_dev or the split-precision tcgen05 forms), the
                molecules' launches overlapping on their streams;
   Fock, DIIS   on the device for the padded batch: F = h + J + K, the error
-               vectors F D S - S D F of REST's DIIS (src/scf_io/mod.rs:3094-3136),
-               the B-matrix solve of diis_solver (:3138-3188) per molecule;
+               vectors F D S - S D F of REST's DIIS (src/scf_io/mod.rs:3094-3136)
+               kept as a batched history, the B matrices of diis_solver
+               (:3138-3188) formed in one batched product and solved per molecule;
   diagonalise  the generalised eigenproblem F C = S C e of diagonalize_hamiltonian
                (:1843-1873) as one batched symmetric eigensolve of X^T F X
                (X = S^-1/2 per molecule, padding rows pushed to the top of the
                spectrum) on the device;
   density      D = 2 C_occ C_occ^T on the device.
 
-All of it is FP64.  Molecules converge independently (REST's three criteria,
-:1875-1951) and stop being updated once converged.
+Precision of the exchange build:
+  fp64   every K in FP64 (DMMA);
+  mixed  incremental split-precision K: K_k = K_{k-1} + K_split(D_k - D_{k-1}) with
+         the density difference in its exact low-rank form V S V^T (batched thin
+         QR of [Y_k, Y_{k-1}] and an eigendecomposition of the small core, so the
+         split error scales with |dD|), a full FP64 rebuild every
+         ``rebuild_every`` split steps, FP64 builds once the molecule is loosely
+         converged, and convergence only on consecutive FP64 builds, so every
+         reported energy is an FP64 energy;
+  split  every K in split precision (no FP64 finish; for loose criteria only).
+Everything else is FP64.  Molecules converge independently (REST's three
+criteria, :1875-1951) and stop being updated once converged.
 """
 from __future__ import annotations
 
@@ -25,7 +39,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .basis import Molecule, int1e, int2c2e, int3c2e
+from .basis import DEVICE_MAX_L_AO, DEVICE_MAX_L_AUX, int1e, int2c2e, int2c2e_dev, int3c2e
+from .geometry import alkane, water_cluster  # noqa: F401  (re-exported)
 from .rijk import RIJK
 from .scf import metric_inv_sqrt
 
@@ -42,56 +57,69 @@ class BatchResult:
 
 class BatchedRHF:
     def __init__(self, mols: list, basis: str, auxbas: str, device: int = 0, metric: str = "inv_sqrt",
-                 precision: str = "fp64"):
+                 precision: str = "fp64", integrals: str = "auto", rebuild_every: int = 8,
+                 switch_etot: float = 1e-5, switch_rho: float = 1e-4):
         import torch
 
+        if precision not in ("fp64", "mixed", "split"):
+            raise ValueError(f"unknown precision {precision!r}")
+        if metric not in ("inv_sqrt", "cholesky"):
+            raise ValueError(f"unknown metric {metric!r}")
         self.torch = torch
         self.dev = torch.device("cuda", device)
         self.precision = precision
+        self.rebuild_every, self.switch_etot, self.switch_rho = rebuild_every, switch_etot, switch_rho
         t0 = time.perf_counter()
         self.mols = mols
         self.ctx, self.n, self.nocc, self.enuc = [], [], [], []
         hs, ss = [], []
         for mol in mols:
+            if mol.spin != 1 or mol.nelec % 2:
+                raise ValueError("BatchedRHF handles closed-shell molecules")
             bas, aux = mol.shells(basis), mol.shells(auxbas)
             n = bas.nfun
             s = int1e(mol, bas, "ovlp")
             h = int1e(mol, bas, "kinetic") + int1e(mol, bas, "nuclear")
-            v2 = int2c2e(aux)
-            i3 = int3c2e(bas, aux)
             ctx = RIJK(device)
-            if metric == "inv_sqrt":
-                ctx.fit_rimatr(metric_inv_sqrt(v2), i3, n)
+            on_device = integrals == "device" or (
+                integrals == "auto" and int(bas.l.max()) <= DEVICE_MAX_L_AO and int(aux.l.max()) <= DEVICE_MAX_L_AUX)
+            if on_device:
+                factor = metric_inv_sqrt(int2c2e_dev(aux).cpu().numpy()) if metric == "inv_sqrt" else None
+                ctx.build_rimatr_from_shells(bas, aux, factor)
             else:
-                ctx.build_rimatr_cholesky(v2, i3, n)
+                v2, i3 = int2c2e(aux), int3c2e(bas, aux)
+                if metric == "inv_sqrt":
+                    ctx.fit_rimatr(metric_inv_sqrt(v2), i3, n)
+                else:
+                    ctx.build_rimatr_cholesky(v2, i3, n)
             self.ctx.append(ctx)
             self.n.append(n)
-            if mol.spin != 1 or mol.nelec % 2:
-                raise ValueError("BatchedRHF handles closed-shell molecules")
             self.nocc.append(mol.nelec // 2)
             self.enuc.append(mol.nuclear_repulsion())
             hs.append(h)
             ss.append(s)
         self.B = len(mols)
         self.nmax = max(self.n)
+        self.omax = max(self.nocc)
         f64 = torch.float64
         B, nm = self.B, self.nmax
         self.S = torch.zeros(B, nm, nm, dtype=f64, device=self.dev)
         self.H = torch.zeros(B, nm, nm, dtype=f64, device=self.dev)
-        self.X = torch.zeros(B, nm, nm, dtype=f64, device=self.dev)
         for i, (h, s) in enumerate(zip(hs, ss)):
             n = self.n[i]
             self.S[i, :n, :n] = torch.as_tensor(s, device=self.dev)
             self.H[i, :n, :n] = torch.as_tensor(h, device=self.dev)
-            w, u = torch.linalg.eigh(self.S[i, :n, :n])
-            self.X[i, :n, :n] = (u * w.rsqrt()) @ u.T
-        # padded rows of X^T F X get a large diagonal so their eigenvalues come last
-        self.pad_shift = torch.zeros(B, nm, nm, dtype=f64, device=self.dev)
+        # X = S^-1/2 per molecule (identity on the padding), one batched eigensolve
+        pad_eye = torch.zeros(B, nm, nm, dtype=f64, device=self.dev)
         for i in range(B):
             idx = torch.arange(self.n[i], nm, device=self.dev)
-            self.pad_shift[i, idx, idx] = 1.0e6
-        # packed-upper <-> full index maps per size
+            pad_eye[i, idx, idx] = 1.0
+        w, u = torch.linalg.eigh(self.S + pad_eye)
+        self.X = (u * w.rsqrt()[:, None, :]) @ u.transpose(1, 2) - pad_eye
+        # padded rows of X^T F X get a large diagonal so their eigenvalues come last
+        self.pad_shift = 1.0e6 * pad_eye
         self._tri = {}
+        torch.cuda.synchronize()
         self.setup_s = time.perf_counter() - t0
 
     def _tri_idx(self, n):
@@ -107,11 +135,43 @@ class BatchedRHF:
         m[j, i] = u
         return m
 
+    def _delta_factors(self, Y, idx):
+        """For molecules idx: dD = Y Y^T - Yref Yref^T as V S V^T, V = Q U |lam|^1/2
+        with positive columns first (batched thin QR + eigensolve of the 2o x 2o core)."""
+        torch = self.torch
+        om = self.omax
+        Yn = Y[idx]
+        Yr = torch.stack([self._yref[i] for i in idx])
+        W = torch.cat([Yn, Yr], dim=2)
+        Q, R = torch.linalg.qr(W)
+        sgn = torch.cat([torch.ones(om, dtype=W.dtype, device=self.dev), -torch.ones(om, dtype=W.dtype, device=self.dev)])
+        M = (R * sgn[None, None, :]) @ R.transpose(1, 2)
+        lam, U = torch.linalg.eigh(M)
+        lam_h = lam.cpu().numpy()
+        out = {}
+        for b, i in enumerate(idx):
+            lb = lam_h[b]
+            big = np.max(np.abs(lb)) if lb.size else 0.0
+            keep = np.nonzero(np.abs(lb) > 1e-14 * max(big, 1e-300))[0]
+            keep = keep[np.argsort(-lb[keep])]
+            if keep.size == 0:
+                out[i] = (None, 0)
+                continue
+            kt = torch.as_tensor(keep, device=self.dev)
+            sq = torch.as_tensor(np.sqrt(np.abs(lb[keep])), dtype=W.dtype, device=self.dev)
+            V = (Q[b] @ U[b][:, kt]) * sq[None, :]
+            out[i] = (V[:self.n[i]], int(np.sum(lb[keep] > 0)))
+        return out
+
     def _jk(self, C, active):
         """J + K (full, padded batch) for the active molecules from their orbitals."""
         torch = self.torch
-        B, nm = self.B, self.nmax
+        B, nm, om = self.B, self.nmax, self.omax
         out = torch.zeros(B, nm, nm, dtype=torch.float64, device=self.dev)
+        Y = np.sqrt(2.0) * C[:, :, :om] * self._occ_mask[:, None, :om]  # D = Y Y^T
+        incr = [self.precision == "mixed" and active[i] and self._kref[i] is not None and not self._fp64_now[i]
+                and self._split_steps[i] < self.rebuild_every for i in range(B)]
+        factors = self._delta_factors(Y, [i for i in range(B) if incr[i]]) if any(incr) else {}
         cur = torch.cuda.current_stream()
         ev = torch.cuda.Event()
         ev.record(cur)
@@ -125,22 +185,45 @@ class BatchedRHF:
             with torch.cuda.stream(st):
                 c = C[i, :n, :o]
                 d = 2.0 * (c @ c.T)
-                c_cm = c.T.contiguous()  # column-major n x o
-                occ = torch.full((o,), 2.0, dtype=torch.float64, device=self.dev)
                 npair = n * (n + 1) // 2
                 vj = torch.empty(npair, dtype=torch.float64, device=self.dev)
-                vk = torch.empty(npair, dtype=torch.float64, device=self.dev)
                 ctx.vj_upper_dev(d.contiguous().data_ptr(), 1, 1.0, 1, vj.data_ptr(), ctx.stream)
-                if self.precision == "split":
-                    ctx.vk_upper_occ_split_dev(c_cm.data_ptr(), o, [o - 1], occ.data_ptr(), 1, -0.5, vk.data_ptr(),
-                                               ctx.stream)
+                keep = [d, vj]
+                if incr[i]:
+                    vk = self._kref[i].clone()
+                    V, npos = factors[i]
+                    if V is not None:
+                        ld = n + (n & 1)
+                        buf = torch.zeros(V.shape[1], ld, dtype=torch.float64, device=self.dev)
+                        buf[:, :n] = V.T
+                        ctx.vk_upper_lowrank_split_dev(buf.data_ptr(), ld, V.shape[1], npos, -0.5, True,
+                                                       vk.data_ptr(), ctx.stream)
+                        keep.append(buf)
+                    self._split_steps[i] += 1
+                    self._nsplit[i] += 1
+                    self._streak[i] = 0
                 else:
-                    ctx.vk_upper_occ_dev(c_cm.data_ptr(), o, [o - 1], occ.data_ptr(), 1, -0.5, vk.data_ptr(),
-                                         ctx.stream)
+                    c_cm = c.T.contiguous()  # column-major n x o
+                    occ = torch.full((o,), 2.0, dtype=torch.float64, device=self.dev)
+                    vk = torch.empty(npair, dtype=torch.float64, device=self.dev)
+                    if self.precision == "split":
+                        ctx.vk_upper_occ_split_dev(c_cm.data_ptr(), o, [o - 1], occ.data_ptr(), 1, -0.5,
+                                                   vk.data_ptr(), ctx.stream)
+                        self._nsplit[i] += 1
+                    else:
+                        ctx.vk_upper_occ_dev(c_cm.data_ptr(), o, [o - 1], occ.data_ptr(), 1, -0.5, vk.data_ptr(),
+                                             ctx.stream)
+                        self._nfp64[i] += 1
+                        self._streak[i] += 1
+                    self._split_steps[i] = 0
+                    keep += [c_cm, occ]
+                if self.precision == "mixed":
+                    self._kref[i] = vk
+                    self._yref[i] = Y[i].clone()
                 out[i, :n, :n] = self._upper_to_full(vj + vk, n)
                 done = torch.cuda.Event()
                 done.record(st)
-                parts.append((done, d, c_cm, occ, vj, vk))
+                parts.append((done, keep, vk))
         for done, *_ in parts:
             cur.wait_event(done)
         return out
@@ -150,11 +233,16 @@ class BatchedRHF:
         torch = self.torch
         t0 = time.perf_counter()
         B, nm = self.B, self.nmax
-        enuc = torch.tensor(self.enuc, dtype=torch.float64, device=self.dev)
-        ns = torch.tensor(self.n, dtype=torch.float64, device=self.dev)
-        nocc_mask = torch.zeros(B, nm, dtype=torch.float64, device=self.dev)
+        f64 = torch.float64
+        enuc = torch.tensor(self.enuc, dtype=f64, device=self.dev)
+        ns = torch.tensor(self.n, dtype=f64, device=self.dev)
+        self._occ_mask = torch.zeros(B, nm, dtype=f64, device=self.dev)
         for i in range(B):
-            nocc_mask[i, :self.nocc[i]] = 1.0
+            self._occ_mask[i, :self.nocc[i]] = 1.0
+        self._kref, self._yref = [None] * B, [None] * B
+        self._split_steps, self._nsplit, self._nfp64, self._streak = [0] * B, [0] * B, [0] * B, [0] * B
+        self._fp64_now = [self.precision != "mixed"] * B
+        nmask = torch.arange(nm, device=self.dev)[None, :] < ns[:, None]
 
         def diag(F):
             fp = self.X.transpose(1, 2) @ F @ self.X + self.pad_shift
@@ -162,91 +250,117 @@ class BatchedRHF:
             return e, self.X @ cp
 
         def density(C):
-            co = C * nocc_mask[:, None, :]
+            co = C * self._occ_mask[:, None, :]
             return 2.0 * co @ co.transpose(1, 2)
 
         active = [True] * B
         e, C = diag(self.H)  # hcore guess
         D = density(C)
         F = self.H + self._jk(C, active)
-        energy = enuc + 0.5 * ((D * (self.H + F)).sum(dim=(1, 2)))
-        e_prev, D_prev, E_prev = e, D, energy
-        errs, targets = [[] for _ in range(B)], [[] for _ in range(B)]
+        E_prev = enuc + 0.5 * ((D * (self.H + F)).sum(dim=(1, 2)))
+        e_prev = e
+        # DIIS history as a ring buffer per molecule
+        m = num_max_diis
+        err_hist = torch.zeros(B, m, nm * nm, dtype=f64, device=self.dev)
+        f_hist = torch.zeros(B, m, nm, nm, dtype=f64, device=self.dev)
+        count = [0] * B
         iters = [0] * B
         conv = [False] * B
         for it in range(1, max_cycle + 1):
-            # DIIS extrapolation of F per molecule (error F D S - S D F)
             err = F @ D @ self.S
             err = err - err.transpose(1, 2)
-            Fx = F.clone()
+            act = torch.tensor(active, device=self.dev)
+            slot = torch.tensor([count[i] % m for i in range(B)], device=self.dev)
+            rows = torch.arange(B, device=self.dev)
+            err_hist[rows[act], slot[act]] = err[act].reshape(int(act.sum()), -1)
+            f_hist[rows[act], slot[act]] = F[act]
             for i in range(B):
-                if not active[i]:
+                if active[i]:
+                    count[i] += 1
+            bm = (err_hist @ err_hist.transpose(1, 2)).cpu().numpy()
+            coef = np.zeros((B, m))
+            for i in range(B):
+                k = min(count[i], m)
+                if not active[i] or k == 0:
                     continue
-                if len(errs[i]) == num_max_diis:
-                    errs[i].pop(0)
-                    targets[i].pop(0)
-                errs[i].append(err[i].reshape(-1))
-                targets[i].append(F[i])
-                E = torch.stack(errs[i])
-                bm = (E @ E.T).cpu().numpy()
                 try:
-                    binv = np.linalg.inv(bm)
-                    coef = binv.sum(axis=1) / binv.sum()
-                    Fx[i] = sum(float(c) * t for c, t in zip(coef, targets[i]))
+                    binv = np.linalg.inv(bm[i, :k, :k])
+                    if not np.all(np.isfinite(binv)):
+                        raise np.linalg.LinAlgError
+                    coef[i, :k] = binv.sum(axis=1) / binv.sum()
                 except np.linalg.LinAlgError:
-                    errs[i], targets[i] = [], []
+                    # singular B: restart the history from the newest Fock matrix
+                    last = (count[i] - 1) % m
+                    err_hist[i, 0] = err_hist[i, last].clone()
+                    f_hist[i, 0] = f_hist[i, last].clone()
+                    err_hist[i, 1:] = 0.0
+                    f_hist[i, 1:] = 0.0
+                    count[i] = 1
+                    coef[i, 0] = 1.0
+            Fx = torch.einsum("bm,bmij->bij", torch.as_tensor(coef, device=self.dev), f_hist)
+            Fx = torch.where(act[:, None, None], Fx, F)
             e, C = diag(Fx)
             Dn = density(C)
             Fn = self.H + self._jk(C, active)
             En = enuc + 0.5 * ((Dn * (self.H + Fn)).sum(dim=(1, 2)))
             de = (En - E_prev).abs()
             ddm = ((Dn - D).pow(2).sum(dim=(1, 2))).sqrt() / ns
-            nmask = torch.arange(nm, device=self.dev)[None, :] < ns[:, None]
             deev = (((e - e_prev) * nmask).pow(2).sum(dim=1)).sqrt()
             de_h, ddm_h, deev_h = de.cpu().numpy(), ddm.cpu().numpy(), deev.cpu().numpy()
+            newly = []
             for i in range(B):
-                if active[i]:
-                    iters[i] = it
-                    if de_h[i] <= acc_etot and ddm_h[i] <= acc_rho and deev_h[i] <= acc_eev:
-                        conv[i] = True
-                        active[i] = False
-            upd = torch.tensor([1.0 if (a or conv[i] and iters[i] == it) else 0.0 for i, a in enumerate(active)],
-                               dtype=torch.float64, device=self.dev)[:, None, None]
-            F = upd * Fn + (1 - upd) * F
-            D = upd * Dn + (1 - upd) * D
-            E_prev = torch.where(upd[:, 0, 0] > 0, En, E_prev)
-            e_prev = torch.where(upd[:, :, 0] > 0, e, e_prev)
+                if not active[i]:
+                    continue
+                iters[i] = it
+                ok = de_h[i] <= acc_etot and ddm_h[i] <= acc_rho and deev_h[i] <= acc_eev
+                if self.precision == "mixed":
+                    ok = ok and self._streak[i] >= 2
+                    if not self._fp64_now[i] and de_h[i] <= self.switch_etot and ddm_h[i] <= self.switch_rho:
+                        self._fp64_now[i] = True
+                if ok:
+                    conv[i] = True
+                    newly.append(i)
+            upd = torch.tensor([1.0 if active[i] else 0.0 for i in range(B)], dtype=f64, device=self.dev)
+            F = torch.where(upd[:, None, None] > 0, Fn, F)
+            D = torch.where(upd[:, None, None] > 0, Dn, D)
+            E_prev = torch.where(upd > 0, En, E_prev)
+            e_prev = torch.where(upd[:, None] > 0, e, e_prev)
+            for i in newly:
+                active[i] = False
             if not any(active):
                 break
         torch.cuda.synchronize()
         scf_s = time.perf_counter() - t0
-        return BatchResult([float(x) for x in E_prev.cpu()], conv, iters, self.setup_s, scf_s)
+        timings = {"fp64_k_builds": list(self._nfp64), "split_k_builds": list(self._nsplit)}
+        return BatchResult([float(x) for x in E_prev.cpu()], conv, iters, self.setup_s, scf_s, timings)
 
     def close(self):
         for c in self.ctx:
             c.close()
+        self.ctx = []
 
 
-def water_cluster(k: int, seed: int) -> Molecule:
-    """(H2O)_k: O atoms by seeded rejection sampling in a cube of side 3.1 k^(1/3) A
-    with min O-O 2.7 A; each water at the gas-phase geometry (0.9572 A, 104.52 deg)
-    with a uniformly random orientation."""
-    rng = np.random.default_rng(seed)
-    side = 3.1 * k ** (1.0 / 3.0)
-    oxy = []
-    while len(oxy) < k:
-        p = rng.uniform(0.0, side, 3)
-        if all(np.linalg.norm(p - q) >= 2.7 for q in oxy):
-            oxy.append(p)
-    r, ang = 0.9572, np.deg2rad(104.52)
-    local = np.array([[0.0, 0.0, 0.0], [r * np.sin(ang / 2), r * np.cos(ang / 2), 0.0],
-                      [-r * np.sin(ang / 2), r * np.cos(ang / 2), 0.0]])
-    symbols, coords = [], []
-    for o in oxy:
-        q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
-        if np.linalg.det(q) < 0:
-            q[:, 0] = -q[:, 0]
-        for sym, x in zip(["O", "H", "H"], local @ q.T + o):
-            symbols.append(sym)
-            coords.append(x)
-    return Molecule.from_angstrom(symbols, np.array(coords))
+def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, device: int = 0,
+                     **kw) -> BatchResult:
+    """Converge a molecule set in groups of ``group_size`` molecules of similar
+    size (sorted by basis size so that padding stays small); the groups run one
+    after another on the device, results come back in the input order."""
+    run_kw = {k: kw.pop(k) for k in ("max_cycle", "acc_etot", "acc_rho", "acc_eev", "num_max_diis") if k in kw}
+    sizes = [m.shells(basis).nfun for m in mols]
+    order = sorted(range(len(mols)), key=lambda i: sizes[i])
+    energies, conv, iters = [None] * len(mols), [False] * len(mols), [0] * len(mols)
+    nfp64, nsplit = [0] * len(mols), [0] * len(mols)
+    setup = scf = 0.0
+    for g0 in range(0, len(order), group_size):
+        idx = order[g0:g0 + group_size]
+        b = BatchedRHF([mols[i] for i in idx], basis, auxbas, device=device, **kw)
+        try:
+            r = b.run(**run_kw)
+        finally:
+            b.close()
+        setup += r.setup_s
+        scf += r.scf_s
+        for j, i in enumerate(idx):
+            energies[i], conv[i], iters[i] = r.energies[j], r.converged[j], r.iterations[j]
+            nfp64[i], nsplit[i] = r.timings["fp64_k_builds"][j], r.timings["split_k_builds"][j]
+    return BatchResult(energies, conv, iters, setup, scf, {"fp64_k_builds": nfp64, "split_k_builds": nsplit})
