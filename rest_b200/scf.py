@@ -58,6 +58,17 @@ def metric_inv_sqrt(v: np.ndarray, threshold: float = AUXBAS_THRESHOLD) -> np.nd
     return np.asfortranarray((u[:, keep] * lam[keep] ** -0.5) @ u[:, keep].T)
 
 
+def metric_inv_sqrt_dev(v) -> np.ndarray:
+    """metric_inv_sqrt of a device matrix (torch, FP64): the eigendecomposition and
+    the product run on the device; the factor comes back as a host array."""
+    import torch
+
+    lam, u = torch.linalg.eigh(v)
+    keep = lam >= AUXBAS_THRESHOLD
+    uk = u[:, keep]
+    return np.asfortranarray(((uk * lam[keep].rsqrt()) @ uk.T).cpu().numpy())
+
+
 @dataclass
 class ScfOptions:
     """The [ctrl] keys of REST's input that steer this path (src/ctrl_io/mod.rs)."""
@@ -127,7 +138,7 @@ class SCF:
             # integrals, metric and fit on the device; V^-1/2 needs V on the host
             factor = None
             if self.opts.metric == "inv_sqrt":
-                factor = metric_inv_sqrt(int2c2e_dev(self.aux).cpu().numpy())
+                factor = metric_inv_sqrt_dev(int2c2e_dev(self.aux))
             t2 = time.perf_counter()
             self.ctx.build_rimatr_from_shells(self.bas, self.aux, factor)
         else:

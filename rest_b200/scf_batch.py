@@ -42,7 +42,7 @@ import numpy as np
 from .basis import DEVICE_MAX_L_AO, DEVICE_MAX_L_AUX, int1e, int2c2e, int2c2e_dev, int3c2e
 from .geometry import alkane, water_cluster  # noqa: F401  (re-exported)
 from .rijk import RIJK
-from .scf import metric_inv_sqrt
+from .scf import metric_inv_sqrt, metric_inv_sqrt_dev
 
 
 @dataclass
@@ -84,7 +84,7 @@ class BatchedRHF:
             on_device = integrals == "device" or (
                 integrals == "auto" and int(bas.l.max()) <= DEVICE_MAX_L_AO and int(aux.l.max()) <= DEVICE_MAX_L_AUX)
             if on_device:
-                factor = metric_inv_sqrt(int2c2e_dev(aux).cpu().numpy()) if metric == "inv_sqrt" else None
+                factor = metric_inv_sqrt_dev(int2c2e_dev(aux)) if metric == "inv_sqrt" else None
                 ctx.build_rimatr_from_shells(bas, aux, factor)
             else:
                 v2, i3 = int2c2e(aux), int3c2e(bas, aux)
@@ -341,10 +341,12 @@ class BatchedRHF:
 
 
 def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, device: int = 0,
-                     **kw) -> BatchResult:
+                     metric: str = "cholesky", **kw) -> BatchResult:
     """Converge a molecule set in groups of ``group_size`` molecules of similar
     size (sorted by basis size so that padding stays small); the groups run one
-    after another on the device, results come back in the input order."""
+    after another on the device, results come back in the input order.  The
+    metric defaults to the device Cholesky fit (no host eigendecomposition)."""
+    kw["metric"] = metric
     run_kw = {k: kw.pop(k) for k in ("max_cycle", "acc_etot", "acc_rho", "acc_eev", "num_max_diis") if k in kw}
     sizes = [m.shells(basis).nfun for m in mols]
     order = sorted(range(len(mols)), key=lambda i: sizes[i])
