@@ -258,6 +258,31 @@ int rijk_int3c2e_dev(const rijk_shells* bas, const rijk_shells* aux, const doubl
 int rijk_build_rimatr_from_shells(rijk_ctx* ctx, const rijk_shells* bas, const rijk_shells* aux,
                                   const double* const* c2s, const double* metric_factor, int64_t* failed_pivot);
 
+/* ---- learned initial guess: per-atom-pair MLP kernels ----------------------------
+ * No counterpart in REST, whose guesses (src/initial_guess/mod.rs) remain the
+ * fallback of the driver that uses them.  Device pointers; BF16 values are
+ * passed as uint16_t bit patterns; matrices are row-major; act 0 = identity,
+ * 1 = SiLU.  Launches are asynchronous on `stream`.
+ * Forward of one layer: z = x w^T + bias (m x n, FP32 accumulation), y = act(z);
+ * any of z (FP32), y_bf16, y_f32 may be NULL but not all. */
+int rijk_mlp_linear_fwd(const uint16_t* x, const uint16_t* w, const float* bias, int64_t m, int64_t k, int64_t n,
+                        int act, float* z, uint16_t* y_bf16, float* y_f32, void* stream);
+/* Backward of one layer from dy = dL/dy (m x n, FP32) and the forward's z:
+ * dz = dy * act'(z) (into dz_scratch, BF16, m x n), dw = dz^T x (n x k, FP32),
+ * db = column sums of the FP32 dz (n, may be NULL), dx = dz w (m x k, FP32, may be NULL).
+ * dw, db, dx are overwritten (the split-k sums use FP32 atomics). */
+int rijk_mlp_linear_bwd(const uint16_t* x, const uint16_t* w, const float* z, const float* dy, int64_t m, int64_t k,
+                        int64_t n, int act, uint16_t* dz_scratch, float* dw, float* db, float* dx, void* stream);
+/* loss += sum_e (mask_e (y_e - t_e))^2 / norm; dy_e = 2 mask_e (y_e - t_e) / norm
+ * (mask may be NULL = all ones; loss may be NULL). */
+int rijk_mlp_masked_mse(const float* y, const float* t, const float* mask, int64_t count, double norm, float* dy,
+                        float* loss, void* stream);
+/* Adam step `step` (1-based) on FP32 master weights w with moments m, v; the
+ * BF16 copy w_bf16 (may be NULL) is refreshed. */
+int rijk_mlp_adam(float* w, uint16_t* w_bf16, const float* g, float* m, float* v, int64_t count, double lr,
+                  double beta1, double beta2, double eps, int64_t step, void* stream);
+int rijk_mlp_to_bf16(const float* src, uint16_t* dst, int64_t count, void* stream);
+
 /* ---- MO-basis three-centre tensor -------------------------------------------- */
 /* generate_ri3mo_rayon / ao2mo_rayon (src/scf_io/mod.rs:2331-2359, :3270-3307):
  * ri3mo[P, a, i] = sum_{mu,nu} C[mu, a] B_P[mu, nu] C[nu, i] for a in

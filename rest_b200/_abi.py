@@ -130,6 +130,26 @@ SIGNATURES = {
         C.c_int,
         [_ctxp, C.POINTER(RijkShells), C.POINTER(RijkShells), C.c_void_p, C.c_void_p, _i64p],
     ),
+    "rijk_mlp_linear_fwd": (
+        C.c_int,
+        [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_void_p, C.c_void_p,
+         C.c_void_p, C.c_void_p],
+    ),
+    "rijk_mlp_linear_bwd": (
+        C.c_int,
+        [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_void_p,
+         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    ),
+    "rijk_mlp_masked_mse": (
+        C.c_int,
+        [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p],
+    ),
+    "rijk_mlp_adam": (
+        C.c_int,
+        [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_double, C.c_double,
+         C.c_double, C.c_double, C.c_int64, C.c_void_p],
+    ),
+    "rijk_mlp_to_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
 }
 
 

@@ -110,6 +110,23 @@ int cuda_fail(rijk_ctx* c, cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);  \
   } while (0)
 
+// Frees the scratch only the metric step and the fit use (once per geometry):
+// the metric, its factor and inverse, the fit's output panel and large staging.
+int release_fit_scratch(rijk_ctx* ctx) {
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (DevBuf* b : {&ctx->mV, &ctx->mLinv, &ctx->mT, &ctx->mLinvd, &ctx->mOut}) {
+    if (b->p) cudaFree(b->p);
+    b->p = nullptr;
+    b->bytes = 0;
+  }
+  if (ctx->stage.bytes > ((size_t)256 << 20)) {
+    cudaFree(ctx->stage.p);
+    ctx->stage.p = nullptr;
+    ctx->stage.bytes = 0;
+  }
+  return RIJK_OK;
+}
+
 int ensure(rijk_ctx* ctx, DevBuf& b, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (b.bytes >= bytes) return RIJK_OK;
@@ -667,7 +684,7 @@ int cholesky_fit(rijk_ctx* ctx, int64_t* failed_pivot) {
   RIJK_TRY(fit_in_place(ctx, Linv, np, 1, 2));
   RIJK_TRY(sync_and_check(ctx, ctx->stream));
   ctx->have = true;
-  return RIJK_OK;
+  return release_fit_scratch(ctx);
 }
 
 struct PlanGuard {
@@ -735,7 +752,8 @@ int rijk_build_rimatr_from_shells(rijk_ctx* ctx, const rijk_shells* bas, const r
   const Geom& g = ctx->g;
   // three-centre rows, a run of auxiliary shells at a time, packed as they come;
   // large runs keep every class kernel's grid wide
-  const size_t chunk_bytes = std::max<size_t>(ctx->scratch_budget / 2, (size_t)9 * g.npair * 8);
+  const size_t chunk_bytes = std::max<size_t>(std::min<size_t>(ctx->scratch_budget / 2, (size_t)naux * g.npair * 8),
+                                              (size_t)9 * g.npair * 8);
   RIJK_TRY(ensure(ctx, ctx->stage, std::max<size_t>(chunk_bytes, (size_t)naux * naux * 8)));
   double* st = static_cast<double*>(ctx->stage.p);
   const int nsh = rijk::ri_plan_aux_shells(pg.p);
@@ -759,7 +777,7 @@ int rijk_build_rimatr_from_shells(rijk_ctx* ctx, const rijk_shells* bas, const r
     RIJK_TRY(fit_in_place(ctx, static_cast<double*>(ctx->mV.p), npad, 0, 0));
     RIJK_TRY(sync_and_check(ctx, ctx->stream));
     ctx->have = true;
-    return RIJK_OK;
+    return release_fit_scratch(ctx);
   }
   RIJK_TRY(ensure(ctx, ctx->mV, (size_t)npad * npad * 8));
   rijk::launch_int2c2e(pg.p, st, naux, ctx->stream);
@@ -779,7 +797,7 @@ int rijk_fit_rimatr(rijk_ctx* ctx, const double* metric_factor, const double* in
   RIJK_TRY(fit_in_place(ctx, static_cast<double*>(ctx->mV.p), np, 0, 0));
   RIJK_TRY(sync_and_check(ctx, ctx->stream));
   ctx->have = true;
-  return RIJK_OK;
+  return release_fit_scratch(ctx);
 }
 
 // ---- J ------------------------------------------------------------------------

@@ -1,0 +1,447 @@
+"""Learned initial guess: a per-atom-pair MLP that predicts AO density blocks.
+
+For every ordered atom pair (A, B) closer than 6 A, the network maps features
+of the pair and its surroundings to the density block D[AO(A), AO(B)] written
+in the local frame of A's water molecule; the predicted blocks are rotated
+back, symmetrised and assembled into the AO density that starts the SCF.
+
+  frame       per water: origin O, axes p = unit(OH1 - OH2), b = unit(OH1 + OH2),
+              n = p x b (rows of F); a block in the frame is G_A^T D_AB G_B with
+              G_X the block-diagonal rotation of X's shells (real solid
+              harmonics of l = 0, 1, 2 under r -> F^T r, from exact
+              polynomial fits on sample points);
+  features    element one-hots, B and B's water atoms in A's frame, A in its own
+              frame, and Gaussian radial counts of O and H neighbours of A and of
+              B (8 + 8 each, smooth 6 A cutoff): 53 numbers, standardised;
+  network     53 -> 256 -> 256 -> 256 -> 256 -> 196 (SiLU), BF16 weights and
+              activations with FP32 accumulation; output = the 14 x 14 block
+              (O: 14 functions, H: 5 in def2-SVP; unused entries masked),
+              standardised per element pair and entry;
+  kernels     forward, backward, masked MSE and Adam are the library's own
+              (rijk_mlp_*); torch only holds the device memory;
+  fallback    a prediction whose electron count tr(D S) is off by more than 5 %
+              (or not finite) is dropped for REST's own guess (hcore here).
+
+REST has no learned guess: its guesses (src/initial_guess/mod.rs) are the fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from ._abi import RijkError, lib
+from .basis import ANG, cart_components, solid_harmonic_c2s
+
+CUTOFF = 6.0  # A
+NFEAT = 53
+BLOCK = 14
+HIDDEN = 256
+LAYERS = [NFEAT, HIDDEN, HIDDEN, HIDDEN, HIDDEN, BLOCK * BLOCK]
+ELEMENT = {"O": 0, "H": 1}
+RAD_MU = np.linspace(1.0, 6.0, 8)
+RAD_SIGMA = 0.5
+DEFAULT_WEIGHTS = Path(__file__).resolve().parent / "data" / "guess_h2o_def2svp.npz"
+
+
+# ---------------------------------------------------------------------------
+# geometry: frames, shell rotations, atom blocks
+# ---------------------------------------------------------------------------
+def _harmonics(l: int, u: np.ndarray) -> np.ndarray:
+    """Real solid harmonics of degree l at points u (S x 3): S x (2l+1)."""
+    mono = np.stack([u[:, 0] ** i * u[:, 1] ** j * u[:, 2] ** k for i, j, k in cart_components(l)], axis=1)
+    return mono @ solid_harmonic_c2s(l).T
+
+
+_SAMPLES = np.random.default_rng(12345).standard_normal((40, 3))
+
+
+def shell_rotation(l: int, F: np.ndarray) -> np.ndarray:
+    """G with Y_l(F^T u) = G Y_l(u) for all u (exact: both sides are degree-l
+    harmonic polynomials, fitted on 40 points)."""
+    if l == 0:
+        return np.ones((1, 1))
+    y_loc = _harmonics(l, _SAMPLES)
+    y_rot = _harmonics(l, _SAMPLES @ F)  # rows: F^T u_s
+    gt, *_ = np.linalg.lstsq(y_loc, y_rot, rcond=None)
+    return gt.T
+
+
+def water_frames(mol):
+    """Per water (atoms 3w, 3w+1, 3w+2 = O, H1, H2): origin (A) and frame F (rows)."""
+    xyz = np.asarray(mol.coords) * ANG
+    nw = len(mol.symbols) // 3
+    if [s for s in mol.symbols] != ["O", "H", "H"] * nw:
+        raise ValueError("the learned guess is trained on water clusters (atoms ordered O, H, H per water)")
+    frames = []
+    for w in range(nw):
+        o, h1, h2 = xyz[3 * w], xyz[3 * w + 1], xyz[3 * w + 2]
+        p = (h1 - o) - (h2 - o)
+        b = (h1 - o) + (h2 - o)
+        p /= np.linalg.norm(p)
+        b -= (b @ p) * p
+        b /= np.linalg.norm(b)
+        frames.append((o, np.stack([p, b, np.cross(p, b)])))
+    return xyz, frames
+
+
+def atom_layout(sh):
+    """Per atom: (first AO, number of AOs, tuple of shell l)."""
+    layout = {}
+    off = 0
+    for l, a in zip(sh.l, sh.atom):
+        a = int(a)
+        if a not in layout:
+            layout[a] = [off, 0, []]
+        if layout[a][0] + layout[a][1] != off:
+            raise ValueError("shells of an atom must be contiguous")
+        layout[a][1] += 2 * int(l) + 1
+        layout[a][2].append(int(l))
+        off += 2 * int(l) + 1
+    return {a: (v[0], v[1], tuple(v[2])) for a, v in layout.items()}
+
+
+def atom_rotation(shell_ls, rots) -> np.ndarray:
+    n = sum(2 * l + 1 for l in shell_ls)
+    g = np.zeros((n, n))
+    o = 0
+    for l in shell_ls:
+        g[o:o + 2 * l + 1, o:o + 2 * l + 1] = rots[l]
+        o += 2 * l + 1
+    return g
+
+
+def _radial(d: np.ndarray) -> np.ndarray:
+    """Gaussian radial counts with a smooth cutoff: d (...,) -> (..., 8)."""
+    fc = np.where(d < CUTOFF, 0.5 * (np.cos(np.pi * d / CUTOFF) + 1.0), 0.0)
+    return np.exp(-((d[..., None] - RAD_MU) ** 2) / RAD_SIGMA ** 2) * fc[..., None]
+
+
+@dataclass
+class PairSet:
+    feats: np.ndarray  # (P, NFEAT)
+    pairs: np.ndarray  # (P, 2) atom indices (A, B)
+    kind: np.ndarray  # (P,) 2 * type(A) + type(B)
+
+
+def pair_features(mol) -> PairSet:
+    xyz, frames = water_frames(mol)
+    na = len(mol.symbols)
+    typ = np.array([ELEMENT[s] for s in mol.symbols])
+    d = np.linalg.norm(xyz[:, None] - xyz[None], axis=-1)
+    env = np.zeros((na, 16))
+    for a in range(na):
+        others = np.arange(na) != a
+        for t in (0, 1):
+            sel = others & (typ == t)
+            env[a, 8 * t:8 * t + 8] = _radial(d[a, sel]).sum(axis=0)
+    A, B = np.nonzero(d <= CUTOFF)
+    feats = np.zeros((len(A), NFEAT))
+    for p, (a, b) in enumerate(zip(A, B)):
+        wa, wb = a // 3, b // 3
+        o, F = frames[wa]
+        f = [np.eye(2)[typ[a]], np.eye(2)[typ[b]]]
+        db = F @ (xyz[b] - xyz[a])
+        f += [db, [np.linalg.norm(db)], [1.0 if wa == wb else 0.0]]
+        f += [F @ (xyz[3 * wb + j] - xyz[a]) for j in range(3)]
+        f += [F @ (xyz[a] - o), env[a], env[b]]
+        feats[p] = np.concatenate(f)
+    return PairSet(feats, np.stack([A, B], axis=1), 2 * typ[A] + typ[B])
+
+
+class Rotator:
+    """G_X(F_w): rotation of atom X's AO block into the frame of water w (cached)."""
+
+    def __init__(self, mol, sh):
+        self.frames = [F for _, F in water_frames(mol)[1]]
+        self.layout = atom_layout(sh)
+        self._shell = {}
+        self._atom = {}
+
+    def __call__(self, atom: int, w: int) -> np.ndarray:
+        key = (atom, w)
+        if key not in self._atom:
+            if w not in self._shell:
+                self._shell[w] = {l: shell_rotation(l, self.frames[w]) for l in range(3)}
+            self._atom[key] = atom_rotation(self.layout[atom][2], self._shell[w])
+        return self._atom[key]
+
+
+def local_blocks(mol, sh, D: np.ndarray, ps: PairSet):
+    """Targets: G_A^T D_AB G_B in A's water frame, padded to 14 x 14, with masks."""
+    rot = Rotator(mol, sh)
+    lay = rot.layout
+    T = np.zeros((len(ps.pairs), BLOCK * BLOCK))
+    M = np.zeros_like(T)
+    for p, (a, b) in enumerate(ps.pairs):
+        w = a // 3
+        oa, na_, _ = lay[a]
+        ob, nb_, _ = lay[b]
+        blk = rot(a, w).T @ D[oa:oa + na_, ob:ob + nb_] @ rot(b, w)
+        t = np.zeros((BLOCK, BLOCK))
+        m = np.zeros((BLOCK, BLOCK))
+        t[:na_, :nb_] = blk
+        m[:na_, :nb_] = 1.0
+        T[p], M[p] = t.ravel(), m.ravel()
+    return T, M
+
+
+def assemble_density(mol, sh, ps: PairSet, blocks: np.ndarray) -> np.ndarray:
+    """Rotate predicted local blocks back, D_AB = G_A B G_B^T, and average the
+    (A, B) and (B, A)^T predictions; pairs beyond the cutoff stay zero."""
+    rot = Rotator(mol, sh)
+    lay = rot.layout
+    n = sh.nfun
+    D = np.zeros((n, n))
+    cnt = np.zeros((n, n))
+    for p, (a, b) in enumerate(ps.pairs):
+        w = a // 3
+        oa, na_, _ = lay[a]
+        ob, nb_, _ = lay[b]
+        full = rot(a, w) @ blocks[p].reshape(BLOCK, BLOCK)[:na_, :nb_] @ rot(b, w).T
+        D[oa:oa + na_, ob:ob + nb_] += full
+        cnt[oa:oa + na_, ob:ob + nb_] += 1.0
+        D[ob:ob + nb_, oa:oa + na_] += full.T
+        cnt[ob:ob + nb_, oa:oa + na_] += 1.0
+    return D / np.maximum(cnt, 1.0)
+
+
+# ---------------------------------------------------------------------------
+# the network on the device (library kernels)
+# ---------------------------------------------------------------------------
+def _ck(st: int, what: str):
+    if st != 0:
+        raise RijkError(st, what)
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class PairMLP:
+    """MLP with FP32 master weights, BF16 working copies and Adam moments, all
+    on the device; every step is a library kernel on torch's current stream."""
+
+    def __init__(self, layers=LAYERS, seed: int = 0, device: int = 0):
+        import torch
+
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        self.layers = list(layers)
+        rng = np.random.default_rng(seed)
+        self.W, self.b, self.Wbf = [], [], []
+        self.mW, self.vW, self.mb, self.vb = [], [], [], []
+        for k, n in zip(self.layers[:-1], self.layers[1:]):
+            lim = np.sqrt(6.0 / (k + n))
+            w = torch.tensor(rng.uniform(-lim, lim, (n, k)), dtype=torch.float32, device=self.dev)
+            self.W.append(w)
+            self.b.append(torch.zeros(n, dtype=torch.float32, device=self.dev))
+            self.Wbf.append(torch.empty(n, k, dtype=torch.int16, device=self.dev))
+            for lst, shape in ((self.mW, (n, k)), (self.vW, (n, k)), (self.mb, (n,)), (self.vb, (n,))):
+                lst.append(torch.zeros(shape, dtype=torch.float32, device=self.dev))
+        self.step = 0
+        self.sync_bf16()
+
+    @property
+    def stream(self):
+        return C.c_void_p(self.torch.cuda.current_stream().cuda_stream)
+
+    def sync_bf16(self):
+        for w, wb in zip(self.W, self.Wbf):
+            _ck(lib().rijk_mlp_to_bf16(_p(w), _p(wb), w.numel(), self.stream), "to_bf16")
+
+    def to_bf16(self, x):
+        out = self.torch.empty(x.shape, dtype=self.torch.int16, device=self.dev)
+        _ck(lib().rijk_mlp_to_bf16(_p(x), _p(out), x.numel(), self.stream), "to_bf16")
+        return out
+
+    def forward(self, xbf, keep: bool = False):
+        """x (m x in, BF16 bits) -> y (m x out, FP32); keep=True also returns the
+        per-layer inputs (BF16) and pre-activations for the backward pass."""
+        torch = self.torch
+        m = xbf.shape[0]
+        h, acts, zs = xbf, [xbf], []
+        nl = len(self.W)
+        y = None
+        for li, (wb, b) in enumerate(zip(self.Wbf, self.b)):
+            n, k = wb.shape
+            last = li == nl - 1
+            z = torch.empty(m, n, dtype=torch.float32, device=self.dev) if keep else None
+            if last:
+                y = torch.empty(m, n, dtype=torch.float32, device=self.dev)
+                _ck(lib().rijk_mlp_linear_fwd(_p(h), _p(wb), _p(b), m, k, n, 0, _p(z), None, _p(y), self.stream),
+                    "linear_fwd")
+            else:
+                hn = torch.empty(m, n, dtype=torch.int16, device=self.dev)
+                _ck(lib().rijk_mlp_linear_fwd(_p(h), _p(wb), _p(b), m, k, n, 1, _p(z), _p(hn), None, self.stream),
+                    "linear_fwd")
+                h = hn
+                acts.append(h)
+            zs.append(z)
+        return (y, acts, zs) if keep else y
+
+    def gradients(self, xbf, target, mask, norm: float):
+        """Loss and per-layer (dW, db) of the masked MSE for one minibatch."""
+        torch = self.torch
+        y, acts, zs = self.forward(xbf, keep=True)
+        m = xbf.shape[0]
+        loss = torch.zeros(1, dtype=torch.float32, device=self.dev)
+        dy = torch.empty_like(y)
+        _ck(lib().rijk_mlp_masked_mse(_p(y), _p(target), _p(mask), y.numel(), float(norm), _p(dy), _p(loss),
+                                      self.stream), "masked_mse")
+        grads = [None] * len(self.W)
+        for li in range(len(self.W) - 1, -1, -1):
+            wb = self.Wbf[li]
+            n, k = wb.shape
+            dz = torch.empty(m, n, dtype=torch.int16, device=self.dev)
+            dw = torch.empty(n, k, dtype=torch.float32, device=self.dev)
+            db = torch.empty(n, dtype=torch.float32, device=self.dev)
+            dx = torch.empty(m, k, dtype=torch.float32, device=self.dev) if li > 0 else None
+            act = 0 if li == len(self.W) - 1 else 1
+            _ck(lib().rijk_mlp_linear_bwd(_p(acts[li]), _p(wb), _p(zs[li]), _p(dy), m, k, n, act, _p(dz), _p(dw),
+                                          _p(db), _p(dx), self.stream), "linear_bwd")
+            grads[li] = (dw, db)
+            dy = dx
+        return loss, grads
+
+    def adam_step(self, grads, lr: float, beta1=0.9, beta2=0.999, eps=1e-8):
+        self.step += 1
+        for li, (dw, db) in enumerate(grads):
+            _ck(lib().rijk_mlp_adam(_p(self.W[li]), _p(self.Wbf[li]), _p(dw), _p(self.mW[li]), _p(self.vW[li]),
+                                    dw.numel(), lr, beta1, beta2, eps, self.step, self.stream), "adam")
+            _ck(lib().rijk_mlp_adam(_p(self.b[li]), None, _p(db), _p(self.mb[li]), _p(self.vb[li]), db.numel(), lr,
+                                    beta1, beta2, eps, self.step, self.stream), "adam")
+
+    def state(self) -> dict:
+        out = {}
+        for i, (w, b) in enumerate(zip(self.W, self.b)):
+            out[f"W{i}"] = w.cpu().numpy()
+            out[f"b{i}"] = b.cpu().numpy()
+        return out
+
+    def load_state(self, st: dict):
+        torch = self.torch
+        for i in range(len(self.W)):
+            self.W[i] = torch.tensor(st[f"W{i}"], dtype=torch.float32, device=self.dev)
+            self.b[i] = torch.tensor(st[f"b{i}"], dtype=torch.float32, device=self.dev)
+        self.sync_bf16()
+
+
+# ---------------------------------------------------------------------------
+# normalisation, training, prediction
+# ---------------------------------------------------------------------------
+@dataclass
+class Normaliser:
+    f_mean: np.ndarray
+    f_std: np.ndarray
+    t_mean: np.ndarray  # (4, 196) per element pair
+    t_std: np.ndarray  # (4, 196)
+
+    @staticmethod
+    def fit(feats, targets, masks, kinds):
+        t_mean = np.zeros((4, BLOCK * BLOCK))
+        t_std = np.ones((4, BLOCK * BLOCK))
+        for k in range(4):
+            sel = kinds == k
+            if sel.any():
+                t_mean[k] = targets[sel].mean(axis=0)
+                t_std[k] = np.maximum(targets[sel].std(axis=0), 1e-3) * masks[sel].max(axis=0) + \
+                    (1.0 - masks[sel].max(axis=0))
+        return Normaliser(feats.mean(axis=0), np.maximum(feats.std(axis=0), 1e-6), t_mean, t_std)
+
+    def feats(self, f):
+        return (f - self.f_mean) / self.f_std
+
+    def targets(self, t, kinds):
+        return (t - self.t_mean[kinds]) / self.t_std[kinds]
+
+    def blocks(self, y, kinds):
+        return y * self.t_std[kinds] + self.t_mean[kinds]
+
+
+def training_arrays(samples, basis: str = "def2-SVP"):
+    """samples: (molecule, converged density) pairs -> features, targets, masks, kinds."""
+    F, T, M, K = [], [], [], []
+    for mol, D in samples:
+        sh = mol.shells(basis)
+        ps = pair_features(mol)
+        t, m = local_blocks(mol, sh, D, ps)
+        F.append(ps.feats)
+        T.append(t)
+        M.append(m)
+        K.append(ps.kind)
+    return np.concatenate(F), np.concatenate(T), np.concatenate(M), np.concatenate(K)
+
+
+def train(samples, epochs: int = 60, batch: int = 4096, lr: float = 1e-3, seed: int = 0, basis: str = "def2-SVP",
+          log=None):
+    """Train the pair MLP on (molecule, converged FP64 density) samples on the device."""
+    import torch
+
+    feats, targets, masks, kinds = training_arrays(samples, basis)
+    norm = Normaliser.fit(feats, targets, masks, kinds)
+    net = PairMLP(seed=seed)
+    dev = net.dev
+    X = net.to_bf16(torch.tensor(norm.feats(feats), dtype=torch.float32, device=dev))
+    Tn = torch.tensor(norm.targets(targets, kinds) * masks, dtype=torch.float32, device=dev)
+    Mk = torch.tensor(masks, dtype=torch.float32, device=dev)
+    P = X.shape[0]
+    rng = np.random.default_rng(seed)
+    history = []
+    for ep in range(epochs):
+        perm = torch.as_tensor(rng.permutation(P), device=dev)
+        tot = torch.zeros(1, dtype=torch.float32, device=dev)
+        lr_ep = lr * 0.5 * (1.0 + np.cos(np.pi * ep / epochs))  # cosine decay
+        for s in range(0, P, batch):
+            idx = perm[s:s + batch]
+            xb, tb, mb = X[idx].contiguous(), Tn[idx].contiguous(), Mk[idx].contiguous()
+            loss, grads = net.gradients(xb, tb, mb, float(mb.sum()))
+            net.adam_step(grads, lr_ep)
+            tot += loss * len(idx)
+        history.append(float(tot) / P)
+        if log:
+            log(f"epoch {ep} loss {history[-1]:.4e}")
+    return net, norm, history
+
+
+class LearnedGuess:
+    """Predicts the AO density of a water cluster; ``density`` returns None when
+    the prediction fails its electron-count check (use REST's guess instead)."""
+
+    def __init__(self, net: PairMLP, norm: Normaliser, basis: str = "def2-SVP"):
+        self.net, self.norm, self.basis = net, norm, basis
+
+    @staticmethod
+    def load(path: Path = DEFAULT_WEIGHTS, device: int = 0) -> "LearnedGuess":
+        st = dict(np.load(path))
+        net = PairMLP(seed=0, device=device)
+        net.load_state(st)
+        norm = Normaliser(st["f_mean"], st["f_std"], st["t_mean"], st["t_std"])
+        return LearnedGuess(net, norm, str(st["basis"]))
+
+    def save(self, path: Path):
+        st = self.net.state()
+        st.update(f_mean=self.norm.f_mean, f_std=self.norm.f_std, t_mean=self.norm.t_mean, t_std=self.norm.t_std,
+                  basis=np.array(self.basis))
+        Path(path).parent.mkdir(parents=True, exist_ok=True)
+        np.savez_compressed(path, **st)
+
+    def predict_blocks(self, ps: PairSet) -> np.ndarray:
+        import torch
+
+        x = self.net.to_bf16(torch.tensor(self.norm.feats(ps.feats), dtype=torch.float32, device=self.net.dev))
+        y = self.net.forward(x).cpu().numpy().astype(np.float64)
+        return self.norm.blocks(y, ps.kind)
+
+    def density(self, mol, ovlp: np.ndarray | None = None, tol: float = 0.05):
+        sh = mol.shells(self.basis)
+        ps = pair_features(mol)
+        D = assemble_density(mol, sh, ps, self.predict_blocks(ps))
+        if ovlp is not None:
+            ne = float(np.sum(D * ovlp))
+            if not np.isfinite(ne) or abs(ne - mol.nelec) > tol * mol.nelec:
+                return None
+            D *= mol.nelec / ne
+        return D

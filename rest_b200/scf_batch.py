@@ -53,6 +53,7 @@ class BatchResult:
     setup_s: float
     scf_s: float
     timings: dict = field(default_factory=dict)
+    densities: list = field(default_factory=list)  # converged AO densities (host), when asked for
 
 
 class BatchedRHF:
@@ -228,8 +229,44 @@ class BatchedRHF:
             cur.wait_event(done)
         return out
 
+    def _jk_dm(self, D, which):
+        """J + K from densities (REST's dm-only exchange, a4/a5) for molecules in
+        ``which``: the first build from a supplied initial density."""
+        torch = self.torch
+        B, nm = self.B, self.nmax
+        out = torch.zeros(B, nm, nm, dtype=torch.float64, device=self.dev)
+        cur = torch.cuda.current_stream()
+        ev = torch.cuda.Event()
+        ev.record(cur)
+        parts = []
+        for i in range(B):
+            if not which[i]:
+                continue
+            ctx, n = self.ctx[i], self.n[i]
+            st = torch.cuda.ExternalStream(ctx.stream)
+            st.wait_event(ev)
+            with torch.cuda.stream(st):
+                d = D[i, :n, :n].contiguous()
+                npair = n * (n + 1) // 2
+                vj = torch.empty(npair, dtype=torch.float64, device=self.dev)
+                vk = torch.empty(npair, dtype=torch.float64, device=self.dev)
+                ctx.vj_upper_dev(d.data_ptr(), 1, 1.0, 1, vj.data_ptr(), ctx.stream)
+                ctx.vk_upper_dm_dev(d.data_ptr(), 1, -0.5, vk.data_ptr(), ctx.stream)
+                self._nfp64[i] += 1
+                self._streak[i] += 1
+                out[i, :n, :n] = self._upper_to_full(vj + vk, n)
+                done = torch.cuda.Event()
+                done.record(st)
+                parts.append((done, d, vj, vk))
+        for done, *_ in parts:
+            cur.wait_event(done)
+        return out
+
     def run(self, max_cycle: int = 100, acc_etot: float = 1e-8, acc_rho: float = 1e-5, acc_eev: float = 1e-5,
-            num_max_diis: int = 8) -> BatchResult:
+            num_max_diis: int = 8, initial_densities: list | None = None,
+            return_densities: bool = False) -> BatchResult:
+        """Converge every molecule.  ``initial_densities``: per molecule an AO
+        density (n x n) to start from, or None for REST's hcore guess."""
         torch = self.torch
         t0 = time.perf_counter()
         B, nm = self.B, self.nmax
@@ -256,7 +293,15 @@ class BatchedRHF:
         active = [True] * B
         e, C = diag(self.H)  # hcore guess
         D = density(C)
-        F = self.H + self._jk(C, active)
+        given = [d is not None for d in (initial_densities or [None] * B)]
+        for i in range(B):
+            if given[i]:
+                n = self.n[i]
+                D[i] = 0.0
+                D[i, :n, :n] = torch.as_tensor(np.asarray(initial_densities[i]), dtype=f64, device=self.dev)
+        F = self.H + self._jk(C, [not g for g in given])
+        if any(given):
+            F = F + self._jk_dm(D, given)
         E_prev = enuc + 0.5 * ((D * (self.H + F)).sum(dim=(1, 2)))
         e_prev = e
         # DIIS history as a ring buffer per molecule
@@ -332,7 +377,8 @@ class BatchedRHF:
         torch.cuda.synchronize()
         scf_s = time.perf_counter() - t0
         timings = {"fp64_k_builds": list(self._nfp64), "split_k_builds": list(self._nsplit)}
-        return BatchResult([float(x) for x in E_prev.cpu()], conv, iters, self.setup_s, scf_s, timings)
+        dens = [D[i, :self.n[i], :self.n[i]].cpu().numpy() for i in range(B)] if return_densities else []
+        return BatchResult([float(x) for x in E_prev.cpu()], conv, iters, self.setup_s, scf_s, timings, dens)
 
     def close(self):
         for c in self.ctx:
@@ -347,17 +393,20 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
     after another on the device, results come back in the input order.  The
     metric defaults to the device Cholesky fit (no host eigendecomposition)."""
     kw["metric"] = metric
-    run_kw = {k: kw.pop(k) for k in ("max_cycle", "acc_etot", "acc_rho", "acc_eev", "num_max_diis") if k in kw}
+    run_kw = {k: kw.pop(k) for k in ("max_cycle", "acc_etot", "acc_rho", "acc_eev", "num_max_diis",
+                                      "return_densities") if k in kw}
+    guesses = kw.pop("initial_densities", None)
     sizes = [m.shells(basis).nfun for m in mols]
     order = sorted(range(len(mols)), key=lambda i: sizes[i])
     energies, conv, iters = [None] * len(mols), [False] * len(mols), [0] * len(mols)
     nfp64, nsplit = [0] * len(mols), [0] * len(mols)
+    dens = [None] * len(mols) if run_kw.get("return_densities") else []
     setup = scf = 0.0
     for g0 in range(0, len(order), group_size):
         idx = order[g0:g0 + group_size]
         b = BatchedRHF([mols[i] for i in idx], basis, auxbas, device=device, **kw)
         try:
-            r = b.run(**run_kw)
+            r = b.run(initial_densities=None if guesses is None else [guesses[i] for i in idx], **run_kw)
         finally:
             b.close()
         setup += r.setup_s
@@ -365,4 +414,6 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
         for j, i in enumerate(idx):
             energies[i], conv[i], iters[i] = r.energies[j], r.converged[j], r.iterations[j]
             nfp64[i], nsplit[i] = r.timings["fp64_k_builds"][j], r.timings["split_k_builds"][j]
-    return BatchResult(energies, conv, iters, setup, scf, {"fp64_k_builds": nfp64, "split_k_builds": nsplit})
+            if dens:
+                dens[i] = r.densities[j]
+    return BatchResult(energies, conv, iters, setup, scf, {"fp64_k_builds": nfp64, "split_k_builds": nsplit}, dens)
