@@ -423,6 +423,16 @@ def run_ours(args, w):
         cpu_base = {"value": cflops / min(times) / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
                     "sample": sample}
 
+    torch.cuda.synchronize()
+    torch.cuda.set_stream(torch.cuda.default_stream())  # the context's stream ends with it
+    ctx.close()
+    torch.cuda.empty_cache()
+    apps = {}
+    if rank == 0 and not args.no_apps:
+        apps["ri_tensor_build"] = measure_tensor_build(local)
+        apps["precision_alkanes"] = measure_alkanes(local)
+        apps["molecule_set"] = measure_molecule_set(local, args.set_size)
+
     if rank == 0:
         line = {
             "metric": "RI-JK TFLOP/s",
@@ -447,12 +457,157 @@ def run_ours(args, w):
             "cpu_baseline": cpu_base,
             "split_precision": split,
             "scf_water": scf,
+            **apps,
         }
         print(json.dumps(line), flush=True)
-    ctx.close()
     if pg:
         pg.destroy_process_group()
     return 0
+
+
+# ---------------------------------------------------------------------------
+# application configs: device tensor build, alkane precision runs, molecule sets
+# ---------------------------------------------------------------------------
+def _shell_prefix(sh, nshell):
+    """The first nshell shells of a ShellSet (a bounded CPU sample)."""
+    from rest_b200.basis import ShellSet
+
+    return ShellSet(sh.l[:nshell].copy(), sh.nprim[:nshell].copy(), sh.prim_off[:nshell].copy(), sh.exps, sh.coefs,
+                    sh.centers[:nshell].copy(), sh.atom[:nshell].copy())
+
+
+def measure_tensor_build(device: int, k: int = 50) -> dict:
+    """All-device fitted tensor for (H2O)_k (def2-SVP / def2-SVP-JKFIT): device
+    integrals + Cholesky metric + fit, against the host integral engine timed
+    on the first water's auxiliary shells and scaled by the function count."""
+    import numpy as np
+    import torch
+
+    from rest_b200 import RIJK
+    from rest_b200.basis import int3c2e
+    from rest_b200.geometry import water_cluster
+
+    mol = water_cluster(k, seed=11)
+    bas, aux = mol.shells("def2-SVP"), mol.shells("def2-SVP-JKFIT")
+    n, naux = bas.nfun, aux.nfun
+    npair = n * (n + 1) // 2
+    ctx = RIJK(device)
+    try:
+        small = water_cluster(2, seed=5)
+        ctx.build_rimatr_from_shells(small.shells("def2-SVP"), small.shells("def2-SVP-JKFIT"))  # load kernels
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.build_rimatr_from_shells(bas, aux)
+        torch.cuda.synchronize()
+        t_build = time.perf_counter() - t0
+    finally:
+        ctx.close()
+    torch.cuda.empty_cache()
+    nsh = int(np.sum(aux.atom < 3))  # the first water's auxiliary shells
+    sub = _shell_prefix(aux, nsh)
+    t0 = time.perf_counter()
+    int3c2e(bas, sub)
+    t_cpu = time.perf_counter() - t0
+    cpu_full = t_cpu * naux / sub.nfun
+    return {
+        "molecule": f"(H2O)_{k} def2-SVP / def2-SVP-JKFIT, {n} AO, {naux} aux",
+        "device_build_s": t_build,
+        "integrals_per_s": npair * naux / t_build,
+        "host_int3c2e_sample": f"{sub.nfun} of {naux} auxiliary functions, {os.cpu_count()} threads",
+        "host_int3c2e_s_scaled": cpu_full,
+        "device_vs_host_int3c2e_only": cpu_full / t_build,
+    }
+
+
+def measure_alkanes(device: int, sizes=(10, 20, 40)) -> list:
+    """Precision config: FP64 vs mixed-precision batched driver on C_nH_{2n+2}."""
+    from rest_b200.geometry import alkane
+    from rest_b200.scf_batch import BatchedRHF
+
+    crit = dict(acc_etot=1e-8, acc_rho=1e-6, acc_eev=1e-6, max_cycle=100)
+    out = []
+    for nc in sizes:
+        mol = alkane(nc)
+        rec = {"molecule": f"C{nc}H{2 * nc + 2}", "num_basis": mol.shells("def2-SVP").nfun,
+               "num_auxbas": mol.shells("def2-SVP-JKFIT").nfun, "nocc": mol.nelec // 2}
+        for prec in ("fp64", "mixed"):
+            b = BatchedRHF([mol], "def2-SVP", "def2-SVP-JKFIT", device=device, precision=prec, metric="cholesky")
+            try:
+                r = b.run(**crit)
+            finally:
+                b.close()
+            rec[prec] = {"energy": r.energies[0], "converged": r.converged[0], "iterations": r.iterations[0],
+                         "scf_s": r.scf_s, "setup_s": r.setup_s, "fp64_k_builds": r.timings["fp64_k_builds"][0],
+                         "split_k_builds": r.timings["split_k_builds"][0]}
+        rec["mixed_minus_fp64_energy"] = rec["mixed"]["energy"] - rec["fp64"]["energy"]
+        rec["scf_speedup_mixed_vs_fp64"] = rec["fp64"]["scf_s"] / rec["mixed"]["scf_s"]
+        out.append(rec)
+    return out
+
+
+def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: int = 32) -> dict:
+    """Batched config: water clusters k uniform in 1..16 converged together
+    (FP64; mixed precision; mixed precision from the learned guess) against the
+    plain per-molecule FP64 GPU path on a subset."""
+    import numpy as np
+    import torch
+
+    from rest_b200 import RIJK
+    from rest_b200.basis import int1e
+    from rest_b200.geometry import water_cluster
+    from rest_b200.guess import LearnedGuess
+    from rest_b200.scf import SCF, ScfOptions
+    from rest_b200.scf_batch import run_molecule_set
+
+    crit = dict(acc_etot=1e-8, acc_rho=1e-6, acc_eev=1e-6, max_cycle=100)
+    rng = np.random.default_rng(2024)
+    ks = rng.integers(1, 17, nmol)
+    mols = [water_cluster(int(k), seed=50000 + i) for i, k in enumerate(ks)]
+    run_molecule_set(mols[:4], "def2-SVP", "def2-SVP-JKFIT", group_size=4, precision="mixed", device=device, **crit)
+    res = {}
+
+    def timed(tag, **kw):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        extra = 0.0
+        if kw.pop("learned", False):
+            guess = LearnedGuess.load(device=device)
+            t1 = time.perf_counter()
+            dens = [guess.density(m, ovlp=int1e(m, m.shells("def2-SVP"), "ovlp")) for m in mols]
+            extra = time.perf_counter() - t1
+            kw["initial_densities"] = dens
+        r = run_molecule_set(mols, "def2-SVP", "def2-SVP-JKFIT", group_size=group, device=device, **kw, **crit)
+        wall = time.perf_counter() - t0
+        res[tag] = {"molecules_per_s": nmol / wall, "wall_s": wall, "setup_s": r.setup_s, "scf_s": r.scf_s,
+                    "iterations_mean": float(np.mean(r.iterations)), "converged": int(sum(r.converged)),
+                    "guess_s": extra}
+        return r
+
+    ref = timed("batched_fp64", precision="fp64")
+    mix = timed("batched_mixed", precision="mixed")
+    lrn = timed("batched_mixed_learned_guess", precision="mixed", learned=True)
+    e_ref = np.array(ref.energies)
+    res["batched_mixed"]["max_abs_energy_error_vs_fp64"] = float(np.max(np.abs(np.array(mix.energies) - e_ref)))
+    res["batched_mixed_learned_guess"]["max_abs_energy_error_vs_fp64"] = float(
+        np.max(np.abs(np.array(lrn.energies) - e_ref)))
+    sctx = RIJK(device)
+    t0 = time.perf_counter()
+    e_plain = []
+    for m in mols[:plain_subset]:
+        r = SCF(m, "def2-SVP", "def2-SVP-JKFIT", ScfOptions(scf_acc_etot=1e-8, scf_acc_rho=1e-6, scf_acc_eev=1e-6),
+                ctx=sctx).run()
+        e_plain.append(r.energy)
+    wall = time.perf_counter() - t0
+    sctx.close()
+    plain = plain_subset / wall
+    res["plain_fp64_per_molecule"] = {"molecules_per_s": plain, "molecules_timed": plain_subset,
+                                      "max_abs_energy_error_vs_batched_fp64": float(
+                                          np.max(np.abs(np.array(e_plain) - e_ref[:plain_subset])))}
+    for tag in ("batched_fp64", "batched_mixed", "batched_mixed_learned_guess"):
+        res[tag]["speedup_vs_plain_fp64"] = res[tag]["molecules_per_s"] / plain
+    res["set"] = f"{nmol} water clusters (H2O)_k, k uniform in 1..16 (seeded), def2-SVP / def2-SVP-JKFIT, " \
+                 f"RHF to 1e-8 Eh, groups of {group}, device Cholesky metric"
+    return res
 
 
 # DRAM bytes per build of each kernel class from the ncu capture summarised in
@@ -471,6 +626,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision (tcgen05) measurement")
     ap.add_argument("--no-scf", action="store_true", help="skip the water SCF timing")
+    ap.add_argument("--no-apps", action="store_true",
+                    help="skip the application configs (device tensor build, alkanes, molecule set)")
+    ap.add_argument("--set-size", type=int, default=64, help="molecules in the batched water-cluster set")
     args = ap.parse_args()
     w = workload(args.n)
     if args.impl == "reference":

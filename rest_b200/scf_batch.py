@@ -281,10 +281,21 @@ class BatchedRHF:
         self._fp64_now = [self.precision != "mixed"] * B
         nmask = torch.arange(nm, device=self.dev)[None, :] < ns[:, None]
 
-        def diag(F):
-            fp = self.X.transpose(1, 2) @ F @ self.X + self.pad_shift
-            e, cp = torch.linalg.eigh(fp)
-            return e, self.X @ cp
+        def diag(F, rows=None):
+            """Eigenpairs of the molecules in ``rows`` (all when None); the other
+            rows of the result are zero and are not used."""
+            if rows is None:
+                fp = self.X.transpose(1, 2) @ F @ self.X + self.pad_shift
+                e, cp = torch.linalg.eigh(fp)
+                return e, self.X @ cp
+            r = torch.as_tensor(rows, device=self.dev)
+            Xr = self.X[r]
+            e_r, cp = torch.linalg.eigh(Xr.transpose(1, 2) @ F[r] @ Xr + self.pad_shift[r])
+            e = torch.zeros(B, nm, dtype=f64, device=self.dev)
+            C = torch.zeros(B, nm, nm, dtype=f64, device=self.dev)
+            e[r] = e_r
+            C[r] = Xr @ cp
+            return e, C
 
         def density(C):
             co = C * self._occ_mask[:, None, :]
@@ -344,7 +355,7 @@ class BatchedRHF:
                     coef[i, 0] = 1.0
             Fx = torch.einsum("bm,bmij->bij", torch.as_tensor(coef, device=self.dev), f_hist)
             Fx = torch.where(act[:, None, None], Fx, F)
-            e, C = diag(Fx)
+            e, C = diag(Fx, [i for i in range(B) if active[i]])
             Dn = density(C)
             Fn = self.H + self._jk(C, active)
             En = enuc + 0.5 * ((Dn * (self.H + Fn)).sum(dim=(1, 2)))
