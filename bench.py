@@ -296,7 +296,9 @@ def run_ours(args, w):
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6.65 TB/s"}
     roof["kernel"] = dom
     roof["launches_per_step"] = dom_launches
-    roof["traffic"] = TRAFFIC_PER_BUILD.get(dom)
+    roof["traffic"] = traffic_per_launch(dom, w, dom_launches)
+    if roof["traffic"] is not None:
+        roof["traffic_source"] = TRAFFIC_SOURCE
     # J kernels' own HBM roofline, reported beside the dominant one
     j_rates = {}
     for k in ("j_pass1", "j_pass2"):
@@ -610,9 +612,32 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
     return res
 
 
-# DRAM bytes per build of each kernel class from the ncu capture summarised in
-# profiles/ (None until captured).
-TRAFFIC_PER_BUILD: dict = {}
+# DRAM traffic of the half-transform per launch.  ncu at n=600 (N=2400, one
+# launch over all aux rows; profiles/k_half_transform_rank_update_n600.md)
+# measured dram read 3.7385 GB + write 1.5520 GB = 5.2905 GB, which is 0.9966
+# of the bytes the launch must move: the tile-packed tensor rows it reads plus
+# the X rows it writes.  The n=1200 tensor (29 GB) is too large to capture under
+# a multi-pass ncu run, so its traffic is that ratio times the same byte count
+# for the rows of one n=1200 launch.
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_half_transform at n=600 "
+                  "(0.9966 of tensor rows read + X rows written), scaled to this launch's rows and sizes")
+
+
+def half_transform_bytes(n: int, nocc: int, rows: float) -> float:
+    nt = -(-n // 32)
+    ldb = nt * (nt + 1) // 2 * 1024
+    ldx = -(-n // 128) * 128
+    ocols = -(-nocc // 128) * 128
+    return rows * 8.0 * (ldb + ldx * ocols)
+
+
+TRAFFIC_RATIO_K_HALF = 5.2905e9 / half_transform_bytes(600, 100, 2400)
+
+
+def traffic_per_launch(kernel: str, w: dict, launches: int):
+    if kernel != "k_half":
+        return None
+    return TRAFFIC_RATIO_K_HALF * half_transform_bytes(w["n"], w["nocc"], w["naux"] / max(1, launches))
 
 
 def main():

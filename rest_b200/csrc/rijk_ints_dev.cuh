@@ -18,6 +18,7 @@ constexpr int GLA = 2;                                    // max AO l
 constexpr int GLC = 4;                                    // max auxiliary l
 constexpr int GL = 2 * GLA + GLC;                         // max total l of (ab|c) and (c|d)
 constexpr int NTET = (GL + 1) * (GL + 2) * (GL + 3) / 6;  // R_tuv with t+u+v <= GL
+constexpr double SCREEN_EXPONENT = 75.0;  // skip primitive pairs with mu |AB|^2 above this
 constexpr int C2S_TOTAL = 1 * 1 + 3 * 3 + 5 * 6 + 7 * 10 + 9 * 15;
 struct DShells {
   int nshell;
@@ -273,6 +274,7 @@ __global__ void __launch_bounds__(128) k_int3c2e_cls(DShells A, DShells Cs, cons
   const double* Rb = A.centers + 3 * j;
   const double* Rc = Cs.centers + 3 * k;
   const double AB[3] = {Ra[0] - Rb[0], Ra[1] - Rb[1], Ra[2] - Rb[2]};
+  const double AB2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
   double acc[NA * NB * SC];  // (Cartesian a, Cartesian b | spherical c)
 #pragma unroll
   for (int x = 0; x < NA * NB * SC; ++x) acc[x] = 0.0;
@@ -281,8 +283,12 @@ __global__ void __launch_bounds__(128) k_int3c2e_cls(DShells A, DShells Cs, cons
   for (int pa = 0; pa < npa; ++pa)
     for (int pb = 0; pb < npb; ++pb) {
       const double a = A.exps[oa + pa], b = A.exps[ob + pb];
-      const double cab = A.coefs[oa + pa] * A.coefs[ob + pb];
       const double p = a + b;
+      // primitive-pair screening (libcint's exponent cutoff): the Gaussian
+      // product carries exp(-mu |AB|^2); beyond mu |AB|^2 = 75 every term of the
+      // pair is below 1e-28 of the largest integral
+      if (a * b / p * AB2 > SCREEN_EXPONENT) continue;
+      const double cab = A.coefs[oa + pa] * A.coefs[ob + pb];
       double ex[LA + 1][LB + 1][LA + LB + 1], ey[LA + 1][LB + 1][LA + LB + 1], ez[LA + 1][LB + 1][LA + LB + 1];
       herm_pair_t<LA, LB>(a, b, AB[0], ex);
       herm_pair_t<LA, LB>(a, b, AB[1], ey);

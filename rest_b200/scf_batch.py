@@ -59,7 +59,7 @@ class BatchResult:
 class BatchedRHF:
     def __init__(self, mols: list, basis: str, auxbas: str, device: int = 0, metric: str = "inv_sqrt",
                  precision: str = "fp64", integrals: str = "auto", rebuild_every: int = 8,
-                 switch_etot: float = 1e-5, switch_rho: float = 1e-4):
+                 switch_etot: float = 1e-5, switch_rho: float = 1e-4, eig_workers: int = 8):
         import torch
 
         if precision not in ("fp64", "mixed", "split"):
@@ -70,6 +70,7 @@ class BatchedRHF:
         self.dev = torch.device("cuda", device)
         self.precision = precision
         self.rebuild_every, self.switch_etot, self.switch_rho = rebuild_every, switch_etot, switch_rho
+        self.eig_workers, self._pool = eig_workers, None
         t0 = time.perf_counter()
         self.mols = mols
         self.ctx, self.n, self.nocc, self.enuc = [], [], [], []
@@ -122,6 +123,42 @@ class BatchedRHF:
         self._tri = {}
         torch.cuda.synchronize()
         self.setup_s = time.perf_counter() - t0
+
+    def _eigh(self, fp):
+        """Batched symmetric eigensolve, split over several streams from host
+        threads: each cuSOLVER call is a chain of small kernels, and chains on
+        different streams overlap on the GPU."""
+        torch = self.torch
+        nw = min(self.eig_workers, fp.shape[0])
+        if nw <= 1:
+            return torch.linalg.eigh(fp)
+        if self._pool is None:
+            from concurrent.futures import ThreadPoolExecutor
+
+            self._pool = ThreadPoolExecutor(self.eig_workers)
+            self._eig_streams = [torch.cuda.Stream(device=self.dev) for _ in range(self.eig_workers)]
+        main = torch.cuda.current_stream()
+        ready = torch.cuda.Event()
+        ready.record(main)
+        bounds = np.linspace(0, fp.shape[0], nw + 1).astype(int)
+
+        def work(j):
+            st = self._eig_streams[j]
+            st.wait_event(ready)
+            with torch.cuda.stream(st):
+                part = fp[bounds[j]:bounds[j + 1]]
+                e, v = torch.linalg.eigh(part)
+                done = torch.cuda.Event()
+                done.record(st)
+            part.record_stream(st)
+            e.record_stream(main)
+            v.record_stream(main)
+            return e, v, done
+
+        res = list(self._pool.map(work, range(nw)))
+        for _, _, done in res:
+            main.wait_event(done)
+        return torch.cat([e for e, _, _ in res]), torch.cat([v for _, v, _ in res])
 
     def _tri_idx(self, n):
         if n not in self._tri:
@@ -284,13 +321,10 @@ class BatchedRHF:
         def diag(F, rows=None):
             """Eigenpairs of the molecules in ``rows`` (all when None); the other
             rows of the result are zero and are not used."""
-            if rows is None:
-                fp = self.X.transpose(1, 2) @ F @ self.X + self.pad_shift
-                e, cp = torch.linalg.eigh(fp)
-                return e, self.X @ cp
+            rows = list(range(B)) if rows is None else rows
             r = torch.as_tensor(rows, device=self.dev)
             Xr = self.X[r]
-            e_r, cp = torch.linalg.eigh(Xr.transpose(1, 2) @ F[r] @ Xr + self.pad_shift[r])
+            e_r, cp = self._eigh(Xr.transpose(1, 2) @ F[r] @ Xr + self.pad_shift[r])
             e = torch.zeros(B, nm, dtype=f64, device=self.dev)
             C = torch.zeros(B, nm, nm, dtype=f64, device=self.dev)
             e[r] = e_r
@@ -392,6 +426,9 @@ class BatchedRHF:
         return BatchResult([float(x) for x in E_prev.cpu()], conv, iters, self.setup_s, scf_s, timings, dens)
 
     def close(self):
+        if self._pool is not None:
+            self._pool.shutdown()
+            self._pool = None
         for c in self.ctx:
             c.close()
         self.ctx = []
