@@ -91,6 +91,13 @@ int rijk_ctx_set_tiles(rijk_ctx* ctx, int half_transform_cfg, int update_cfg);
  * non-NULL, 8 doubles) receives {half, update} milliseconds per shape. */
 int rijk_ctx_autotune(rijk_ctx* ctx, int64_t ncols, int64_t sample_rows, int* best_half, int* best_update,
                       double* ms);
+/* No counterpart in REST.  While pinned != 0 the context never allocates,
+ * grows or frees device memory: a call that would need more scratch than it
+ * holds fails with RIJK_ERR_TOO_LARGE, and loading a new tensor fails with
+ * RIJK_ERR_ARG.  Pin after one warm-up call of each *_dev form and before
+ * capturing those calls into a CUDA graph, so that the graph's pointers stay
+ * valid for as long as it is replayed. */
+int rijk_ctx_pin_buffers(rijk_ctx* ctx, int pinned);
 int rijk_ctx_profile(rijk_ctx* ctx, int enable);
 int rijk_ctx_profile_read(rijk_ctx* ctx, double* ms, int64_t* launches);
 /* Wait for the work enqueued on `stream` (NULL = the context's stream) and

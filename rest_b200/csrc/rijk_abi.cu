@@ -44,6 +44,7 @@ struct rijk_ctx {
   int64_t tensor_version = 0, tc_version = -1;
   size_t scratch_budget = (size_t)4 << 30;
   int ht_cfg = 1, rk_cfg = 1;  // CTA shapes of the K kernels (fastest measured on B200)
+  bool pinned = false;         // scratch and tensor may not be (re)allocated or freed
   std::string last;
   // per-kernel-class event timers
   struct ProfRec {
@@ -113,6 +114,7 @@ int cuda_fail(rijk_ctx* c, cudaError_t e, const char* what) {
 // Frees the scratch only the metric step and the fit use (once per geometry):
 // the metric, its factor and inverse, the fit's output panel and large staging.
 int release_fit_scratch(rijk_ctx* ctx) {
+  if (ctx->pinned) return RIJK_OK;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (DevBuf* b : {&ctx->mV, &ctx->mLinv, &ctx->mT, &ctx->mLinvd, &ctx->mOut}) {
     if (b->p) cudaFree(b->p);
@@ -130,6 +132,9 @@ int release_fit_scratch(rijk_ctx* ctx) {
 int ensure(rijk_ctx* ctx, DevBuf& b, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (b.bytes >= bytes) return RIJK_OK;
+  if (ctx->pinned)
+    return set_err(ctx, RIJK_ERR_TOO_LARGE,
+                   "buffers are pinned: this call needs " + std::to_string(bytes) + " bytes of scratch");
   if (b.p) cudaFree(b.p);
   b.p = nullptr;
   b.bytes = 0;
@@ -183,6 +188,7 @@ int need_tensor(rijk_ctx* ctx) {
 // Allocate the tile-packed tensor for (n, naux); pad rows are zero.
 int alloc_tensor(rijk_ctx* ctx, int64_t n, int64_t naux) {
   if (n <= 0 || naux <= 0) return set_err(ctx, RIJK_ERR_ARG, "num_basis and num_auxbas must be positive");
+  if (ctx->pinned) return set_err(ctx, RIJK_ERR_ARG, "buffers are pinned: no new tensor can be loaded");
   if (n > 46000) return set_err(ctx, RIJK_ERR_TOO_LARGE, "num_basis above 46000");
   Geom g = rijk::make_geom(n, naux);
   const int64_t naux_pad = round_up(naux, rijk::TS);
@@ -490,6 +496,12 @@ int rijk_ctx_info(const rijk_ctx* ctx, int64_t* num_basis, int64_t* num_auxbas, 
 void* rijk_ctx_stream(rijk_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 int64_t rijk_kernel_launches(void) { return rijk::launch_count(); }
+
+int rijk_ctx_pin_buffers(rijk_ctx* ctx, int pinned) {
+  if (!ctx) return RIJK_ERR_ARG;
+  ctx->pinned = pinned != 0;
+  return RIJK_OK;
+}
 
 int rijk_ctx_set_tiles(rijk_ctx* ctx, int half_transform_cfg, int update_cfg) {
   if (!ctx || half_transform_cfg < 0 || half_transform_cfg > 3 || update_cfg < 0 || update_cfg > 3)

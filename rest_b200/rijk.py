@@ -100,6 +100,10 @@ class RIJK:
 
     PROF_CLASSES = ("j_pass1", "j_pass2", "j_other", "k_half", "k_rank", "k_dm", "k_other")
 
+    def pin_buffers(self, pinned: bool = True):
+        """Freeze the context's device memory (for CUDA graph capture of *_dev calls)."""
+        self._check(lib().rijk_ctx_pin_buffers(self._h, int(bool(pinned))))
+
     def set_tiles(self, half_transform_cfg: int, update_cfg: int):
         self._check(lib().rijk_ctx_set_tiles(self._h, int(half_transform_cfg), int(update_cfg)))
 

@@ -59,7 +59,8 @@ class BatchResult:
 class BatchedRHF:
     def __init__(self, mols: list, basis: str, auxbas: str, device: int = 0, metric: str = "inv_sqrt",
                  precision: str = "fp64", integrals: str = "auto", rebuild_every: int = 8,
-                 switch_etot: float = 1e-5, switch_rho: float = 1e-4, eig_workers: int = 8):
+                 switch_etot: float = 1e-5, switch_rho: float = 1e-4, eig_workers: int = 8,
+                 graphs: bool = False):
         import torch
 
         if precision not in ("fp64", "mixed", "split"):
@@ -71,6 +72,10 @@ class BatchedRHF:
         self.precision = precision
         self.rebuild_every, self.switch_etot, self.switch_rho = rebuild_every, switch_etot, switch_rho
         self.eig_workers, self._pool = eig_workers, None
+        # CUDA graphs of the per-molecule FP64 J/K (orbital form), captured after
+        # the first build with every context's buffers pinned
+        self.graphs = graphs and precision == "fp64"
+        self._graph = None
         t0 = time.perf_counter()
         self.mols = mols
         self.ctx, self.n, self.nocc, self.enuc = [], [], [], []
@@ -201,8 +206,68 @@ class BatchedRHF:
             out[i] = (V[:self.n[i]], int(np.sum(lb[keep] > 0)))
         return out
 
+    def _capture(self):
+        """One CUDA graph per molecule: D = 2 C C^T, J and K through the device
+        entry points on the molecule's capture stream, unpacked into a static
+        padded output.  Inputs are read from a static orbital buffer."""
+        torch = self.torch
+        B, nm, om = self.B, self.nmax, self.omax
+        self._gC = torch.zeros(B, nm, om, dtype=torch.float64, device=self.dev)
+        self._gout = torch.zeros(B, nm, nm, dtype=torch.float64, device=self.dev)
+        self._gocc = torch.full((om,), 2.0, dtype=torch.float64, device=self.dev)
+        self._graph = []
+        for i in range(B):
+            ctx, n, o = self.ctx[i], self.n[i], self.nocc[i]
+            self._tri_idx(n)
+            st = torch.cuda.Stream(device=self.dev)
+            npair = n * (n + 1) // 2
+
+            def body():
+                c = self._gC[i, :n, :o]
+                d = 2.0 * (c @ c.T)
+                c_cm = c.T.contiguous()
+                vj = torch.empty(npair, dtype=torch.float64, device=self.dev)
+                vk = torch.empty(npair, dtype=torch.float64, device=self.dev)
+                ctx.vj_upper_dev(d.data_ptr(), 1, 1.0, 1, vj.data_ptr(), st.cuda_stream)
+                ctx.vk_upper_occ_dev(c_cm.data_ptr(), o, [o - 1], self._gocc.data_ptr(), 1, -0.5, vk.data_ptr(),
+                                     st.cuda_stream)
+                self._gout[i, :n, :n] = self._upper_to_full(vj + vk, n)
+
+            st.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(st):
+                body()  # warm-up on the capture stream (library scratch already sized)
+            st.synchronize()
+            ctx.pin_buffers(True)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=st):
+                body()
+            self._graph.append((g, st))
+        torch.cuda.synchronize()
+
+    def _jk_replay(self, C, active):
+        torch = self.torch
+        self._gC.copy_(C[:, :, :self.omax] * self._occ_mask[:, None, :self.omax])
+        cur = torch.cuda.current_stream()
+        ev = torch.cuda.Event()
+        ev.record(cur)
+        for i in range(self.B):
+            if not active[i]:
+                continue
+            g, st = self._graph[i]
+            st.wait_event(ev)
+            with torch.cuda.stream(st):
+                g.replay()
+            done = torch.cuda.Event()
+            done.record(st)
+            cur.wait_event(done)
+            self._nfp64[i] += 1
+            self._streak[i] += 1
+        return self._gout.clone()
+
     def _jk(self, C, active):
         """J + K (full, padded batch) for the active molecules from their orbitals."""
+        if self._graph is not None:
+            return self._jk_replay(C, active)
         torch = self.torch
         B, nm, om = self.B, self.nmax, self.omax
         out = torch.zeros(B, nm, nm, dtype=torch.float64, device=self.dev)
@@ -347,6 +412,8 @@ class BatchedRHF:
         F = self.H + self._jk(C, [not g for g in given])
         if any(given):
             F = F + self._jk_dm(D, given)
+        if self.graphs and self._graph is None:
+            self._capture()
         E_prev = enuc + 0.5 * ((D * (self.H + F)).sum(dim=(1, 2)))
         e_prev = e
         # DIIS history as a ring buffer per molecule
@@ -426,6 +493,7 @@ class BatchedRHF:
         return BatchResult([float(x) for x in E_prev.cpu()], conv, iters, self.setup_s, scf_s, timings, dens)
 
     def close(self):
+        self._graph = None  # graphs go before the contexts whose memory they use
         if self._pool is not None:
             self._pool.shutdown()
             self._pool = None

@@ -70,3 +70,46 @@ def test_alkane_c10_mixed_precision_matches_fp64(ctx):
     assert out["mixed"][1]["split_k_builds"][0] > 0
     assert abs(out["mixed"][0] - out["fp64"][0]) < 1e-8
     assert abs(out["fp64"][0] - _single(ctx, mol)) < 1e-8
+
+
+def test_graph_replay_matches_eager_build():
+    """FP64 J/K captured as one CUDA graph per molecule (contexts pinned) gives
+    the eager driver's energies."""
+    mols = [water_cluster(k, seed=70 + k) for k in (2, 1, 3)]
+    out = {}
+    for graphs in (False, True):
+        b = BatchedRHF(mols, "def2-SVP", "def2-SVP-JKFIT", precision="fp64", graphs=graphs)
+        try:
+            r = b.run(max_cycle=100, **TIGHT_BATCH)
+        finally:
+            b.close()
+        assert all(r.converged)
+        out[graphs] = r
+    for e0, e1 in zip(out[False].energies, out[True].energies):
+        assert abs(e0 - e1) < 1e-10
+    assert out[False].iterations == out[True].iterations
+
+
+def test_pinned_context_refuses_to_grow(ctx):
+    import torch
+
+    from rest_b200._abi import RijkError
+
+    mol = water_cluster(1, seed=3)
+    bas, aux = mol.shells("def2-SVP"), mol.shells("def2-SVP-JKFIT")
+    ctx.build_rimatr_from_shells(bas, aux)
+    n = bas.nfun
+    d = torch.eye(n, dtype=torch.float64, device="cuda")
+    vj = torch.empty(n * (n + 1) // 2, dtype=torch.float64, device="cuda")
+    ctx.vj_upper_dev(d.data_ptr(), 1, 1.0, 1, vj.data_ptr(), 0)
+    ctx.synchronize()
+    ctx.pin_buffers(True)
+    try:
+        ctx.vj_upper_dev(d.data_ptr(), 1, 1.0, 1, vj.data_ptr(), 0)  # same sizes: allowed
+        with pytest.raises(RijkError) as e:
+            ctx.build_rimatr_from_shells(bas, aux)  # a new tensor needs new memory
+        assert e.value.status in (1, 8)
+    finally:
+        ctx.pin_buffers(False)
+    ctx.synchronize()
+    ctx.build_rimatr_from_shells(bas, aux)
