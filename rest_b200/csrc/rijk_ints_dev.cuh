@@ -19,6 +19,13 @@ constexpr int GLC = 4;                                    // max auxiliary l
 constexpr int GL = 2 * GLA + GLC;                         // max total l of (ab|c) and (c|d)
 constexpr int NTET = (GL + 1) * (GL + 2) * (GL + 3) / 6;  // R_tuv with t+u+v <= GL
 constexpr double SCREEN_EXPONENT = 75.0;  // skip primitive pairs with mu |AB|^2 above this
+// Boys function table: F_n(T) for n = 0..BOYS_NMAX at T = i * BOYS_STEP,
+// i = 0..BOYS_NGRID-1 (T <= 40); orders above GL feed the Taylor expansion.
+constexpr int BOYS_TAYLOR = 7;
+constexpr int BOYS_NMAX = GL + BOYS_TAYLOR;
+constexpr int BOYS_NGRID = 801;
+constexpr double BOYS_STEP = 0.05;
+constexpr double BOYS_TMAX = 40.0;
 constexpr int C2S_TOTAL = 1 * 1 + 3 * 3 + 5 * 6 + 7 * 10 + 9 * 15;
 struct DShells {
   int nshell;
@@ -37,19 +44,21 @@ using Int3cKernel = void (*)(DShells, DShells, const int*, const int*, int, cons
 Int3cKernel int3c_kernel_la0(int lb, int lc);
 Int3cKernel int3c_kernel_la1(int lb, int lc);
 Int3cKernel int3c_kernel_la2(int lb, int lc);
-int int3c_tables_la0(const double* flat, const int* off);
-int int3c_tables_la1(const double* flat, const int* off);
-int int3c_tables_la2(const double* flat, const int* off);
+int int3c_tables_la0(const double* flat, const int* off, const double* boys);
+int int3c_tables_la1(const double* flat, const int* off, const double* boys);
+int int3c_tables_la2(const double* flat, const int* off, const double* boys);
 
 namespace {
 
 __constant__ double c_c2s[C2S_TOTAL];
 __constant__ int c_c2s_off[GLC + 1];
+__device__ double g_boys[BOYS_NGRID * (BOYS_NMAX + 1)];
 
-// loads this translation unit's copy of the c2s table
-int upload_tables(const double* flat, const int* off) {
+// loads this translation unit's copies of the c2s and Boys tables
+int upload_tables(const double* flat, const int* off, const double* boys) {
   if (cudaMemcpyToSymbol(c_c2s, flat, C2S_TOTAL * sizeof(double)) != cudaSuccess) return 1;
   if (cudaMemcpyToSymbol(c_c2s_off, off, (GLC + 1) * sizeof(int)) != cudaSuccess) return 1;
+  if (cudaMemcpyToSymbol(g_boys, boys, sizeof(double) * BOYS_NGRID * (BOYS_NMAX + 1)) != cudaSuccess) return 1;
   return 0;
 }
 
@@ -69,28 +78,30 @@ __device__ __forceinline__ void cart_ijk(int l, int c, int& i, int& j, int& k) {
 }
 __device__ __forceinline__ double c2s_at(int l, int m, int c) { return c_c2s[c_c2s_off[l] + m * ncart_d(l) + c]; }
 
-// Boys function F_n(T), n = 0..nmax: series at the top order with downward
-// recursion, or the asymptotic F_0 with upward recursion for T > 40.
+// Boys function F_n(T), n = 0..nmax (nmax <= GL).  T <= 40: F_nmax from a
+// Taylor expansion about the nearest tabulated point, dF_n/dT = -F_{n+1}, so
+// F_nmax(T0 + d) = sum_k F_{nmax+k}(T0) (-d)^k / k! (|d| <= 0.025, seven terms:
+// truncation below 2e-15 relative), then downward recursion
+// F_{m-1} = (2T F_m + e^-T) / (2m-1).  T > 40: the asymptotic F_0 and upward
+// recursion (stable there).  The table is filled on the host from the series.
 __device__ void boys_d(int nmax, double T, double* F) {
-  if (T < 1e-14) {
-    for (int n = 0; n <= nmax; ++n) F[n] = 1.0 / (2 * n + 1);
-    return;
-  }
-  if (T > 40.0) {
+  if (T > BOYS_TMAX) {
     F[0] = 0.5 * sqrt(3.14159265358979323846 / T);
     const double e = exp(-T);
-    for (int n = 0; n < nmax; ++n) F[n + 1] = ((2 * n + 1) * F[n] - e) / (2 * T);
+    const double h = 0.5 / T;
+    for (int n = 0; n < nmax; ++n) F[n + 1] = ((2 * n + 1) * F[n] - e) * h;
     return;
   }
+  const int i = __double2int_rn(T * (1.0 / BOYS_STEP));
+  const double d = T - i * BOYS_STEP;
+  const double* row = g_boys + i * (BOYS_NMAX + 1) + nmax;
+  // Horner form of sum_k row[k] (-d)^k / k!
+  double f = row[BOYS_TAYLOR - 1];
+#pragma unroll
+  for (int k = BOYS_TAYLOR - 1; k >= 1; --k) f = row[k - 1] - d * f * (1.0 / k);
+  F[nmax] = f;
   const double e = exp(-T);
-  double term = 1.0 / (2 * nmax + 1), sum = term;
-  for (int k = 1; k < 400; ++k) {
-    term *= 2 * T / (2 * nmax + 2 * k + 1);
-    sum += term;
-    if (term < 1e-17 * sum) break;
-  }
-  F[nmax] = e * sum;
-  for (int m = nmax; m > 0; --m) F[m - 1] = (2 * T * F[m] + e) / (2 * m - 1);
+  for (int m = nmax; m > 0; --m) F[m - 1] = (2 * T * F[m] + e) * (1.0 / (2 * m - 1));
 }
 
 // ---- three-centre integrals, one kernel per angular class (LA, LB, LC) -----------

@@ -13,6 +13,8 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -268,6 +270,31 @@ struct RiIntPlan {
 
 namespace {
 
+// F_n(T_i) for the device table: the series sum_k (2T)^k / ((2n+1)(2n+3)...(2n+2k+1))
+// times e^-T at the top order, in long double (all terms positive), then
+// downward recursion; computed once per process.
+const std::vector<double>& boys_table() {
+  static const std::vector<double> tab = [] {
+    std::vector<double> t((size_t)BOYS_NGRID * (BOYS_NMAX + 1));
+    for (int i = 0; i < BOYS_NGRID; ++i) {
+      const long double T = (long double)i * BOYS_STEP;
+      long double F[BOYS_NMAX + 1];
+      const long double e = expl(-T);
+      long double term = 1.0L / (2 * BOYS_NMAX + 1), sum = term;
+      for (int k = 1; k < 2000; ++k) {
+        term *= 2 * T / (2 * BOYS_NMAX + 2 * k + 1);
+        sum += term;
+        if (term < 1e-22L * sum) break;
+      }
+      F[BOYS_NMAX] = e * sum;
+      for (int m = BOYS_NMAX; m > 0; --m) F[m - 1] = (2 * T * F[m] + e) / (2 * m - 1);
+      for (int n = 0; n <= BOYS_NMAX; ++n) t[(size_t)i * (BOYS_NMAX + 1) + n] = (double)F[n];
+    }
+    return t;
+  }();
+  return tab;
+}
+
 int upload_c2s(const double* const* c2s, cudaStream_t st) {
   for (int l = 0; l <= GLC; ++l)
     if (!c2s[l]) return RIJK_ERR_ARG;
@@ -278,12 +305,22 @@ int upload_c2s(const double* const* c2s, cudaStream_t st) {
     const int n = (2 * l + 1) * (l + 1) * (l + 2) / 2;
     flat.insert(flat.end(), c2s[l], c2s[l] + n);
   }
+  // the tables change only with the caller's c2s matrices: upload once per device
+  static std::mutex mu;
+  static std::map<int, std::vector<double>> uploaded;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return RIJK_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = uploaded.find(dev);
+  if (it != uploaded.end() && it->second == flat) return RIJK_OK;
   // earlier launches on this stream may still read the table: order after them
   if (cudaStreamSynchronize(st) != cudaSuccess) return RIJK_ERR_CUDA;
   // every translation unit with integral kernels holds its own copy of the table
-  if (upload_tables(flat.data(), off) || int3c_tables_la0(flat.data(), off) || int3c_tables_la1(flat.data(), off) ||
-      int3c_tables_la2(flat.data(), off))
+  const double* boys = boys_table().data();
+  if (upload_tables(flat.data(), off, boys) || int3c_tables_la0(flat.data(), off, boys) ||
+      int3c_tables_la1(flat.data(), off, boys) || int3c_tables_la2(flat.data(), off, boys))
     return RIJK_ERR_CUDA;
+  uploaded[dev] = flat;
   return RIJK_OK;
 }
 
