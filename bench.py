@@ -430,7 +430,7 @@ def run_ours(args, w):
     ctx.close()
     torch.cuda.empty_cache()
     apps = {}
-    if rank == 0 and not args.no_apps:
+    if rank == 0 and world == 1 and not args.no_apps:
         apps["ri_tensor_build"] = measure_tensor_build(local)
         apps["precision_alkanes"] = measure_alkanes(local)
         apps["molecule_set"] = measure_molecule_set(local, args.set_size)

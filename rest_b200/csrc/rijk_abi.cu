@@ -444,8 +444,8 @@ int rijk_ctx_create(int device, rijk_ctx** out) {
   if (cudaSetDevice(device) != cudaSuccess) return RIJK_ERR_CUDA;
   rijk_ctx* c = new rijk_ctx();
   c->device = device;
-  if (const char* s = getenv("RIJK_HT_CFG")) c->ht_cfg = std::max(0, std::min(3, atoi(s)));
-  if (const char* s = getenv("RIJK_RK_CFG")) c->rk_cfg = std::max(0, std::min(3, atoi(s)));
+  if (const char* s = getenv("RIJK_HT_CFG")) c->ht_cfg = std::max(0, std::min(RIJK_TILE_CFGS - 1, atoi(s)));
+  if (const char* s = getenv("RIJK_RK_CFG")) c->rk_cfg = std::max(0, std::min(RIJK_TILE_CFGS - 1, atoi(s)));
   if (const char* s = getenv("RIJK_SCRATCH_BYTES")) {
     const long long v = atoll(s);
     if (v > (1 << 20)) c->scratch_budget = (size_t)v;
@@ -504,7 +504,8 @@ int rijk_ctx_pin_buffers(rijk_ctx* ctx, int pinned) {
 }
 
 int rijk_ctx_set_tiles(rijk_ctx* ctx, int half_transform_cfg, int update_cfg) {
-  if (!ctx || half_transform_cfg < 0 || half_transform_cfg > 3 || update_cfg < 0 || update_cfg > 3)
+  if (!ctx || half_transform_cfg < 0 || half_transform_cfg >= RIJK_TILE_CFGS || update_cfg < 0 ||
+      update_cfg >= RIJK_TILE_CFGS)
     return set_err(ctx, RIJK_ERR_ARG, "tile configuration out of range");
   ctx->ht_cfg = ctx->g.ht_cfg = half_transform_cfg;
   ctx->rk_cfg = ctx->g.rk_cfg = update_cfg;
@@ -532,7 +533,7 @@ int rijk_ctx_autotune(rijk_ctx* ctx, int64_t ncols, int64_t sample_rows, int* be
   RIJK_CK(cudaEventCreate(&b));
   double best_ht_ms = 1e30, best_rk_ms = 1e30;
   int bh = ctx->ht_cfg, br = ctx->rk_cfg;
-  for (int cfg = 0; cfg < 4; ++cfg) {
+  for (int cfg = 0; cfg < RIJK_TILE_CFGS; ++cfg) {
     g.ht_cfg = cfg;
     g.rk_cfg = cfg;
     const int splits = rijk::k_rank_splits(g, np, 0);

@@ -365,6 +365,13 @@ using HtCfg0 = DmmaCfg<2, 2, 2, 2, 3, true>;  // 64 x 64, 4 warps of 32 x 32, cp
 using HtCfg1 = DmmaCfg<2, 2, 2, 2, 2, true>;  // 64 x 64, cp.async, 2 stages (3 CTAs/SM)
 using HtCfg2 = DmmaCfg<2, 2, 2, 2, 4, true>;  // 64 x 64, cp.async, 4 stages (1 CTA/SM)
 using HtCfg3 = DmmaCfg<2, 2, 2, 2, 3>;        // 64 x 64, bulk copies + producer warp, 3 stages
+using HtCfg4 = DmmaCfg<4, 2, 4, 2, 2, true>;  // 128 x 64, 8 warps of 32 x 32, cp.async, 2 stages (2 CTAs/SM)
+
+// Register budget: 256-thread shapes are held to 128 registers so that two CTAs fit an SM.
+template <class Cfg>
+constexpr int min_ctas() {
+  return Cfg::THREADS >= 256 ? 2 : 1;
+}
 
 struct HalfTransformSched {
   const double* Bp;  // row P of the tile-packed tensor
@@ -391,7 +398,7 @@ struct LastTileK {
 // Grid: blockIdx.x = cb + ncb * (rb + nrb * p), so that the column blocks of
 // one row block run back to back and share its B tiles in L2.
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::THREADS, 1) k_half_transform(const double* __restrict__ B, int64_t ldB, int64_t p0,
+__global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_half_transform(const double* __restrict__ B, int64_t ldB, int64_t p0,
                                                                  int nrb, int ncb, const double* __restrict__ W,
                                                                  int64_t ldw, int n, int nt, int ncol_valid,
                                                                  double* __restrict__ X, int64_t ldx, int64_t sxp,
@@ -435,6 +442,7 @@ void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t n
     case 1: return half_transform_cfg<HtCfg1>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
     case 2: return half_transform_cfg<HtCfg2>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
     case 3: return half_transform_cfg<HtCfg3>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
+    case 4: return half_transform_cfg<HtCfg4>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
     default: return half_transform_cfg<HtCfg0>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
   }
 }
@@ -446,9 +454,10 @@ using RkCfg0 = DmmaCfg<2, 2, 2, 2, 3, true>;  // 64 x 64, 4 warps of 32 x 32, cp
 using RkCfg1 = DmmaCfg<2, 2, 2, 2, 2, true>;  // 64 x 64, cp.async, 2 stages (3 CTAs/SM)
 using RkCfg2 = DmmaCfg<2, 2, 2, 2, 4, true>;  // 64 x 64, cp.async, 4 stages (1 CTA/SM)
 using RkCfg3 = DmmaCfg<2, 2, 2, 2, 3>;        // 64 x 64, bulk copies + producer warp, 3 stages
+using RkCfg4 = DmmaCfg<4, 2, 4, 2, 2, true>;  // 128 x 64, 8 warps, cp.async, 2 stages (2 CTAs/SM)
 constexpr int KB = 128;                       // K block edge
 
-static int rk_subs(int) { return 4; }
+static int rk_subs(int cfg) { return cfg == 4 ? 2 : 4; }  // CTA sub-blocks of a 128 x 128 K block
 static int rk_ctas_per_sm(int cfg) { return cfg == 1 ? 3 : cfg == 2 ? 1 : 2; }
 
 int64_t k_block_pairs(const Geom& g, int full) {
@@ -515,7 +524,7 @@ struct RankK {
 };
 
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::THREADS, 1) k_rank_update(const double* __restrict__ X, int64_t ldx, int64_t sxp,
+__global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_rank_update(const double* __restrict__ X, int64_t ldx, int64_t sxp,
                                                               int64_t np, int c0t, int ctiles, int lastk, int n,
                                                               int splits, int full, int64_t nkb, int64_t pairs,
                                                               double* __restrict__ Kpart, int* err) {
@@ -558,6 +567,7 @@ void launch_k_rank_update(const Geom& g, const double* X, int64_t ldx, int64_t s
     case 1: return rank_update_cfg<RkCfg1>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
     case 2: return rank_update_cfg<RkCfg2>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
     case 3: return rank_update_cfg<RkCfg3>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
+    case 4: return rank_update_cfg<RkCfg4>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
     default: return rank_update_cfg<RkCfg0>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
   }
 }
@@ -590,7 +600,7 @@ struct KdmSched {
 };
 
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::THREADS, 1) k_dm_update(const double* __restrict__ T, int64_t ldt, int64_t stp,
+__global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_dm_update(const double* __restrict__ T, int64_t ldt, int64_t stp,
                                                             const double* __restrict__ B, int64_t ldB, int64_t pg0,
                                                             int64_t np, int n, int nt, int splits, int full,
                                                             int64_t nkb, int64_t pairs, double* __restrict__ Kpart,
@@ -631,6 +641,7 @@ void launch_k_dm_update(const Geom& g, const double* T, int64_t ldt, int64_t stp
     case 1: return dm_update_cfg<RkCfg1>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
     case 2: return dm_update_cfg<RkCfg2>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
     case 3: return dm_update_cfg<RkCfg3>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
+    case 4: return dm_update_cfg<RkCfg4>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
     default: return dm_update_cfg<RkCfg0>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
   }
 }

@@ -45,6 +45,9 @@ def _rest_list(parts):
     return out
 
 
+TILE_CFGS = 5  # CTA shapes of the K kernels (RIJK_TILE_CFGS in include/rest_b200.h)
+
+
 class RIJK:
     """A device context holding one fitted three-centre tensor."""
 
@@ -111,9 +114,9 @@ class RIJK:
         """Time every CTA shape on this tensor, keep the fastest; returns
         (half_cfg, update_cfg, {cfg: (half_ms, update_ms)})."""
         bh, br = C.c_int(), C.c_int()
-        ms = (C.c_double * 8)()
+        ms = (C.c_double * (2 * TILE_CFGS))()
         self._check(lib().rijk_ctx_autotune(self._h, int(ncols), int(sample_rows), C.byref(bh), C.byref(br), ms))
-        return bh.value, br.value, {c: (ms[2 * c], ms[2 * c + 1]) for c in range(4)}
+        return bh.value, br.value, {c: (ms[2 * c], ms[2 * c + 1]) for c in range(TILE_CFGS)}
 
     def profile(self, enable: bool = True):
         self._check(lib().rijk_ctx_profile(self._h, int(bool(enable))))
