@@ -21,13 +21,14 @@ stream), and the SCF iterations of the whole set advance together:
 
 Precision of the exchange build:
   fp64   every K in FP64 (DMMA);
-  mixed  incremental split-precision K: K_k = K_{k-1} + K_split(D_k - D_{k-1}) with
+  mixed  for molecules with at least ``split_min_basis`` (512) basis functions,
+         incremental split-precision K: K_k = K_{k-1} + K_split(D_k - D_{k-1}) with
          the density difference in its exact low-rank form V S V^T (batched thin
          QR of [Y_k, Y_{k-1}] and an eigendecomposition of the small core, so the
          split error scales with |dD|), a full FP64 rebuild every
          ``rebuild_every`` split steps, FP64 builds once the molecule is loosely
          converged, and convergence only on consecutive FP64 builds, so every
-         reported energy is an FP64 energy;
+         reported energy is an FP64 energy; smaller molecules take FP64 builds;
   split  every K in split precision (no FP64 finish; for loose criteria only).
 Everything else is FP64.  Molecules converge independently (REST's three
 criteria, :1875-1951) and stop being updated once converged.
@@ -60,7 +61,7 @@ class BatchedRHF:
     def __init__(self, mols: list, basis: str, auxbas: str, device: int = 0, metric: str = "inv_sqrt",
                  precision: str = "fp64", integrals: str = "auto", rebuild_every: int = 8,
                  switch_etot: float = 1e-5, switch_rho: float = 1e-4, eig_workers: int = 8,
-                 graphs: bool = False):
+                 graphs: bool = False, split_min_basis: int = 512):
         import torch
 
         if precision not in ("fp64", "mixed", "split"):
@@ -71,6 +72,10 @@ class BatchedRHF:
         self.dev = torch.device("cuda", device)
         self.precision = precision
         self.rebuild_every, self.switch_etot, self.switch_rho = rebuild_every, switch_etot, switch_rho
+        # split-precision K pays only where K dominates: measured on B200, below
+        # about 500 basis functions the operand preparation and the low-rank
+        # factorisation of dD cost more than the split build saves
+        self.split_min_basis = split_min_basis
         self.eig_workers, self._pool = eig_workers, None
         # CUDA graphs of the per-molecule FP64 J/K (orbital form), captured after
         # the first build with every context's buffers pinned
@@ -380,7 +385,7 @@ class BatchedRHF:
             self._occ_mask[i, :self.nocc[i]] = 1.0
         self._kref, self._yref = [None] * B, [None] * B
         self._split_steps, self._nsplit, self._nfp64, self._streak = [0] * B, [0] * B, [0] * B, [0] * B
-        self._fp64_now = [self.precision != "mixed"] * B
+        self._fp64_now = [self.precision != "mixed" or self.n[i] < self.split_min_basis for i in range(B)]
         nmask = torch.arange(nm, device=self.dev)[None, :] < ns[:, None]
 
         def diag(F, rows=None):

@@ -29,7 +29,8 @@ def _single(ctx, mol):
 @pytest.mark.parametrize("precision", ["fp64", "mixed", "split"])
 def test_batched_water_clusters_match_single_scf(ctx, precision):
     mols = [water_cluster(k, seed=10 + k) for k in (1, 2, 3, 1, 2)]
-    batch = BatchedRHF(mols, "def2-SVP", "def2-SVP-JKFIT", precision=precision)
+    # split_min_basis=0: exercise the split path on these small molecules too
+    batch = BatchedRHF(mols, "def2-SVP", "def2-SVP-JKFIT", precision=precision, split_min_basis=0)
     # all-split builds carry ~1e-5 relative noise in K: converge them loosely
     crit = TIGHT_BATCH if precision != "split" else dict(acc_etot=1e-5, acc_rho=1e-4, acc_eev=1e-3)
     try:
@@ -60,7 +61,7 @@ def test_alkane_c10_mixed_precision_matches_fp64(ctx):
     mol = alkane(10)
     out = {}
     for prec in ("fp64", "mixed"):
-        b = BatchedRHF([mol], "def2-SVP", "def2-SVP-JKFIT", precision=prec)
+        b = BatchedRHF([mol], "def2-SVP", "def2-SVP-JKFIT", precision=prec, split_min_basis=0)
         try:
             r = b.run(max_cycle=100, **TIGHT_BATCH)
         finally:
@@ -113,3 +114,14 @@ def test_pinned_context_refuses_to_grow(ctx):
         ctx.pin_buffers(False)
     ctx.synchronize()
     ctx.build_rimatr_from_shells(bas, aux)
+
+
+def test_mixed_precision_keeps_small_molecules_in_fp64():
+    """Below split_min_basis the mixed driver builds K in FP64 only."""
+    mols = [water_cluster(2, seed=5)]
+    b = BatchedRHF(mols, "def2-SVP", "def2-SVP-JKFIT", precision="mixed")
+    try:
+        r = b.run(max_cycle=100, **TIGHT_BATCH)
+    finally:
+        b.close()
+    assert r.converged[0] and r.timings["split_k_builds"][0] == 0
