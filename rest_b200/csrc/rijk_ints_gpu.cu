@@ -353,12 +353,22 @@ int ri_plan_create(const rijk_shells* bas, const rijk_shells* aux, const double*
           pi.push_back(i);
           pj.push_back(j);
         }
+      // class, then primitive count, then separation: neighbouring lanes share
+      // their loop trip counts and, mostly, their screening outcomes
       auto key = [&](int x) {
         return (int64_t)(bas->l[pi[x]] * 3 + bas->l[pj[x]]) * 4096 + bas->nprim[pi[x]] * bas->nprim[pj[x]];
       };
+      auto dist2 = [&](int x) {
+        const double* a = bas->centers + 3 * pi[x];
+        const double* b = bas->centers + 3 * pj[x];
+        return (a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]);
+      };
       std::vector<int> order(pi.size());
       std::iota(order.begin(), order.end(), 0);
-      std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key(x) < key(y); });
+      std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const int64_t kx = key(x), ky = key(y);
+        return kx != ky ? kx < ky : dist2(x) < dist2(y);
+      });
       std::vector<int> si(pi.size()), sj(pi.size());
       for (size_t t = 0; t < order.size(); ++t) {
         si[t] = pi[order[t]];
