@@ -491,9 +491,20 @@ class BatchedRHF:
                 active[i] = False
             if not any(active):
                 break
+        # a converged density must hold the electrons and be idempotent
+        # (D S D = 2 D); a molecule that fails either is reported as not converged
+        ne = (D * self.S).sum(dim=(1, 2))
+        idem = (D @ self.S @ D - 2.0 * D).abs().amax(dim=(1, 2))
+        ne_h, idem_h = ne.cpu().numpy(), idem.cpu().numpy()
+        checks = []
+        for i in range(B):
+            ok = abs(ne_h[i] - 2 * self.nocc[i]) < 1e-6 * max(1, 2 * self.nocc[i]) and idem_h[i] < 1e-6
+            checks.append(bool(ok))
+            conv[i] = conv[i] and ok
         torch.cuda.synchronize()
         scf_s = time.perf_counter() - t0
-        timings = {"fp64_k_builds": list(self._nfp64), "split_k_builds": list(self._nsplit)}
+        timings = {"fp64_k_builds": list(self._nfp64), "split_k_builds": list(self._nsplit),
+                   "density_checks": checks}
         dens = [D[i, :self.n[i], :self.n[i]].cpu().numpy() for i in range(B)] if return_densities else []
         return BatchResult([float(x) for x in E_prev.cpu()], conv, iters, self.setup_s, scf_s, timings, dens)
 
@@ -507,29 +518,59 @@ class BatchedRHF:
         self.ctx = []
 
 
+def device_bytes(n: int, naux: int, nocc: int, precision: str = "fp64") -> int:
+    """Device memory one molecule's context holds during the SCF: the tile-packed
+    tensor, the half-transform scratch (capped at the context's 4 GiB budget),
+    and for split precision the BF16 hi/lo copies of the full B_P."""
+    nt = -(-n // 32)
+    naux_pad = -(-naux // 32) * 32
+    tensor = naux_pad * (nt * (nt + 1) // 2 * 1024) * 8
+    ldx = -(-n // 128) * 128
+    scratch = min(4 << 30, naux * ldx * (-(-nocc // 128) * 128) * 8)
+    split = naux_pad * ldx * ldx * 4 if precision in ("mixed", "split") else 0
+    return tensor + scratch + split + 8 * n * n * 8
+
+
 def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, device: int = 0,
-                     metric: str = "cholesky", **kw) -> BatchResult:
-    """Converge a molecule set in groups of ``group_size`` molecules of similar
-    size (sorted by basis size so that padding stays small); the groups run one
-    after another on the device, results come back in the input order.  The
-    metric defaults to the device Cholesky fit (no host eigendecomposition)."""
+                     metric: str = "cholesky", memory_fraction: float = 0.5, **kw) -> BatchResult:
+    """Converge a molecule set in groups of at most ``group_size`` molecules of
+    similar size (sorted by basis size so that padding stays small) whose
+    estimated device memory stays within ``memory_fraction`` of the memory free
+    at the start; the groups run one after another on the device, results come
+    back in the input order.  The metric defaults to the device Cholesky fit (no
+    host eigendecomposition)."""
+    import torch
+
     kw["metric"] = metric
     run_kw = {k: kw.pop(k) for k in ("max_cycle", "acc_etot", "acc_rho", "acc_eev", "num_max_diis",
                                       "return_densities") if k in kw}
     guesses = kw.pop("initial_densities", None)
     sizes = [m.shells(basis).nfun for m in mols]
     order = sorted(range(len(mols)), key=lambda i: sizes[i])
+    torch.cuda.empty_cache()
+    budget = memory_fraction * torch.cuda.mem_get_info(device)[0]
+    prec = kw.get("precision", "fp64")
+    need = {i: device_bytes(sizes[i], mols[i].shells(auxbas).nfun, mols[i].nelec // 2, prec) for i in order}
+    groups, cur, used = [], [], 0
+    for i in order:  # consecutive molecules of similar size, within the count and memory limits
+        if cur and (len(cur) == group_size or used + need[i] > budget):
+            groups.append(cur)
+            cur, used = [], 0
+        cur.append(i)
+        used += need[i]
+    if cur:
+        groups.append(cur)
     energies, conv, iters = [None] * len(mols), [False] * len(mols), [0] * len(mols)
     nfp64, nsplit = [0] * len(mols), [0] * len(mols)
     dens = [None] * len(mols) if run_kw.get("return_densities") else []
     setup = scf = 0.0
-    for g0 in range(0, len(order), group_size):
-        idx = order[g0:g0 + group_size]
+    for idx in groups:
         b = BatchedRHF([mols[i] for i in idx], basis, auxbas, device=device, **kw)
         try:
             r = b.run(initial_densities=None if guesses is None else [guesses[i] for i in idx], **run_kw)
         finally:
             b.close()
+            torch.cuda.empty_cache()
         setup += r.setup_s
         scf += r.scf_s
         for j, i in enumerate(idx):

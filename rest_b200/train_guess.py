@@ -75,7 +75,14 @@ def main():
     ap.add_argument("--eval", type=int, default=32)
     ap.add_argument("--eval-kmin", type=int, default=13)
     ap.add_argument("--eval-kmax", type=int, default=24)
+    ap.add_argument("--eval-only", default=None, metavar="WEIGHTS",
+                    help="skip training: evaluate the weights in this file")
     a = ap.parse_args()
+    if a.eval_only:
+        guess = LearnedGuess.load(a.eval_only)
+        res = evaluate(guess, clusters(a.eval, a.eval_kmin, a.eval_kmax, a.seed + 7919))
+        print(json.dumps({"weights": a.eval_only, "eval": res}), flush=True)
+        return
     t0 = time.perf_counter()
     mols = clusters(a.train, 1, a.kmax, a.seed)
     res = run_molecule_set(mols, BASIS, AUXBAS, group_size=64, return_densities=True, **CRIT)

@@ -38,6 +38,7 @@ def test_batched_water_clusters_match_single_scf(ctx, precision):
     finally:
         batch.close()
     assert all(res.converged)
+    assert all(res.timings["density_checks"])
     if precision == "mixed":
         assert all(s > 0 for s in res.timings["split_k_builds"])
         assert all(f >= 2 for f in res.timings["fp64_k_builds"])
