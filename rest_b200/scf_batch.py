@@ -498,9 +498,9 @@ class BatchedRHF:
         ne_h, idem_h = ne.cpu().numpy(), idem.cpu().numpy()
         checks = []
         for i in range(B):
-            ok = abs(ne_h[i] - 2 * self.nocc[i]) < 1e-6 * max(1, 2 * self.nocc[i]) and idem_h[i] < 1e-6
-            checks.append(bool(ok))
-            conv[i] = conv[i] and ok
+            ok = bool(abs(ne_h[i] - 2 * self.nocc[i]) < 1e-6 * max(1, 2 * self.nocc[i]) and idem_h[i] < 1e-6)
+            checks.append(ok)
+            conv[i] = bool(conv[i] and ok)
         torch.cuda.synchronize()
         scf_s = time.perf_counter() - t0
         timings = {"fp64_k_builds": list(self._nfp64), "split_k_builds": list(self._nsplit),
