@@ -7,6 +7,7 @@
 #include <stdlib.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -21,6 +22,7 @@ namespace {
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  bool pooled = false;  // from the stream-ordered pool (freed with cudaFreeAsync)
 };
 
 int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
@@ -111,21 +113,26 @@ int cuda_fail(rijk_ctx* c, cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);  \
   } while (0)
 
+void free_buf(rijk_ctx* ctx, DevBuf& b) {
+  if (b.p) {
+    if (b.pooled)
+      cudaFreeAsync(b.p, ctx->stream);
+    else
+      cudaFree(b.p);
+  }
+  b.p = nullptr;
+  b.bytes = 0;
+  b.pooled = false;
+}
+
 // Frees the scratch only the metric step and the fit use (once per geometry):
 // the metric, its factor and inverse, the fit's output panel and large staging.
+// They come from the stream-ordered pool, so the frees are ordered after the
+// fit on the context's stream and need no device synchronisation.
 int release_fit_scratch(rijk_ctx* ctx) {
   if (ctx->pinned) return RIJK_OK;
-  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  for (DevBuf* b : {&ctx->mV, &ctx->mLinv, &ctx->mT, &ctx->mLinvd, &ctx->mOut}) {
-    if (b->p) cudaFree(b->p);
-    b->p = nullptr;
-    b->bytes = 0;
-  }
-  if (ctx->stage.bytes > ((size_t)256 << 20)) {
-    cudaFree(ctx->stage.p);
-    ctx->stage.p = nullptr;
-    ctx->stage.bytes = 0;
-  }
+  for (DevBuf* b : {&ctx->mV, &ctx->mLinv, &ctx->mT, &ctx->mLinvd, &ctx->mOut}) free_buf(ctx, *b);
+  if (ctx->stage.bytes > ((size_t)256 << 20)) free_buf(ctx, ctx->stage);
   return RIJK_OK;
 }
 
@@ -144,6 +151,28 @@ int ensure(rijk_ctx* ctx, DevBuf& b, size_t bytes) {
     return set_err(ctx, RIJK_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
   }
   b.bytes = bytes;
+  return RIJK_OK;
+}
+
+// Scratch used only by work on the context's own stream (staging, metric and
+// fit buffers) comes from the device's stream-ordered pool: allocation and
+// release are ordered on that stream, and the pool keeps freed memory for the
+// next geometry instead of unmapping it.
+int ensure_pooled(rijk_ctx* ctx, DevBuf& b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.bytes >= bytes) return RIJK_OK;
+  if (ctx->pinned)
+    return set_err(ctx, RIJK_ERR_TOO_LARGE,
+                   "buffers are pinned: this call needs " + std::to_string(bytes) + " bytes of scratch");
+  free_buf(ctx, b);
+  cudaError_t e = cudaMallocAsync(&b.p, bytes, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b.p = nullptr;
+    return set_err(ctx, RIJK_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  b.bytes = bytes;
+  b.pooled = true;
   return RIJK_OK;
 }
 
@@ -227,7 +256,7 @@ int upload_tensor(rijk_ctx* ctx, const double* host, int64_t n, int64_t naux, in
   const Geom& g = ctx->g;
   const int64_t row = kind == 0 ? g.npair : n * n;
   const int64_t rows_per = std::max<int64_t>(1, std::min<int64_t>(naux, ((int64_t)256 << 20) / (row * 8)));
-  RIJK_TRY(ensure(ctx, ctx->stage, (size_t)rows_per * row * 8));
+  RIJK_TRY(ensure_pooled(ctx, ctx->stage, (size_t)rows_per * row * 8));
   double* st = static_cast<double*>(ctx->stage.p);
   for (int64_t p0 = 0; p0 < naux; p0 += rows_per) {
     const int64_t np = std::min(rows_per, naux - p0);
@@ -244,8 +273,8 @@ int upload_tensor(rijk_ctx* ctx, const double* host, int64_t n, int64_t naux, in
 }
 
 int upload_square_padded(rijk_ctx* ctx, const double* host, int64_t n, int64_t np, DevBuf& dst) {
-  RIJK_TRY(ensure(ctx, ctx->stage, (size_t)n * n * 8));
-  RIJK_TRY(ensure(ctx, dst, (size_t)np * np * 8));
+  RIJK_TRY(ensure_pooled(ctx, ctx->stage, (size_t)n * n * 8));
+  RIJK_TRY(ensure_pooled(ctx, dst, (size_t)np * np * 8));
   RIJK_CK(cudaMemcpyAsync(ctx->stage.p, host, (size_t)n * n * 8, cudaMemcpyHostToDevice, ctx->stream));
   rijk::launch_pad_matrix(static_cast<double*>(ctx->stage.p), n, np, static_cast<double*>(dst.p), ctx->stream);
   return after_launch(ctx, "pad metric");
@@ -267,7 +296,7 @@ int fit_in_place(rijk_ctx* ctx, const double* dF, int64_t ldf, int tb, int klim)
   const int64_t np = ctx->naux_pad;
   int64_t chunk = std::max<int64_t>(1024, (((int64_t)512 << 20) / (np * 8)) / 1024 * 1024);
   chunk = std::min(chunk, g.ldB);
-  RIJK_TRY(ensure(ctx, ctx->mOut, (size_t)chunk * np * 8));
+  RIJK_TRY(ensure_pooled(ctx, ctx->mOut, (size_t)chunk * np * 8));
   double* out = static_cast<double*>(ctx->mOut.p);
   for (int64_t k0 = 0; k0 < g.ldB; k0 += chunk) {
     const int64_t kc = std::min(chunk, g.ldB - k0);
@@ -430,6 +459,25 @@ const char* rijk_status_string(int status) {
   }
 }
 
+namespace {
+// The stream-ordered pool returns freed memory to the system at every
+// synchronisation unless told otherwise; let it keep up to 8 GiB for this
+// process so that the next geometry's scratch comes back without new mappings.
+void keep_pool_memory(int device) {
+  static std::mutex mu;
+  static std::vector<int> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (std::find(done.begin(), done.end(), device) != done.end()) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = (uint64_t)8 << 30;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  done.push_back(device);
+}
+}  // namespace
+
 int rijk_ctx_create(int device, rijk_ctx** out) {
   if (!out) return RIJK_ERR_ARG;
   *out = nullptr;
@@ -438,9 +486,9 @@ int rijk_ctx_create(int device, rijk_ctx** out) {
     cudaGetLastError();
     return RIJK_ERR_CUDA;
   }
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return RIJK_ERR_CUDA;
-  if (prop.major != 10) return RIJK_ERR_CUDA;  // built for sm_100a only
+  int major = 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess) return RIJK_ERR_CUDA;
+  if (major != 10) return RIJK_ERR_CUDA;  // built for sm_100a only
   if (cudaSetDevice(device) != cudaSuccess) return RIJK_ERR_CUDA;
   rijk_ctx* c = new rijk_ctx();
   c->device = device;
@@ -450,9 +498,16 @@ int rijk_ctx_create(int device, rijk_ctx** out) {
     const long long v = atoll(s);
     if (v > (1 << 20)) c->scratch_budget = (size_t)v;
   }
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess || cudaMalloc(&c->d_info, sizeof(int)) != cudaSuccess ||
-      cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess || cudaMemset(c->d_info, 0, sizeof(int)) != cudaSuccess) {
+  keep_pool_memory(device);
+  // the timeout flag and the Cholesky pivot share one allocation (d_err owns it)
+  bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaMalloc(&c->d_err, 2 * sizeof(int)) == cudaSuccess;
+  if (ok) {
+    c->d_info = c->d_err + 1;
+    ok = cudaMemsetAsync(c->d_err, 0, 2 * sizeof(int), c->stream) == cudaSuccess &&
+         cudaStreamSynchronize(c->stream) == cudaSuccess;
+  }
+  if (!ok) {
     rijk_ctx_destroy(c);
     return RIJK_ERR_CUDA;
   }
@@ -468,16 +523,15 @@ int rijk_ctx_destroy(rijk_ctx* ctx) {
                     &ctx->dout,  &ctx->docc, &ctx->mV, &ctx->mLinv, &ctx->mT, &ctx->mLinvd, &ctx->mOut,
                     &ctx->Cr,    &ctx->Y,    &ctx->Yp, &ctx->tcBhi, &ctx->tcBlo, &ctx->tcVhi, &ctx->tcVlo,
                     &ctx->tcXhi, &ctx->tcXlo, &ctx->tcPart};
-  for (DevBuf* b : bufs)
-    if (b->p) cudaFree(b->p);
+  for (DevBuf* b : bufs) free_buf(ctx, *b);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto& r : ctx->prof_pending) {
     cudaEventDestroy(r.a);
     cudaEventDestroy(r.b);
   }
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->dB) cudaFree(ctx->dB);
-  if (ctx->d_err) cudaFree(ctx->d_err);
-  if (ctx->d_info) cudaFree(ctx->d_info);
+  if (ctx->d_err) cudaFree(ctx->d_err);  // d_info lives in the same allocation
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return RIJK_OK;
@@ -656,7 +710,7 @@ int rijk_get_rimatr(rijk_ctx* ctx, double* rimatr) {
   if (!rimatr) return set_err(ctx, RIJK_ERR_ARG, "null argument");
   const Geom& g = ctx->g;
   const int64_t rows_per = std::max<int64_t>(1, std::min<int64_t>(g.naux, ((int64_t)256 << 20) / (g.npair * 8)));
-  RIJK_TRY(ensure(ctx, ctx->stage, (size_t)rows_per * g.npair * 8));
+  RIJK_TRY(ensure_pooled(ctx, ctx->stage, (size_t)rows_per * g.npair * 8));
   double* st = static_cast<double*>(ctx->stage.p);
   for (int64_t p0 = 0; p0 < g.naux; p0 += rows_per) {
     const int64_t np = std::min(rows_per, g.naux - p0);
@@ -674,9 +728,9 @@ namespace {
 // factor V = L L^T, invert L and fit B = int3c L^-T in place.
 int cholesky_fit(rijk_ctx* ctx, int64_t* failed_pivot) {
   const int64_t np = ctx->naux_pad;
-  RIJK_TRY(ensure(ctx, ctx->mLinvd, (size_t)np * rijk::TS * 8));
-  RIJK_TRY(ensure(ctx, ctx->mLinv, (size_t)np * np * 8));
-  RIJK_TRY(ensure(ctx, ctx->mT, (size_t)np * np * 8));
+  RIJK_TRY(ensure_pooled(ctx, ctx->mLinvd, (size_t)np * rijk::TS * 8));
+  RIJK_TRY(ensure_pooled(ctx, ctx->mLinv, (size_t)np * np * 8));
+  RIJK_TRY(ensure_pooled(ctx, ctx->mT, (size_t)np * np * 8));
   double* V = static_cast<double*>(ctx->mV.p);
   double* Linvd = static_cast<double*>(ctx->mLinvd.p);
   double* Linv = static_cast<double*>(ctx->mLinv.p);
@@ -767,7 +821,7 @@ int rijk_build_rimatr_from_shells(rijk_ctx* ctx, const rijk_shells* bas, const r
   // large runs keep every class kernel's grid wide
   const size_t chunk_bytes = std::max<size_t>(std::min<size_t>(ctx->scratch_budget / 2, (size_t)naux * g.npair * 8),
                                               (size_t)9 * g.npair * 8);
-  RIJK_TRY(ensure(ctx, ctx->stage, std::max<size_t>(chunk_bytes, (size_t)naux * naux * 8)));
+  RIJK_TRY(ensure_pooled(ctx, ctx->stage, std::max<size_t>(chunk_bytes, (size_t)naux * naux * 8)));
   double* st = static_cast<double*>(ctx->stage.p);
   const int nsh = rijk::ri_plan_aux_shells(pg.p);
   for (int k0 = 0; k0 < nsh;) {
@@ -792,7 +846,7 @@ int rijk_build_rimatr_from_shells(rijk_ctx* ctx, const rijk_shells* bas, const r
     ctx->have = true;
     return release_fit_scratch(ctx);
   }
-  RIJK_TRY(ensure(ctx, ctx->mV, (size_t)npad * npad * 8));
+  RIJK_TRY(ensure_pooled(ctx, ctx->mV, (size_t)npad * npad * 8));
   rijk::launch_int2c2e(pg.p, st, naux, ctx->stream);
   RIJK_TRY(after_launch(ctx, "int2c2e"));
   rijk::launch_pad_matrix(st, naux, npad, static_cast<double*>(ctx->mV.p), ctx->stream);

@@ -13,6 +13,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -216,11 +217,16 @@ __global__ void __launch_bounds__(64) k_int2c2e(DShells Cs, int nshell, int64_t 
 // Device copy of an (AO, auxiliary) pair of shell sets.  AO shell pairs are
 // ordered by (l_i, l_j) so that a warp mostly runs one angular class.
 struct RiIntPlan {
-  std::vector<void*> bufs;
+  // Every device array of the plan lives in one allocation from the
+  // stream-ordered pool, filled by one copy and released in stream order.
+  std::vector<unsigned char> host;  // staging image of that allocation
+  std::vector<std::pair<const void**, size_t>> fixups;  // pointer field -> byte offset
+  void* base = nullptr;
+  cudaStream_t stream = nullptr;
   DShells A{}, C{};
   std::vector<int64_t> offA, offC;
   int64_t nA = 0, nC = 0;
-  const int* dpi = nullptr;  // shell pairs sorted by (l_i, l_j, primitive count)
+  const int* dpi = nullptr;  // shell pairs sorted by (l_i, l_j, primitive count, separation)
   const int* dpj = nullptr;
   int npairs = 0;
   int pair_cls[10] = {};  // pairs of class la * 3 + lb are [pair_cls[c], pair_cls[c + 1])
@@ -228,18 +234,26 @@ struct RiIntPlan {
   int aux_l_begin[GLC + 2] = {};
   const int* daux = nullptr;
   ~RiIntPlan() {
-    for (void* p : bufs) cudaFree(p);
+    if (base) cudaFreeAsync(base, stream);
   }
   template <class T>
-  const T* up(const T* h, size_t n) {
-    void* p = nullptr;
-    if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
+  void up(const T*& field, const T* h, size_t n) {
+    const size_t off = (host.size() + 255) / 256 * 256;
+    host.resize(off + std::max<size_t>(n, 1) * sizeof(T));
+    if (n) std::memcpy(host.data() + off, h, n * sizeof(T));
+    fixups.push_back({reinterpret_cast<const void**>(&field), off});
+  }
+  int finalize(cudaStream_t st) {
+    stream = st;
+    if (cudaMallocAsync(&base, host.size(), st) != cudaSuccess) {
       cudaGetLastError();
-      return nullptr;
+      base = nullptr;
+      return RIJK_ERR_NOMEM;
     }
-    bufs.push_back(p);
-    if (n && cudaMemcpy(p, h, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
-    return static_cast<const T*>(p);
+    if (cudaMemcpyAsync(base, host.data(), host.size(), cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return RIJK_ERR_CUDA;
+    for (auto& f : fixups) *f.first = static_cast<unsigned char*>(base) + f.second;
+    return RIJK_OK;
   }
   int load(const rijk_shells* s, int lmax, DShells& d, std::vector<int64_t>& off, int64_t& nfun) {
     if (!s || s->nshell <= 0 || !s->l || !s->nprim || !s->prim_off || !s->exps || !s->coefs || !s->centers)
@@ -257,14 +271,14 @@ struct RiIntPlan {
     }
     off[s->nshell] = nfun;
     d.nshell = (int)s->nshell;
-    d.l = up(s->l, s->nshell);
-    d.nprim = up(s->nprim, s->nshell);
-    d.prim_off = up(s->prim_off, s->nshell);
-    d.exps = up(s->exps, nprim_tot);
-    d.coefs = up(s->coefs, nprim_tot);
-    d.centers = up(s->centers, 3 * s->nshell);
-    d.fun_off = up(off.data(), s->nshell + 1);
-    return (d.l && d.nprim && d.prim_off && d.exps && d.coefs && d.centers && d.fun_off) ? RIJK_OK : RIJK_ERR_NOMEM;
+    up(d.l, s->l, s->nshell);
+    up(d.nprim, s->nprim, s->nshell);
+    up(d.prim_off, s->prim_off, s->nshell);
+    up(d.exps, s->exps, nprim_tot);
+    up(d.coefs, s->coefs, nprim_tot);
+    up(d.centers, s->centers, 3 * s->nshell);
+    up(d.fun_off, (const int64_t*)off.data(), s->nshell + 1);
+    return RIJK_OK;
   }
 };
 
@@ -340,8 +354,7 @@ int ri_plan_create(const rijk_shells* bas, const rijk_shells* aux, const double*
       while (t < p->C.nshell && aux->l[p->aux_sorted[t]] < l) ++t;
       p->aux_l_begin[l] = t;
     }
-    p->daux = p->up(p->aux_sorted.data(), p->aux_sorted.size());
-    if (!p->daux) rc = RIJK_ERR_NOMEM;
+    p->up(p->daux, (const int*)p->aux_sorted.data(), p->aux_sorted.size());
   }
   if (rc == RIJK_OK && bas) {
     rc = p->load(bas, GLA, p->A, p->offA, p->nA);
@@ -379,11 +392,11 @@ int ri_plan_create(const rijk_shells* bas, const rijk_shells* aux, const double*
         while (t < p->npairs && bas->l[si[t]] * 3 + bas->l[sj[t]] < c) ++t;
         p->pair_cls[c] = t;
       }
-      p->dpi = p->up(si.data(), si.size());
-      p->dpj = p->up(sj.data(), sj.size());
-      if (!p->dpi || !p->dpj) rc = RIJK_ERR_NOMEM;
+      p->up(p->dpi, (const int*)si.data(), si.size());
+      p->up(p->dpj, (const int*)sj.data(), sj.size());
     }
   }
+  if (rc == RIJK_OK) rc = p->finalize(st);
   if (rc != RIJK_OK) {
     delete p;
     return rc;
