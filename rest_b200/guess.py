@@ -128,83 +128,104 @@ class PairSet:
 
 def pair_features(mol) -> PairSet:
     xyz, frames = water_frames(mol)
+    origin = np.array([o for o, _ in frames])
+    Fs = np.stack([F for _, F in frames])
     na = len(mol.symbols)
     typ = np.array([ELEMENT[s] for s in mol.symbols])
     d = np.linalg.norm(xyz[:, None] - xyz[None], axis=-1)
-    env = np.zeros((na, 16))
-    for a in range(na):
-        others = np.arange(na) != a
-        for t in (0, 1):
-            sel = others & (typ == t)
-            env[a, 8 * t:8 * t + 8] = _radial(d[a, sel]).sum(axis=0)
+    rad = _radial(d) * (1.0 - np.eye(na))[:, :, None]  # no self term
+    env = np.concatenate([rad[:, typ == 0].sum(axis=1), rad[:, typ == 1].sum(axis=1)], axis=1)
     A, B = np.nonzero(d <= CUTOFF)
-    feats = np.zeros((len(A), NFEAT))
-    for p, (a, b) in enumerate(zip(A, B)):
-        wa, wb = a // 3, b // 3
-        o, F = frames[wa]
-        f = [np.eye(2)[typ[a]], np.eye(2)[typ[b]]]
-        db = F @ (xyz[b] - xyz[a])
-        f += [db, [np.linalg.norm(db)], [1.0 if wa == wb else 0.0]]
-        f += [F @ (xyz[3 * wb + j] - xyz[a]) for j in range(3)]
-        f += [F @ (xyz[a] - o), env[a], env[b]]
-        feats[p] = np.concatenate(f)
+    wa, wb = A // 3, B // 3
+    F = Fs[wa]
+    db = np.einsum("pij,pj->pi", F, xyz[B] - xyz[A])
+    wat = xyz[3 * wb[:, None] + np.arange(3)] - xyz[A][:, None, :]  # B's water, relative to A
+    wat = np.einsum("pij,pkj->pki", F, wat).reshape(len(A), 9)
+    own = np.einsum("pij,pj->pi", F, xyz[A] - origin[wa])
+    eye = np.eye(2)
+    feats = np.concatenate([eye[typ[A]], eye[typ[B]], db, np.linalg.norm(db, axis=1)[:, None],
+                            (wa == wb).astype(float)[:, None], wat, own, env[A], env[B]], axis=1)
     return PairSet(feats, np.stack([A, B], axis=1), 2 * typ[A] + typ[B])
 
 
 class Rotator:
-    """G_X(F_w): rotation of atom X's AO block into the frame of water w (cached)."""
+    """Per water w and element: G(F_w), the rotation of that element's AO block
+    into the water's frame (every atom of an element has the same shells)."""
 
     def __init__(self, mol, sh):
-        self.frames = [F for _, F in water_frames(mol)[1]]
+        Fs = np.stack([F for _, F in water_frames(mol)[1]])
         self.layout = atom_layout(sh)
-        self._shell = {}
-        self._atom = {}
+        typ = np.array([ELEMENT[s] for s in mol.symbols])
+        self.typ = typ
+        self.first = np.array([self.layout[a][0] for a in range(len(typ))])
+        self.size, self.rot = {}, {}
+        rots = {l: shell_rotations(l, Fs) for l in range(3)}
+        for t in (0, 1):
+            atoms = np.nonzero(typ == t)[0]
+            if atoms.size == 0:
+                continue
+            shells = {self.layout[a][2] for a in atoms}
+            if len(shells) != 1:
+                raise ValueError("atoms of one element must carry the same shells")
+            ls = shells.pop()
+            self.size[t] = sum(2 * l + 1 for l in ls)
+            g = np.zeros((len(Fs), self.size[t], self.size[t]))
+            o = 0
+            for l in ls:
+                g[:, o:o + 2 * l + 1, o:o + 2 * l + 1] = rots[l]
+                o += 2 * l + 1
+            self.rot[t] = g
 
-    def __call__(self, atom: int, w: int) -> np.ndarray:
-        key = (atom, w)
-        if key not in self._atom:
-            if w not in self._shell:
-                self._shell[w] = {l: shell_rotation(l, self.frames[w]) for l in range(3)}
-            self._atom[key] = atom_rotation(self.layout[atom][2], self._shell[w])
-        return self._atom[key]
+    def kinds(self, ps: PairSet):
+        """(selection, rows (P,na), cols (P,nb), G_A (P,na,na), G_B (P,nb,nb)) per element pair."""
+        for k in range(4):
+            sel = np.nonzero(ps.kind == k)[0]
+            if sel.size == 0:
+                continue
+            ta, tb = k // 2, k % 2
+            a, b = ps.pairs[sel, 0], ps.pairs[sel, 1]
+            w = a // 3
+            rows = self.first[a][:, None] + np.arange(self.size[ta])
+            cols = self.first[b][:, None] + np.arange(self.size[tb])
+            yield sel, rows, cols, self.rot[ta][w], self.rot[tb][w]
+
+
+def shell_rotations(l: int, Fs: np.ndarray) -> np.ndarray:
+    """shell_rotation for a stack of frames: (nw, 2l+1, 2l+1)."""
+    if l == 0:
+        return np.ones((len(Fs), 1, 1))
+    pinv = np.linalg.pinv(_harmonics(l, _SAMPLES))
+    y_rot = np.stack([_harmonics(l, _SAMPLES @ F) for F in Fs])
+    return np.transpose(pinv @ y_rot, (0, 2, 1))
 
 
 def local_blocks(mol, sh, D: np.ndarray, ps: PairSet):
     """Targets: G_A^T D_AB G_B in A's water frame, padded to 14 x 14, with masks."""
     rot = Rotator(mol, sh)
-    lay = rot.layout
-    T = np.zeros((len(ps.pairs), BLOCK * BLOCK))
+    T = np.zeros((len(ps.pairs), BLOCK, BLOCK))
     M = np.zeros_like(T)
-    for p, (a, b) in enumerate(ps.pairs):
-        w = a // 3
-        oa, na_, _ = lay[a]
-        ob, nb_, _ = lay[b]
-        blk = rot(a, w).T @ D[oa:oa + na_, ob:ob + nb_] @ rot(b, w)
-        t = np.zeros((BLOCK, BLOCK))
-        m = np.zeros((BLOCK, BLOCK))
-        t[:na_, :nb_] = blk
-        m[:na_, :nb_] = 1.0
-        T[p], M[p] = t.ravel(), m.ravel()
-    return T, M
+    for sel, rows, cols, ga, gb in rot.kinds(ps):
+        blk = D[rows[:, :, None], cols[:, None, :]]
+        T[sel, :rows.shape[1], :cols.shape[1]] = np.transpose(ga, (0, 2, 1)) @ blk @ gb
+        M[sel, :rows.shape[1], :cols.shape[1]] = 1.0
+    return T.reshape(len(ps.pairs), -1), M.reshape(len(ps.pairs), -1)
 
 
 def assemble_density(mol, sh, ps: PairSet, blocks: np.ndarray) -> np.ndarray:
     """Rotate predicted local blocks back, D_AB = G_A B G_B^T, and average the
     (A, B) and (B, A)^T predictions; pairs beyond the cutoff stay zero."""
     rot = Rotator(mol, sh)
-    lay = rot.layout
     n = sh.nfun
     D = np.zeros((n, n))
     cnt = np.zeros((n, n))
-    for p, (a, b) in enumerate(ps.pairs):
-        w = a // 3
-        oa, na_, _ = lay[a]
-        ob, nb_, _ = lay[b]
-        full = rot(a, w) @ blocks[p].reshape(BLOCK, BLOCK)[:na_, :nb_] @ rot(b, w).T
-        D[oa:oa + na_, ob:ob + nb_] += full
-        cnt[oa:oa + na_, ob:ob + nb_] += 1.0
-        D[ob:ob + nb_, oa:oa + na_] += full.T
-        cnt[ob:ob + nb_, oa:oa + na_] += 1.0
+    blocks = blocks.reshape(len(ps.pairs), BLOCK, BLOCK)
+    for sel, rows, cols, ga, gb in rot.kinds(ps):
+        full = ga @ blocks[sel, :rows.shape[1], :cols.shape[1]] @ np.transpose(gb, (0, 2, 1))
+        r, c = rows[:, :, None], cols[:, None, :]
+        np.add.at(D, (r, c), full)
+        np.add.at(cnt, (r, c), 1.0)
+        np.add.at(D, (c.transpose(0, 2, 1), r.transpose(0, 2, 1)), np.transpose(full, (0, 2, 1)))
+        np.add.at(cnt, (c.transpose(0, 2, 1), r.transpose(0, 2, 1)), 1.0)
     return D / np.maximum(cnt, 1.0)
 
 
