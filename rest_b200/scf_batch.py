@@ -59,8 +59,8 @@ class BatchResult:
 
 class BatchedRHF:
     def __init__(self, mols: list, basis: str, auxbas: str, device: int = 0, metric: str = "inv_sqrt",
-                 precision: str = "fp64", integrals: str = "auto", rebuild_every: int = 8,
-                 switch_etot: float = 1e-5, switch_rho: float = 1e-4, eig_workers: int = 8,
+                 precision: str = "fp64", integrals: str = "auto", rebuild_every: int = 16,
+                 switch_etot: float = 1e-7, switch_rho: float = 1e-5, eig_workers: int = 8,
                  graphs: bool = False, split_min_basis: int = 512):
         import torch
 
