@@ -177,6 +177,14 @@ class Molecule:
         return e
 
     def shells(self, basis: str) -> ShellSet:
+        """The molecule's shells in ``basis`` (built once per basis and cached;
+        the molecule's geometry is not meant to change after construction)."""
+        cache = self.__dict__.setdefault("_shell_cache", {})
+        if basis not in cache:
+            cache[basis] = self._build_shells(basis)
+        return cache[basis]
+
+    def _build_shells(self, basis: str) -> ShellSet:
         data = load_basis(basis)
         ls, nps, offs, exps, coefs, ctrs, atoms = [], [], [], [], [], [], []
         off = 0
