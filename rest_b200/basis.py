@@ -275,3 +275,36 @@ def int3c2e_dev(bas: ShellSet, aux: ShellSet, stream=None):
     _check(lib().rijk_int3c2e_dev(C.byref(bas.cstruct()), C.byref(aux.cstruct()), _C2S_PTRS,
                                   C.c_void_p(out.data_ptr()), C.c_void_p(st)), "int3c2e_dev")
     return out
+
+
+# A nucleus as an s Gaussian of this exponent, normalised to its charge, is a
+# point charge to double precision: in the three-centre kernel the product
+# exponent p g / (p + g) evaluates to p because p + g rounds to g.
+POINT_CHARGE_EXPONENT = 1.0e20
+
+
+def point_charges(mol: Molecule) -> ShellSet:
+    """The nuclei as auxiliary s shells carrying -Z (divided by the l = 0 solid
+    harmonic factor that the three-centre engine applies)."""
+    z = np.asarray(mol.charges, dtype=np.float64)
+    na = len(z)
+    g = POINT_CHARGE_EXPONENT
+    coef = -z * (g / np.pi) ** 1.5 / _C2S[0][0, 0]
+    return ShellSet(np.zeros(na, dtype=np.int32), np.ones(na, dtype=np.int32), np.arange(na, dtype=np.int64),
+                    np.full(na, g), np.ascontiguousarray(coef), np.ascontiguousarray(mol.coords, dtype=np.float64),
+                    np.arange(na, dtype=np.int64))
+
+
+def int1e_nuclear_dev(mol: Molecule, sh: ShellSet, stream=None):
+    """Nuclear attraction sum_C -Z_C (mu|1/|r - C||nu) on the current CUDA device,
+    as the three-centre integrals with point charges summed over the nuclei: a
+    torch float64 (n, n) tensor (the host engine's int1e(..., "nuclear"))."""
+    import torch
+
+    n = sh.nfun
+    v = int3c2e_dev(sh, point_charges(mol), stream).sum(dim=0)  # packed upper, (i <= j) at j(j+1)/2 + i
+    tri = torch.tril_indices(n, n, device=v.device)
+    out = torch.zeros((n, n), dtype=torch.float64, device=v.device)
+    out[tri[1], tri[0]] = v
+    out[tri[0], tri[1]] = v
+    return out

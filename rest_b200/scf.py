@@ -25,7 +25,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import scipy.linalg as sla
 
-from .basis import DEVICE_MAX_L_AO, DEVICE_MAX_L_AUX, Molecule, int1e, int2c2e, int2c2e_dev, int3c2e
+from .basis import DEVICE_MAX_L_AO, DEVICE_MAX_L_AUX, Molecule, int1e, int1e_nuclear_dev, int2c2e, int2c2e_dev, int3c2e
 from .rijk import RIJK
 
 AUXBAS_THRESHOLD = 1.0e-8  # src/constants/mod.rs:81
@@ -128,15 +128,19 @@ class SCF:
         self.n, self.naux = self.bas.nfun, self.aux.nfun
         self.nuc_energy = mol.nuclear_repulsion()
         self.ovlp = int1e(mol, self.bas, "ovlp")
-        self.h_core = int1e(mol, self.bas, "kinetic") + int1e(mol, self.bas, "nuclear")
+        if self.opts.metric not in ("inv_sqrt", "cholesky"):
+            raise ValueError(f"unknown metric {self.opts.metric!r}")
+        self.integrals_on = self._integral_engine()
+        if self.integrals_on == "device":  # nuclear attraction through the device three-centre engine
+            nuc = int1e_nuclear_dev(mol, self.bas).cpu().numpy()
+        else:
+            nuc = int1e(mol, self.bas, "nuclear")
+        self.h_core = int1e(mol, self.bas, "kinetic") + nuc
         lam = np.linalg.eigvalsh(self.ovlp)
         if lam[0] <= 1e-10:
             raise ValueError(f"overlap matrix is singular (lowest eigenvalue {lam[0]:.3e})")
         self.ovlp_lowest_eig = float(lam[0])
         t1 = time.perf_counter()
-        if self.opts.metric not in ("inv_sqrt", "cholesky"):
-            raise ValueError(f"unknown metric {self.opts.metric!r}")
-        self.integrals_on = self._integral_engine()
         if self.integrals_on == "device":
             # integrals, metric and fit on the device; V^-1/2 needs V on the host
             factor = None

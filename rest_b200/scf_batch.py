@@ -40,7 +40,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .basis import DEVICE_MAX_L_AO, DEVICE_MAX_L_AUX, int1e, int2c2e, int2c2e_dev, int3c2e
+from .basis import DEVICE_MAX_L_AO, DEVICE_MAX_L_AUX, int1e, int1e_nuclear_dev, int2c2e, int2c2e_dev, int3c2e
 from .geometry import alkane, water_cluster  # noqa: F401  (re-exported)
 from .rijk import RIJK
 from .scf import metric_inv_sqrt, metric_inv_sqrt_dev
@@ -91,10 +91,13 @@ class BatchedRHF:
             bas, aux = mol.shells(basis), mol.shells(auxbas)
             n = bas.nfun
             s = int1e(mol, bas, "ovlp")
-            h = int1e(mol, bas, "kinetic") + int1e(mol, bas, "nuclear")
             ctx = RIJK(device)
             on_device = integrals == "device" or (
                 integrals == "auto" and int(bas.l.max()) <= DEVICE_MAX_L_AO and int(aux.l.max()) <= DEVICE_MAX_L_AUX)
+            if on_device:  # kinetic on the host, nuclear attraction on the device
+                h = torch.as_tensor(int1e(mol, bas, "kinetic"), device=self.dev) + int1e_nuclear_dev(mol, bas)
+            else:
+                h = int1e(mol, bas, "kinetic") + int1e(mol, bas, "nuclear")
             if on_device:
                 factor = metric_inv_sqrt_dev(int2c2e_dev(aux)) if metric == "inv_sqrt" else None
                 ctx.build_rimatr_from_shells(bas, aux, factor)

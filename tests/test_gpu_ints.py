@@ -103,3 +103,17 @@ def test_device_engine_rejects_high_angular_momentum(ctx):
     ctx.build_rimatr_from_shells(bas, aux)
     assert ctx.num_basis == bas.nfun
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("name", ["water", "cluster3"])
+@pytest.mark.parametrize("basis", ["def2-SVP", "STO-3G"])
+def test_nuclear_attraction_from_point_charges_matches_host(name, basis):
+    """Nuclear attraction through the device three-centre engine, each nucleus an
+    s Gaussian of exponent 1e20 (a point charge to double precision)."""
+    from rest_b200.basis import int1e, int1e_nuclear_dev
+
+    mol = _molecule(name)
+    bas = mol.shells(basis)
+    ref = int1e(mol, bas, "nuclear")
+    got = int1e_nuclear_dev(mol, bas).cpu().numpy()
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
