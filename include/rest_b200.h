@@ -79,13 +79,14 @@ enum rijk_prof_class {
   RIJK_PROF_NCLASS = 7
 };
 /* CTA shapes of the K kernels (results agree to rounding across them), for
- * both the half-transform and the updates; DMMA warps of 32x32 outputs:
+ * both the half-transform and the updates; DMMA warps of 32x32 outputs unless noted:
  * 0: 64x64, 4 warps, cp.async staging, 3 stages (2 CTAs/SM); 1: 64x64,
  * cp.async, 2 stages (3 CTAs/SM, the default); 2: 64x64, cp.async, 4 stages
  * (1 CTA/SM); 3: 64x64, bulk copies issued by a producer warp, 3 stages;
- * 4: 128x64, 8 warps, cp.async, 2 stages (2 CTAs/SM).  RIJK_HT_CFG /
- * RIJK_RK_CFG override the defaults at context creation. */
-#define RIJK_TILE_CFGS 5
+ * 4: 128x64, 8 warps, cp.async, 2 stages (2 CTAs/SM); 5: 64x128, 4 warps of
+ * 32x64 outputs, cp.async, 2 stages (2 CTAs/SM).  RIJK_HT_CFG / RIJK_RK_CFG
+ * override the defaults at context creation. */
+#define RIJK_TILE_CFGS 6
 int rijk_ctx_set_tiles(rijk_ctx* ctx, int half_transform_cfg, int update_cfg);
 /* Autotuner: times every CTA shape of the half-transform and of the rank
  * update on sample_rows aux rows (<= 0: 512) of the loaded tensor with ncols

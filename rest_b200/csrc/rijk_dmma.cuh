@@ -236,24 +236,28 @@ __device__ __forceinline__ void cpa_issue_stage(const Sched& sc, int kt, double*
   }
 }
 
-// One full k-tile (32 k) of a warp whose tile reads exactly one A slot and one
-// B slot, with the two slots' orientations fixed at compile time: every
-// fragment address is the warp's slot base plus an immediate offset.
+// One full k-tile (32 k) of a warp whose A slots (consecutive, from slot_a) all
+// have orientation TA and whose B slots (consecutive, from slot_b) all have
+// orientation TB: every fragment address is the warp's base plus an immediate.
 template <class Cfg, bool TA, bool TB>
-__device__ __forceinline__ void dmma_ktile_fixed(const double* __restrict__ sbase, int slot_a, int row_a,
-                                                 int slot_b, int col_b, int lane,
+__device__ __forceinline__ void dmma_ktile_fixed(const double* __restrict__ sbase, int slot_a, int slot_b, int lane,
                                                  double (&acc)[Cfg::FM][Cfg::FN][2]) {
   constexpr int AMST = TA ? SLD : 1, AKST = TA ? 1 : SLD;
   constexpr int BNST = TB ? 1 : SLD, BKST = TB ? SLD : 1;
-  const double* sa = sbase + slot_a * SLOT_DOUBLES + (row_a + (lane >> 2)) * AMST + (lane & 3) * AKST;
-  const double* sb = sbase + (Cfg::MT + slot_b) * SLOT_DOUBLES + (col_b + (lane >> 2)) * BNST + (lane & 3) * BKST;
+  constexpr int APS = Cfg::WTM >= TS ? Cfg::WTM / TS : 1;
+  constexpr int BPS = Cfg::WTN >= TS ? Cfg::WTN / TS : 1;
+  constexpr int FPA = Cfg::FM / APS, FPB = Cfg::FN / BPS;
+  const double* sa = sbase + slot_a * SLOT_DOUBLES + (lane >> 2) * AMST + (lane & 3) * AKST;
+  const double* sb = sbase + (Cfg::MT + slot_b) * SLOT_DOUBLES + (lane >> 2) * BNST + (lane & 3) * BKST;
 #pragma unroll
   for (int kk = 0; kk < TS / 4; ++kk) {
     double af[Cfg::FM], bf[Cfg::FN];
 #pragma unroll
-    for (int fm = 0; fm < Cfg::FM; ++fm) af[fm] = sa[(fm * 8) * AMST + (kk * 4) * AKST];
+    for (int fm = 0; fm < Cfg::FM; ++fm)
+      af[fm] = sa[(fm / FPA) * SLOT_DOUBLES + ((fm % FPA) * 8) * AMST + (kk * 4) * AKST];
 #pragma unroll
-    for (int fn = 0; fn < Cfg::FN; ++fn) bf[fn] = sb[(fn * 8) * BNST + (kk * 4) * BKST];
+    for (int fn = 0; fn < Cfg::FN; ++fn)
+      bf[fn] = sb[(fn / FPB) * SLOT_DOUBLES + ((fn % FPB) * 8) * BNST + (kk * 4) * BKST];
 #pragma unroll
     for (int fm = 0; fm < Cfg::FM; ++fm)
 #pragma unroll
@@ -320,19 +324,24 @@ __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktile
     }
     const int kk_lim = (kvalid(kt) + 3) / 4;
     const bool full = kk_lim == TS / 4 && fm_lim == Cfg::FM && fn_lim == Cfg::FN;
-    if constexpr (Cfg::WTM == TS && Cfg::WTN == TS) {
-      if (full) {
-        // the warp's one A slot and one B slot; their orientations are warp-uniform
-        const int sa = warp_m0 / TS, sbs = warp_n0 / TS;
-        const bool ta = fl[sa] != 0, tb = fl[Cfg::MT + sbs] != 0;
+    if constexpr (Cfg::WTM % TS == 0 && Cfg::WTN % TS == 0) {
+      // the warp's A slots and B slots; orientations are warp-uniform per slot
+      const int sa = warp_m0 / TS, sbs = warp_n0 / TS;
+      const bool ta = fl[sa] != 0, tb = fl[Cfg::MT + sbs] != 0;
+      bool uniform = true;
+#pragma unroll
+      for (int j = 1; j < APS; ++j) uniform = uniform && ((fl[sa + j] != 0) == ta);
+#pragma unroll
+      for (int j = 1; j < BPS; ++j) uniform = uniform && ((fl[Cfg::MT + sbs + j] != 0) == tb);
+      if (full && uniform) {
         if (!ta && !tb)
-          dmma_ktile_fixed<Cfg, false, false>(sbase, sa, 0, sbs, 0, lane, acc);
+          dmma_ktile_fixed<Cfg, false, false>(sbase, sa, sbs, lane, acc);
         else if (ta && !tb)
-          dmma_ktile_fixed<Cfg, true, false>(sbase, sa, 0, sbs, 0, lane, acc);
+          dmma_ktile_fixed<Cfg, true, false>(sbase, sa, sbs, lane, acc);
         else if (!ta && tb)
-          dmma_ktile_fixed<Cfg, false, true>(sbase, sa, 0, sbs, 0, lane, acc);
+          dmma_ktile_fixed<Cfg, false, true>(sbase, sa, sbs, lane, acc);
         else
-          dmma_ktile_fixed<Cfg, true, true>(sbase, sa, 0, sbs, 0, lane, acc);
+          dmma_ktile_fixed<Cfg, true, true>(sbase, sa, sbs, lane, acc);
         continue;
       }
     }

@@ -366,11 +366,13 @@ using HtCfg1 = DmmaCfg<2, 2, 2, 2, 2, true>;  // 64 x 64, cp.async, 2 stages (3 
 using HtCfg2 = DmmaCfg<2, 2, 2, 2, 4, true>;  // 64 x 64, cp.async, 4 stages (1 CTA/SM)
 using HtCfg3 = DmmaCfg<2, 2, 2, 2, 3>;        // 64 x 64, bulk copies + producer warp, 3 stages
 using HtCfg4 = DmmaCfg<4, 2, 4, 2, 2, true>;  // 128 x 64, 8 warps of 32 x 32, cp.async, 2 stages (2 CTAs/SM)
+using HtCfg5 = DmmaCfg<2, 4, 2, 2, 2, true>;  // 64 x 128, 4 warps of 32 x 64, cp.async, 2 stages (2 CTAs/SM)
 
-// Register budget: 256-thread shapes are held to 128 registers so that two CTAs fit an SM.
+// Register budget: two CTAs per SM for the 256-thread shape (128 registers) and
+// for the shape with 32 x 64 warp tiles (up to 255 registers).
 template <class Cfg>
 constexpr int min_ctas() {
-  return Cfg::THREADS >= 256 ? 2 : 1;
+  return (Cfg::THREADS >= 256 || Cfg::FM * Cfg::FN >= 32) ? 2 : 1;
 }
 
 struct HalfTransformSched {
@@ -443,6 +445,7 @@ void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t n
     case 2: return half_transform_cfg<HtCfg2>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
     case 3: return half_transform_cfg<HtCfg3>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
     case 4: return half_transform_cfg<HtCfg4>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
+    case 5: return half_transform_cfg<HtCfg5>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
     default: return half_transform_cfg<HtCfg0>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
   }
 }
@@ -455,9 +458,10 @@ using RkCfg1 = DmmaCfg<2, 2, 2, 2, 2, true>;  // 64 x 64, cp.async, 2 stages (3 
 using RkCfg2 = DmmaCfg<2, 2, 2, 2, 4, true>;  // 64 x 64, cp.async, 4 stages (1 CTA/SM)
 using RkCfg3 = DmmaCfg<2, 2, 2, 2, 3>;        // 64 x 64, bulk copies + producer warp, 3 stages
 using RkCfg4 = DmmaCfg<4, 2, 4, 2, 2, true>;  // 128 x 64, 8 warps, cp.async, 2 stages (2 CTAs/SM)
+using RkCfg5 = DmmaCfg<2, 4, 2, 2, 2, true>;  // 64 x 128, 4 warps of 32 x 64, cp.async, 2 stages (2 CTAs/SM)
 constexpr int KB = 128;                       // K block edge
 
-static int rk_subs(int cfg) { return cfg == 4 ? 2 : 4; }  // CTA sub-blocks of a 128 x 128 K block
+static int rk_subs(int cfg) { return cfg >= 4 ? 2 : 4; }  // CTA sub-blocks of a 128 x 128 K block
 static int rk_ctas_per_sm(int cfg) { return cfg == 1 ? 3 : cfg == 2 ? 1 : 2; }
 
 int64_t k_block_pairs(const Geom& g, int full) {
@@ -568,6 +572,7 @@ void launch_k_rank_update(const Geom& g, const double* X, int64_t ldx, int64_t s
     case 2: return rank_update_cfg<RkCfg2>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
     case 3: return rank_update_cfg<RkCfg3>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
     case 4: return rank_update_cfg<RkCfg4>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
+    case 5: return rank_update_cfg<RkCfg5>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
     default: return rank_update_cfg<RkCfg0>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
   }
 }
@@ -642,6 +647,7 @@ void launch_k_dm_update(const Geom& g, const double* T, int64_t ldt, int64_t stp
     case 2: return dm_update_cfg<RkCfg2>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
     case 3: return dm_update_cfg<RkCfg3>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
     case 4: return dm_update_cfg<RkCfg4>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
+    case 5: return dm_update_cfg<RkCfg5>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
     default: return dm_update_cfg<RkCfg0>(g, T, ldt, stp, B, p0, np, splits, full, Kpart, err, st);
   }
 }

@@ -45,7 +45,7 @@ def _rest_list(parts):
     return out
 
 
-TILE_CFGS = 5  # CTA shapes of the K kernels (RIJK_TILE_CFGS in include/rest_b200.h)
+TILE_CFGS = 6  # CTA shapes of the K kernels (RIJK_TILE_CFGS in include/rest_b200.h)
 
 
 class RIJK:

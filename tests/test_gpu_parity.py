@@ -278,7 +278,7 @@ def test_autotuner_picks_a_shape_and_keeps_results(ctx):
     ctx.set_rimatr(case.rimatr, n)
     try:
         bh, br, ms = ctx.autotune(nocc, 256)
-        assert 0 <= bh <= 4 and 0 <= br <= 4 and len(ms) == 5
+        assert 0 <= bh <= 5 and 0 <= br <= 5 and len(ms) == 6
         assert all(v[0] > 0 and v[1] > 0 for v in ms.values())
         assert ms[bh][0] == min(v[0] for v in ms.values())
         occ = np.full(nocc, 2.0)
@@ -303,7 +303,8 @@ def test_ao2mo_ri3mo(ctx, n, naux, rows, cols):
         assert _maxdiff(got[s], ref) <= TOL
 
 
-@pytest.mark.parametrize("ht,rk", [(0, 0), (1, 1), (2, 2), (3, 3), (4, 4), (2, 1), (1, 3), (4, 1), (1, 4)])
+@pytest.mark.parametrize("ht,rk", [(0, 0), (1, 1), (2, 2), (3, 3), (4, 4), (5, 5), (2, 1), (1, 3), (4, 1), (1, 4),
+                                   (5, 1), (1, 5)])
 def test_every_tile_shape_gives_the_same_k(ctx, ht, rk):
     n, naux, nocc = 150, 300, 40
     case = host_case(n, naux, nocc, seed=31)
