@@ -4,7 +4,7 @@ The batch advances water clusters of uneven size together (device integrals and
 J/K per molecule on its own stream, device Fock/DIIS/eigensolve on the padded
 batch).  FP64 and mixed precision (incremental split-precision K with FP64
 builds to convergence) must both reproduce the single-molecule driver's FP64
-energy to 1e-8 Eh (the north-star bar is 1e-6 Eh); all-split builds only to
+energy to 1e-8 Eh (the accuracy asked of the mixed path is 1e-6 Eh); all-split builds only to
 their ~1e-5 relative accuracy.
 """
 import pytest
