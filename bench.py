@@ -533,7 +533,7 @@ def measure_alkanes(device: int, sizes=(10, 20, 40)) -> list:
         rec = {"molecule": f"C{nc}H{2 * nc + 2}", "num_basis": mol.shells("def2-SVP").nfun,
                "num_auxbas": mol.shells("def2-SVP-JKFIT").nfun, "nocc": mol.nelec // 2}
         for prec in ("fp64", "mixed"):
-            # split_min_basis=0: the split path on every alkane (the driver's default
+            # split_min_basis=0: the split path on every alkane (BatchedRHF's default
             # keeps molecules below 512 basis functions in FP64)
             b = BatchedRHF([mol], "def2-SVP", "def2-SVP-JKFIT", device=device, precision=prec, metric="cholesky",
                            split_min_basis=0)
