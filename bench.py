@@ -212,21 +212,12 @@ def run_ours(args, w):
     import numpy as np
     import torch
 
-    from rest_b200 import RIJK, lib
+    from rest_b200 import RIJK, lib, replicas
     from rest_b200.synth import device_case
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-        pg = dist
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rk = replicas.init("nccl", timeout_s=600)
+    world, rank, local = rk.world, rk.rank, rk.local
 
     fp64_peak = measure_dgemm_peak(torch)
     ctx = RIJK(local)
@@ -245,8 +236,7 @@ def run_ours(args, w):
 
     def barrier():
         torch.cuda.synchronize()
-        if pg:
-            pg.barrier()
+        replicas.barrier(rk)
 
     for _ in range(max(3, args.warmup)):
         step()
@@ -266,11 +256,7 @@ def run_ours(args, w):
     ctx.synchronize(st)
     prof = ctx.profile_read()
     ctx.profile(False)
-    dt = e0.elapsed_time(e1) / 1e3
-    if pg:
-        t = torch.tensor([dt], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        dt = float(t)
+    dt = replicas.max_over_ranks(rk, e0.elapsed_time(e1) / 1e3)  # the slowest rank's device time
     t_step = dt / args.steps
     flops = w["j_flops"] + w["k_flops"]
     value = world * flops / t_step / 1e12
@@ -380,11 +366,7 @@ def run_ours(args, w):
         t0 = time.perf_counter()
         for _ in range(args.steps):
             e2e_step()
-        te = time.perf_counter() - t0
-        if pg:
-            t = torch.tensor([te], dtype=torch.float64, device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            te = float(t)
+        te = replicas.max_over_ranks(rk, time.perf_counter() - t0)
         h2d = (n * n + n * nocc + nocc) * 8
         d2h = 2 * npair * 8
         e2e = {"value": world * flops / (te / args.steps) / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
@@ -462,8 +444,7 @@ def run_ours(args, w):
             **apps,
         }
         print(json.dumps(line), flush=True)
-    if pg:
-        pg.destroy_process_group()
+    replicas.finalize(rk)
     return 0
 
 
