@@ -566,7 +566,8 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
         wall = time.perf_counter() - t0
         res[tag] = {"molecules_per_s": nmol / wall, "wall_s": wall, "setup_s": r.setup_s, "scf_s": r.scf_s,
                     "iterations_mean": float(np.mean(r.iterations)), "converged": int(sum(r.converged)),
-                    "guess_s": extra}
+                    "guess_s": extra, "eigensolves": r.timings["eigensolves"],
+                    "setup_parts_s": r.timings["setup_parts"]}
         return r
 
     ref = timed("batched_fp64", precision="fp64")
@@ -587,6 +588,7 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
     sctx.close()
     plain = plain_subset / wall
     res["plain_fp64_per_molecule"] = {"molecules_per_s": plain, "molecules_timed": plain_subset,
+                                      "host_cores": len(os.sched_getaffinity(0)),
                                       "max_abs_energy_error_vs_batched_fp64": float(
                                           np.max(np.abs(np.array(e_plain) - e_ref[:plain_subset])))}
     for tag in ("batched_fp64", "batched_mixed", "batched_mixed_learned_guess"):

@@ -5,7 +5,10 @@ stream), and the SCF iterations of the whole set advance together:
 
   integrals    (P|Q), (mu nu|P), metric and fit on the device per molecule
                (rijk_build_rimatr_from_shells) when the shells fit the device
-               engine, else the host engine;
+               engine, else the host engine; the molecules' setups run on a pool
+               of host threads (``setup_workers``), each with its own stream, so
+               that one molecule's host-side plan and one-electron integrals
+               overlap the others' device work;
   J / K        per molecule through the device entry points (rijk_vj_upper_dev,
                rijk_vk_upper_occ_dev or the split-precision tcgen05 forms), the
                molecules' launches overlapping on their streams;
@@ -14,9 +17,12 @@ stream), and the SCF iterations of the whole set advance together:
                kept as a batched history, the B matrices of diis_solver
                (:3138-3188) formed in one batched product and solved per molecule;
   diagonalise  the generalised eigenproblem F C = S C e of diagonalize_hamiltonian
-               (:1843-1873) as one batched symmetric eigensolve of X^T F X
-               (X = S^-1/2 per molecule, padding rows pushed to the top of the
-               spectrum) on the device;
+               (:1843-1873) in the standard form X^T F X with X = L^-T from the
+               Cholesky factor S = L L^T (the reduction of REST's LAPACK dspgvx),
+               padding rows pushed to the top of the spectrum; each molecule's
+               eigenbasis from the previous iteration is refined by matrix
+               products (eigsolve.refine), and molecules where that does not
+               pass take a batched cuSOLVER eigensolve;
   density      D = 2 C_occ C_occ^T on the device.
 
 Precision of the exchange build:
@@ -35,6 +41,7 @@ criteria, :1875-1951) and stop being updated once converged.
 """
 from __future__ import annotations
 
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -43,6 +50,7 @@ import numpy as np
 from .basis import DEVICE_MAX_L_AO, DEVICE_MAX_L_AUX, int1e, int1e_nuclear_dev, int2c2e, int2c2e_dev, int3c2e
 from .geometry import alkane, water_cluster  # noqa: F401  (re-exported)
 from .rijk import RIJK
+from .eigsolve import refine
 from .scf import metric_inv_sqrt, metric_inv_sqrt_dev
 
 
@@ -61,7 +69,8 @@ class BatchedRHF:
     def __init__(self, mols: list, basis: str, auxbas: str, device: int = 0, metric: str = "inv_sqrt",
                  precision: str = "fp64", integrals: str = "auto", rebuild_every: int = 16,
                  switch_etot: float = 1e-7, switch_rho: float = 1e-5, eig_workers: int = 8,
-                 graphs: bool = False, split_min_basis: int = 512):
+                 graphs: bool = False, split_min_basis: int = 512, refine_eigs: bool = True,
+                 setup_workers: int = 8):
         import torch
 
         if precision not in ("fp64", "mixed", "split"):
@@ -77,42 +86,96 @@ class BatchedRHF:
         # factorisation of dD cost more than the split build saves
         self.split_min_basis = split_min_basis
         self.eig_workers, self._pool = eig_workers, None
+        # eigenbases of the previous iteration refined by matrix products
+        # (eigsolve.refine); a fresh eigensolve only where that does not pass
+        self.refine_eigs = refine_eigs
+        self._vbasis, self._have_basis = None, []
+        self._eig_counts = {"refined": 0, "eigh": 0}
         # CUDA graphs of the per-molecule FP64 J/K (orbital form), captured after
         # the first build with every context's buffers pinned
         self.graphs = graphs and precision == "fp64"
         self._graph = None
         t0 = time.perf_counter()
         self.mols = mols
-        self.ctx, self.n, self.nocc, self.enuc = [], [], [], []
-        hs, ss = [], []
         for mol in mols:
             if mol.spin != 1 or mol.nelec % 2:
                 raise ValueError("BatchedRHF handles closed-shell molecules")
-            bas, aux = mol.shells(basis), mol.shells(auxbas)
-            n = bas.nfun
-            s = int1e(mol, bas, "ovlp")
-            ctx = RIJK(device)
-            on_device = integrals == "device" or (
-                integrals == "auto" and int(bas.l.max()) <= DEVICE_MAX_L_AO and int(aux.l.max()) <= DEVICE_MAX_L_AUX)
-            if on_device:  # kinetic on the host, nuclear attraction on the device
-                h = torch.as_tensor(int1e(mol, bas, "kinetic"), device=self.dev) + int1e_nuclear_dev(mol, bas)
-            else:
-                h = int1e(mol, bas, "kinetic") + int1e(mol, bas, "nuclear")
-            if on_device:
-                factor = metric_inv_sqrt_dev(int2c2e_dev(aux)) if metric == "inv_sqrt" else None
-                ctx.build_rimatr_from_shells(bas, aux, factor)
-            else:
-                v2, i3 = int2c2e(aux), int3c2e(bas, aux)
-                if metric == "inv_sqrt":
-                    ctx.fit_rimatr(metric_inv_sqrt(v2), i3, n)
-                else:
-                    ctx.build_rimatr_cholesky(v2, i3, n)
-            self.ctx.append(ctx)
-            self.n.append(n)
-            self.nocc.append(mol.nelec // 2)
-            self.enuc.append(mol.nuclear_repulsion())
-            hs.append(h)
-            ss.append(s)
+        # torch loads its device linear-algebra backend on first use, and that
+        # first use must not happen on several threads at once (setup and
+        # eigensolve threads): load it here
+        with torch.cuda.device(self.dev):
+            torch.linalg.eigh(torch.eye(2, dtype=torch.float64, device=self.dev))
+        tls = threading.local()
+
+        def one(mol):
+            """One molecule's contexts and integrals (host one-electron parts,
+            device nuclear attraction, device three-centre integrals, metric and
+            fit), on this thread's own stream; returns when its device work is done."""
+            part = {"host_one_electron": 0.0, "contexts": 0.0, "device": 0.0}
+            if not hasattr(tls, "stream"):
+                tls.stream = torch.cuda.Stream(device=self.dev)
+            with torch.cuda.device(self.dev), torch.cuda.stream(tls.stream):
+                bas, aux = mol.shells(basis), mol.shells(auxbas)
+                n = bas.nfun
+                ta = time.perf_counter()
+                s = int1e(mol, bas, "ovlp")
+                on_device = integrals == "device" or (
+                    integrals == "auto" and int(bas.l.max()) <= DEVICE_MAX_L_AO and int(aux.l.max()) <= DEVICE_MAX_L_AUX)
+                tk = int1e(mol, bas, "kinetic") if on_device else None
+                tb = time.perf_counter()
+                ctx = RIJK(device)
+                tc = time.perf_counter()
+                part["host_one_electron"] += tb - ta
+                part["contexts"] += tc - tb
+                try:
+                    if on_device:  # kinetic on the host, nuclear attraction and the tensor on the device
+                        h = torch.as_tensor(tk, device=self.dev) + int1e_nuclear_dev(mol, bas)
+                        factor = metric_inv_sqrt_dev(int2c2e_dev(aux)) if metric == "inv_sqrt" else None
+                        ctx.build_rimatr_from_shells(bas, aux, factor)
+                    else:
+                        h = int1e(mol, bas, "kinetic") + int1e(mol, bas, "nuclear")
+                        v2, i3 = int2c2e(aux), int3c2e(bas, aux)
+                        if metric == "inv_sqrt":
+                            ctx.fit_rimatr(metric_inv_sqrt(v2), i3, n)
+                        else:
+                            ctx.build_rimatr_cholesky(v2, i3, n)
+                    tls.stream.synchronize()
+                except BaseException:
+                    ctx.close()
+                    raise
+                part["device"] += time.perf_counter() - tc
+            return ctx, n, h, s, part
+
+        nw = max(1, min(setup_workers, len(mols)))
+        if nw == 1:
+            outs = [one(m) for m in mols]
+        else:
+            from concurrent.futures import ThreadPoolExecutor
+
+            with ThreadPoolExecutor(nw) as pool:
+                futs = [pool.submit(one, m) for m in mols]
+                outs, err = [], None
+                for f in futs:
+                    try:
+                        outs.append(f.result())
+                    except BaseException as e:  # noqa: BLE001  (closed below, then re-raised)
+                        err = err or e
+            if err is not None:
+                for o in outs:
+                    o[0].close()
+                raise err
+        # host time per phase, summed over the setup threads
+        parts = {"host_one_electron": 0.0, "contexts": 0.0, "device": 0.0}
+        for o in outs:
+            for k, v in o[4].items():
+                parts[k] += v
+        parts["molecules_wall"] = time.perf_counter() - t0
+        self.ctx = [o[0] for o in outs]
+        self.n = [o[1] for o in outs]
+        self.nocc = [m.nelec // 2 for m in mols]
+        self.enuc = [m.nuclear_repulsion() for m in mols]
+        hs = [o[2] for o in outs]
+        ss = [o[3] for o in outs]
         self.B = len(mols)
         self.nmax = max(self.n)
         self.omax = max(self.nocc)
@@ -124,17 +187,32 @@ class BatchedRHF:
             n = self.n[i]
             self.S[i, :n, :n] = torch.as_tensor(s, device=self.dev)
             self.H[i, :n, :n] = torch.as_tensor(h, device=self.dev)
-        # X = S^-1/2 per molecule (identity on the padding), one batched eigensolve
         pad_eye = torch.zeros(B, nm, nm, dtype=f64, device=self.dev)
         for i in range(B):
             idx = torch.arange(self.n[i], nm, device=self.dev)
             pad_eye[i, idx, idx] = 1.0
-        w, u = torch.linalg.eigh(self.S + pad_eye)
-        self.X = (u * w.rsqrt()[:, None, :]) @ u.transpose(1, 2) - pad_eye
+        # X = L^-T from S = L L^T (identity on the padding): the reduction to a
+        # standard eigenproblem that REST's packed generalised solver performs
+        # (LAPACK dspgvx, src/scf_io/mod.rs:1851), batched; an S that is not
+        # numerically positive definite takes X = S^-1/2 instead
+        td = time.perf_counter()
+        L, info = torch.linalg.cholesky_ex(self.S + pad_eye)
+        if bool((info != 0).any()):
+            w, u = torch.linalg.eigh(self.S + pad_eye)
+            self.X = (u * w.rsqrt()[:, None, :]) @ u.transpose(1, 2) - pad_eye
+        else:
+            eye = torch.eye(nm, dtype=f64, device=self.dev).expand(B, nm, nm)
+            self.X = torch.linalg.solve_triangular(L, eye, upper=False).transpose(1, 2) - pad_eye
         # padded rows of X^T F X get a large diagonal so their eigenvalues come last
         self.pad_shift = 1.0e6 * pad_eye
+        self._pad_eye = pad_eye
+        self._have_basis = [False] * B
         self._tri = {}
+        parts["orthogonaliser_submit"] = time.perf_counter() - td
+        td = time.perf_counter()
         torch.cuda.synchronize()
+        parts["device_wait"] = time.perf_counter() - td
+        self.setup_parts = parts
         self.setup_s = time.perf_counter() - t0
 
     def _eigh(self, fp):
@@ -172,6 +250,52 @@ class BatchedRHF:
         for _, _, done in res:
             main.wait_event(done)
         return torch.cat([e for e, _, _ in res]), torch.cat([v for _, v, _ in res])
+
+    def _solve(self, A, rows):
+        """Eigenpairs of the orthogonalised Fock matrices A (one per molecule of
+        ``rows``): molecules with an eigenbasis from the previous iteration
+        refine it (4 steps, 5 more while still converging); the rest, and those
+        whose refinement does not pass, take a fresh eigensolve.  The bases are
+        kept, with the padded block set to the identity, for the next call."""
+        torch = self.torch
+        nr, nm = A.shape[0], A.shape[1]
+        e_r = torch.empty(nr, nm, dtype=A.dtype, device=self.dev)
+        cp = torch.empty(nr, nm, nm, dtype=A.dtype, device=self.dev)
+        done = [False] * nr
+        loc = [k for k, i in enumerate(rows) if self._have_basis[i]] if self.refine_eigs else []
+        if loc:
+            li = torch.as_tensor(loc, device=self.dev)
+            nv = [self.n[rows[k]] for k in loc]
+            gi = torch.as_tensor([rows[k] for k in loc], device=self.dev)
+            lam, V, ok, off = refine(A[li], self._vbasis[gi], nv, steps=4)
+            ok_h, off_h = ok.cpu().numpy(), off.cpu().numpy()
+            more = [j for j in range(len(loc)) if not ok_h[j] and off_h[j] < 1e-2]
+            if more:
+                mj = torch.as_tensor(more, device=self.dev)
+                lam2, V2, ok2, _ = refine(A[li[mj]], V[mj], [nv[j] for j in more], steps=5)
+                lam[mj], V[mj] = lam2, V2
+                for j, o in zip(more, ok2.cpu().numpy()):
+                    ok_h[j] = o
+            e_r[li], cp[li] = lam, V
+            for j, k in enumerate(loc):
+                done[k] = bool(ok_h[j])
+        todo = [k for k in range(nr) if not done[k]]
+        if todo:
+            ti = torch.as_tensor(todo, device=self.dev)
+            e_t, v_t = self._eigh(A[ti])
+            e_r[ti], cp[ti] = e_t, v_t
+        self._eig_counts["refined"] += nr - len(todo)
+        self._eig_counts["eigh"] += len(todo)
+        if self.refine_eigs:
+            r = torch.as_tensor(rows, device=self.dev)
+            if self._vbasis is None:
+                self._vbasis = torch.zeros(self.B, nm, nm, dtype=A.dtype, device=self.dev)
+            pe = self._pad_eye[r]
+            keep = (pe.diagonal(dim1=1, dim2=2) == 0).to(A.dtype)
+            self._vbasis[r] = cp * keep[:, :, None] * keep[:, None, :] + pe
+            for i in rows:
+                self._have_basis[i] = True
+        return e_r, cp
 
     def _tri_idx(self, n):
         if n not in self._tri:
@@ -397,7 +521,7 @@ class BatchedRHF:
             rows = list(range(B)) if rows is None else rows
             r = torch.as_tensor(rows, device=self.dev)
             Xr = self.X[r]
-            e_r, cp = self._eigh(Xr.transpose(1, 2) @ F[r] @ Xr + self.pad_shift[r])
+            e_r, cp = self._solve(Xr.transpose(1, 2) @ F[r] @ Xr + self.pad_shift[r], rows)
             e = torch.zeros(B, nm, dtype=f64, device=self.dev)
             C = torch.zeros(B, nm, nm, dtype=f64, device=self.dev)
             e[r] = e_r
@@ -409,9 +533,14 @@ class BatchedRHF:
             return 2.0 * co @ co.transpose(1, 2)
 
         active = [True] * B
-        e, C = diag(self.H)  # hcore guess
-        D = density(C)
         given = [d is not None for d in (initial_densities or [None] * B)]
+        hc = [i for i in range(B) if not given[i]]  # hcore guess where no density is given
+        if hc:
+            e, C = diag(self.H, hc)
+        else:
+            e = torch.zeros(B, nm, dtype=f64, device=self.dev)
+            C = torch.zeros(B, nm, nm, dtype=f64, device=self.dev)
+        D = density(C)
         for i in range(B):
             if given[i]:
                 n = self.n[i]
@@ -507,7 +636,8 @@ class BatchedRHF:
         torch.cuda.synchronize()
         scf_s = time.perf_counter() - t0
         timings = {"fp64_k_builds": list(self._nfp64), "split_k_builds": list(self._nsplit),
-                   "density_checks": checks}
+                   "density_checks": checks, "eigensolves": dict(self._eig_counts),
+                   "setup_parts": dict(self.setup_parts)}
         dens = [D[i, :self.n[i], :self.n[i]].cpu().numpy() for i in range(B)] if return_densities else []
         return BatchResult([float(x) for x in E_prev.cpu()], conv, iters, self.setup_s, scf_s, timings, dens)
 
@@ -567,6 +697,8 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
     nfp64, nsplit = [0] * len(mols), [0] * len(mols)
     dens = [None] * len(mols) if run_kw.get("return_densities") else []
     setup = scf = 0.0
+    eig = {"refined": 0, "eigh": 0}
+    parts = {}
     for idx in groups:
         b = BatchedRHF([mols[i] for i in idx], basis, auxbas, device=device, **kw)
         try:
@@ -576,9 +708,15 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
             torch.cuda.empty_cache()
         setup += r.setup_s
         scf += r.scf_s
+        for k in eig:
+            eig[k] += r.timings["eigensolves"][k]
+        for k, v in r.timings["setup_parts"].items():
+            parts[k] = parts.get(k, 0.0) + v
         for j, i in enumerate(idx):
             energies[i], conv[i], iters[i] = r.energies[j], r.converged[j], r.iterations[j]
             nfp64[i], nsplit[i] = r.timings["fp64_k_builds"][j], r.timings["split_k_builds"][j]
             if dens:
                 dens[i] = r.densities[j]
-    return BatchResult(energies, conv, iters, setup, scf, {"fp64_k_builds": nfp64, "split_k_builds": nsplit}, dens)
+    return BatchResult(energies, conv, iters, setup, scf,
+                       {"fp64_k_builds": nfp64, "split_k_builds": nsplit, "eigensolves": eig, "setup_parts": parts},
+                       dens)

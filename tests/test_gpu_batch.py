@@ -126,3 +126,40 @@ def test_mixed_precision_keeps_small_molecules_in_fp64():
     finally:
         b.close()
     assert r.converged[0] and r.timings["split_k_builds"][0] == 0
+
+
+def test_refined_eigenbases_match_fresh_eigensolves():
+    """Refining the previous iteration's eigenbases (eigsolve.refine) instead of
+    a fresh cuSOLVER eigensolve: same iterations, energies within 1e-10 Eh, and
+    most eigensolves after the first iterations are refinements."""
+    mols = [water_cluster(k, seed=40 + k) for k in (4, 1, 6, 3, 5, 2)]
+    out = {}
+    for refine_eigs in (False, True):
+        b = BatchedRHF(mols, "def2-SVP", "def2-SVP-JKFIT", precision="fp64", refine_eigs=refine_eigs)
+        try:
+            out[refine_eigs] = b.run(max_cycle=100, **TIGHT_BATCH)
+        finally:
+            b.close()
+    fresh, refined = out[False], out[True]
+    assert all(fresh.converged) and all(refined.converged) and all(refined.timings["density_checks"])
+    assert fresh.timings["eigensolves"]["refined"] == 0
+    counts = refined.timings["eigensolves"]
+    assert counts["refined"] > counts["eigh"]
+    for a, b_, ia, ib in zip(fresh.energies, refined.energies, fresh.iterations, refined.iterations):
+        assert abs(a - b_) < 1e-10
+        assert abs(ia - ib) <= 1
+
+
+def test_threaded_setup_matches_serial_setup():
+    """Molecule setups on a thread pool (each on its own stream) build the same
+    tensors as one after another: identical energies."""
+    mols = [water_cluster(k, seed=60 + k) for k in (3, 1, 4, 2)]
+    out = {}
+    for workers in (1, 4):
+        b = BatchedRHF(mols, "def2-SVP", "def2-SVP-JKFIT", precision="fp64", setup_workers=workers)
+        try:
+            out[workers] = b.run(max_cycle=100, **TIGHT_BATCH)
+        finally:
+            b.close()
+    assert all(out[1].converged) and all(out[4].converged)
+    assert out[1].energies == out[4].energies
