@@ -208,6 +208,8 @@ class BatchedRHF:
         self._pad_eye = pad_eye
         self._have_basis = [False] * B
         self._tri = {}
+        for n in sorted(set(self.n)):
+            self._tri_idx(n)
         parts["orthogonaliser_submit"] = time.perf_counter() - td
         td = time.perf_counter()
         torch.cuda.synchronize()
@@ -298,8 +300,15 @@ class BatchedRHF:
         return e_r, cp
 
     def _tri_idx(self, n):
+        """Row and column of each packed upper-triangle element for size n.  The
+        per-molecule streams of the J/K dispatch read these cached tensors without
+        waiting on the stream that made them, so they are made on the calling
+        stream and synchronised before first use (the constructor makes every
+        size of the batch)."""
         if n not in self._tri:
-            il = self.torch.tril_indices(n, n, device=self.dev)  # REST order: (i <= j), j-major
+            torch = self.torch
+            il = torch.tril_indices(n, n, device=self.dev)  # REST order: (i <= j), j-major
+            torch.cuda.current_stream(self.dev).synchronize()
             self._tri[n] = (il[1], il[0])
         return self._tri[n]
 
@@ -560,7 +569,10 @@ class BatchedRHF:
         count = [0] * B
         iters = [0] * B
         conv = [False] * B
+        # host time between the loop's own synchronisation points
+        tp = {"diis": 0.0, "eigensolve": 0.0, "fock_build": 0.0}
         for it in range(1, max_cycle + 1):
+            ta = time.perf_counter()
             err = F @ D @ self.S
             err = err - err.transpose(1, 2)
             act = torch.tensor(active, device=self.dev)
@@ -591,9 +603,11 @@ class BatchedRHF:
                     f_hist[i, 1:] = 0.0
                     count[i] = 1
                     coef[i, 0] = 1.0
+            tb = time.perf_counter()
             Fx = torch.einsum("bm,bmij->bij", torch.as_tensor(coef, device=self.dev), f_hist)
             Fx = torch.where(act[:, None, None], Fx, F)
             e, C = diag(Fx, [i for i in range(B) if active[i]])
+            tc = time.perf_counter()
             Dn = density(C)
             Fn = self.H + self._jk(C, active)
             En = enuc + 0.5 * ((Dn * (self.H + Fn)).sum(dim=(1, 2)))
@@ -601,6 +615,10 @@ class BatchedRHF:
             ddm = ((Dn - D).pow(2).sum(dim=(1, 2))).sqrt() / ns
             deev = (((e - e_prev) * nmask).pow(2).sum(dim=1)).sqrt()
             de_h, ddm_h, deev_h = de.cpu().numpy(), ddm.cpu().numpy(), deev.cpu().numpy()
+            td = time.perf_counter()
+            tp["diis"] += tb - ta
+            tp["eigensolve"] += tc - tb
+            tp["fock_build"] += td - tc
             newly = []
             for i in range(B):
                 if not active[i]:
@@ -637,7 +655,7 @@ class BatchedRHF:
         scf_s = time.perf_counter() - t0
         timings = {"fp64_k_builds": list(self._nfp64), "split_k_builds": list(self._nsplit),
                    "density_checks": checks, "eigensolves": dict(self._eig_counts),
-                   "setup_parts": dict(self.setup_parts)}
+                   "setup_parts": dict(self.setup_parts), "scf_parts": tp}
         dens = [D[i, :self.n[i], :self.n[i]].cpu().numpy() for i in range(B)] if return_densities else []
         return BatchResult([float(x) for x in E_prev.cpu()], conv, iters, self.setup_s, scf_s, timings, dens)
 
@@ -699,24 +717,28 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
     setup = scf = 0.0
     eig = {"refined": 0, "eigh": 0}
     parts = {}
+    teardown = 0.0
     for idx in groups:
         b = BatchedRHF([mols[i] for i in idx], basis, auxbas, device=device, **kw)
         try:
             r = b.run(initial_densities=None if guesses is None else [guesses[i] for i in idx], **run_kw)
         finally:
+            tt = time.perf_counter()
             b.close()
             torch.cuda.empty_cache()
+            teardown += time.perf_counter() - tt
         setup += r.setup_s
         scf += r.scf_s
         for k in eig:
             eig[k] += r.timings["eigensolves"][k]
-        for k, v in r.timings["setup_parts"].items():
+        for k, v in list(r.timings["setup_parts"].items()) + list(r.timings["scf_parts"].items()):
             parts[k] = parts.get(k, 0.0) + v
         for j, i in enumerate(idx):
             energies[i], conv[i], iters[i] = r.energies[j], r.converged[j], r.iterations[j]
             nfp64[i], nsplit[i] = r.timings["fp64_k_builds"][j], r.timings["split_k_builds"][j]
             if dens:
                 dens[i] = r.densities[j]
+    parts["teardown"] = teardown
     return BatchResult(energies, conv, iters, setup, scf,
                        {"fp64_k_builds": nfp64, "split_k_builds": nsplit, "eigensolves": eig, "setup_parts": parts},
                        dens)

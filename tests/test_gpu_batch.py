@@ -163,3 +163,28 @@ def test_threaded_setup_matches_serial_setup():
             b.close()
     assert all(out[1].converged) and all(out[4].converged)
     assert out[1].energies == out[4].energies
+
+
+def test_same_size_molecules_from_given_densities_are_reproducible():
+    """Molecules of one size share the cached packed-triangle indices that every
+    molecule's stream reads in the J/K dispatch (the first build here is the
+    dm-only one from the given densities).  Two runs, setups threaded and
+    eigensolves on eight streams, must agree bit for bit."""
+    import numpy as np
+
+    from rest_b200.basis import int1e
+    from rest_b200.guess import LearnedGuess
+
+    mols = [water_cluster(4, seed=70 + s) for s in range(10)] + [water_cluster(2, seed=90 + s) for s in range(6)]
+    guess = LearnedGuess.load(device=0)
+    dens = [guess.density(m, ovlp=int1e(m, m.shells("def2-SVP"), "ovlp")) for m in mols]
+    runs = []
+    for _ in range(2):
+        b = BatchedRHF(mols, "def2-SVP", "def2-SVP-JKFIT", precision="fp64", setup_workers=8, eig_workers=8)
+        try:
+            runs.append(b.run(max_cycle=100, initial_densities=dens, **TIGHT_BATCH))
+        finally:
+            b.close()
+    assert all(runs[0].converged) and all(runs[1].converged)
+    assert runs[0].iterations == runs[1].iterations
+    assert np.array_equal(np.array(runs[0].energies), np.array(runs[1].energies))
