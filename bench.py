@@ -415,7 +415,7 @@ def run_ours(args, w):
     if rank == 0 and world == 1 and not args.no_apps:
         apps["ri_tensor_build"] = measure_tensor_build(local)
         apps["precision_alkanes"] = measure_alkanes(local)
-        apps["molecule_set"] = measure_molecule_set(local, args.set_size)
+        apps["molecule_set"] = molecule_set_in_child(local, args.set_size)
 
     if rank == 0:
         line = {
@@ -577,18 +577,34 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
     res["batched_mixed"]["max_abs_energy_error_vs_fp64"] = float(np.max(np.abs(np.array(mix.energies) - e_ref)))
     res["batched_mixed_learned_guess"]["max_abs_energy_error_vs_fp64"] = float(
         np.max(np.abs(np.array(lrn.energies) - e_ref)))
+    from threadpoolctl import threadpool_limits
+
     sctx = RIJK(device)
-    t0 = time.perf_counter()
+    popts = ScfOptions(scf_acc_etot=1e-8, scf_acc_rho=1e-6, scf_acc_eev=1e-6)
+    # The plain path's host work (REST's LAPACK generalised eigensolve and DIIS
+    # products) is timed at the host BLAS thread count that runs it fastest on
+    # this box, chosen on a three-molecule calibration: numpy and scipy each
+    # bring an OpenBLAS pool, and at their defaults the pools compete.
+    cores = len(os.sched_getaffinity(0))
+    cal = {}
+    for th in sorted({1, 2, 4, 8, cores}):
+        with threadpool_limits(limits=th, user_api="blas"):
+            t0 = time.perf_counter()
+            for m in mols[:3]:
+                SCF(m, "def2-SVP", "def2-SVP-JKFIT", popts, ctx=sctx).run()
+            cal[th] = time.perf_counter() - t0
+    blas = min(cal, key=cal.get)
     e_plain = []
-    for m in mols[:plain_subset]:
-        r = SCF(m, "def2-SVP", "def2-SVP-JKFIT", ScfOptions(scf_acc_etot=1e-8, scf_acc_rho=1e-6, scf_acc_eev=1e-6),
-                ctx=sctx).run()
-        e_plain.append(r.energy)
-    wall = time.perf_counter() - t0
+    with threadpool_limits(limits=blas, user_api="blas"):
+        t0 = time.perf_counter()
+        for m in mols[:plain_subset]:
+            e_plain.append(SCF(m, "def2-SVP", "def2-SVP-JKFIT", popts, ctx=sctx).run().energy)
+        wall = time.perf_counter() - t0
     sctx.close()
     plain = plain_subset / wall
     res["plain_fp64_per_molecule"] = {"molecules_per_s": plain, "molecules_timed": plain_subset,
-                                      "host_cores": len(os.sched_getaffinity(0)),
+                                      "host_cores": cores, "host_blas_threads": blas,
+                                      "blas_calibration_s": {str(k): round(v, 3) for k, v in cal.items()},
                                       "max_abs_energy_error_vs_batched_fp64": float(
                                           np.max(np.abs(np.array(e_plain) - e_ref[:plain_subset])))}
     for tag in ("batched_fp64", "batched_mixed", "batched_mixed_learned_guess"):
@@ -626,6 +642,26 @@ def traffic_per_launch(kernel: str, w: dict, launches: int):
     return TRAFFIC_RATIO_K_HALF * half_transform_bytes(w["n"], w["nocc"], w["naux"] / max(1, launches))
 
 
+def molecule_set_in_child(device: int, nmol: int) -> dict:
+    """The molecule-set config (both its batched runs and the plain per-molecule
+    comparator) measured in a fresh process, as a job of its own: the stages
+    before it in this process leave tens of GB of device allocations and their
+    frees behind, which slowed the set's per-context allocations and teardown
+    about twofold when it ran here."""
+    import subprocess
+
+    import torch
+
+    torch.cuda.empty_cache()  # this process's cached blocks go back to the device for the child
+    out = subprocess.run([sys.executable, os.path.abspath(__file__), "--molecule-set-only", str(nmol),
+                          "--device", str(device)], capture_output=True, text=True, timeout=1800)
+    if out.returncode != 0:
+        raise RuntimeError("molecule-set measurement failed:\n" + out.stderr[-4000:])
+    res = json.loads(out.stdout.strip().splitlines()[-1])
+    res["process"] = "measured in a fresh child process"
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -640,7 +676,16 @@ def main():
     ap.add_argument("--no-apps", action="store_true",
                     help="skip the application configs (device tensor build, alkanes, molecule set)")
     ap.add_argument("--set-size", type=int, default=64, help="molecules in the batched water-cluster set")
+    ap.add_argument("--molecule-set-only", type=int, default=0, metavar="NMOL",
+                    help="measure only the molecule-set config with NMOL molecules and print its JSON")
+    ap.add_argument("--device", type=int, default=0, help="device of --molecule-set-only")
     args = ap.parse_args()
+    if args.molecule_set_only:
+        import torch
+
+        torch.cuda.set_device(args.device)
+        print(json.dumps(measure_molecule_set(args.device, args.molecule_set_only)))
+        return 0
     w = workload(args.n)
     if args.impl == "reference":
         return run_reference(args, w)
