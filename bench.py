@@ -616,24 +616,25 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
 
 # DRAM traffic of the half-transform per launch.  ncu at n=600 (N=2400, one
 # launch over all aux rows; profiles/k_half_transform_rank_update_n600.md)
-# measured dram read 3.7385 GB + write 1.5520 GB = 5.2905 GB, which is 0.9966
+# measured dram read 3.7407 GB + write 1.2123 GB = 4.9529 GB, which is 0.9977
 # of the bytes the launch must move: the tile-packed tensor rows it reads plus
-# the X rows it writes.  The n=1200 tensor (29 GB) is too large to capture under
-# a multi-pass ncu run, so its traffic is that ratio times the same byte count
-# for the rows of one n=1200 launch.
+# the X rows it writes (ldx x nocc per aux row).  The n=1200 tensor (29 GB) is
+# too large to capture under a multi-pass ncu run, so its traffic is that ratio
+# times the same byte count for the rows of one n=1200 launch.
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_half_transform at n=600 "
-                  "(0.9966 of tensor rows read + X rows written), scaled to this launch's rows and sizes")
+                  "(0.9977 of tensor rows read + X rows written), scaled to this launch's rows and sizes")
 
 
 def half_transform_bytes(n: int, nocc: int, rows: float) -> float:
+    """Bytes one half-transform launch must move: the tile-packed tensor rows it
+    reads and the X rows it writes (ldx x nocc per aux row, no column padding)."""
     nt = -(-n // 32)
     ldb = nt * (nt + 1) // 2 * 1024
     ldx = -(-n // 128) * 128
-    ocols = -(-nocc // 128) * 128
-    return rows * 8.0 * (ldb + ldx * ocols)
+    return rows * 8.0 * (ldb + ldx * nocc)
 
 
-TRAFFIC_RATIO_K_HALF = 5.2905e9 / half_transform_bytes(600, 100, 2400)
+TRAFFIC_RATIO_K_HALF = 4.9529e9 / half_transform_bytes(600, 100, 2400)
 
 
 def traffic_per_launch(kernel: str, w: dict, launches: int):

@@ -359,26 +359,31 @@ int vk_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int
     ProfScope ps(ctx, RIJK_PROF_K_OTHER, st);
     rijk::launch_k_prepare_c(g, d_eigv, g.n, g.n * num_state, d_occ, num_state, nw, spin, ldx, ocols, Cw, st);
   }
-  const int64_t per_p = ldx * ocols * 8;
+  // X holds, per spin, the chunk's X_p back to back without padding (column
+  // p nw + i), spin beta after spin alpha, and 32 spare columns for the rank
+  // update's last k tile
+  const int64_t xcols = nw[0] + (spin == 2 ? nw[1] : 0);
+  const int64_t per_p = ldx * xcols * 8;
   const int64_t pchunk = std::max<int64_t>(1, std::min<int64_t>(g.naux, (int64_t)ctx->scratch_budget / per_p));
-  RIJK_TRY(ensure(ctx, ctx->X, (size_t)pchunk * per_p));
+  RIJK_TRY(ensure(ctx, ctx->X, (size_t)(pchunk * xcols + rijk::TS) * ldx * 8));
   const int splits_max = rijk::k_rank_splits(g, pchunk, 0);
   RIJK_TRY(ensure(ctx, ctx->Kpart, (size_t)splits_max * rijk::k_block_pairs(g, 0) * 128 * 128 * 8));
   double* X = static_cast<double*>(ctx->X.p);
   double* Kp = static_cast<double*>(ctx->Kpart.p);
   for (int64_t p0 = 0; p0 < g.naux; p0 += pchunk) {
     const int64_t np = std::min(pchunk, g.naux - p0);
+    const rijk::XMap xm{nw[0], (int)nw[0], (int)coff[1], spin == 2 ? (int)nw[1] : 0, np * nw[0], nw[1]};
     {
       ProfScope ps(ctx, RIJK_PROF_K_HALF, st);
-      rijk::launch_half_transform(g, ctx->dB, p0, np, Cw, ldx, ocols, ocols_valid, X, ldx, ldx * ocols, ctx->d_err,
-                                  st);
+      rijk::launch_half_transform(g, ctx->dB, p0, np, Cw, ldx, ocols, ocols_valid, X, ldx, xm, ctx->d_err, st);
     }
     for (int s = 0; s < spin; ++s) {
       if (nw[s] == 0) continue;
       const int splits = rijk::k_rank_splits(g, np, 0);
       {
         ProfScope ps(ctx, RIJK_PROF_K_RANK, st);
-        rijk::launch_k_rank_update(g, X, ldx, ldx * ocols, np, coff[s], nw[s], splits, 0, Kp, ctx->d_err, st);
+        rijk::launch_k_rank_update(g, X + (s == 0 ? 0 : np * nw[0]) * ldx, ldx, np, nw[s], splits, 0, Kp,
+                                   ctx->d_err, st);
       }
       ProfScope ps(ctx, RIJK_PROF_K_OTHER, st);
       rijk::launch_k_finalize(g, Kp, splits, 0, scale, p0 > 0 ? 1 : 0, 0, d_out + s * g.npair, st);
@@ -410,7 +415,8 @@ int vk_dm_dev(rijk_ctx* ctx, const double* d_dm, int spin, double scale, int ful
       const int64_t np = std::min(pchunk, g.naux - p0);
       {
         ProfScope ps(ctx, RIJK_PROF_K_HALF, st);
-        rijk::launch_half_transform(g, ctx->dB, p0, np, Dp, ldx, ldx, g.n, T, ldx, ldx * ldx, ctx->d_err, st);
+        rijk::launch_half_transform(g, ctx->dB, p0, np, Dp, ldx, ldx, g.n, T, ldx, rijk::XMap::dense(ldx),
+                                    ctx->d_err, st);
       }
       const int splits = rijk::k_rank_splits(g, np, full);
       {
@@ -576,7 +582,7 @@ int rijk_ctx_autotune(rijk_ctx* ctx, int64_t ncols, int64_t sample_rows, int* be
   const int64_t ldx = round_up(g.n, 128);
   const int64_t ocols = round_up(ncols, 128);
   RIJK_TRY(ensure(ctx, ctx->Cw, (size_t)ldx * ocols * 8));
-  RIJK_TRY(ensure(ctx, ctx->X, (size_t)np * ldx * ocols * 8));
+  RIJK_TRY(ensure(ctx, ctx->X, (size_t)(np * ncols + rijk::TS) * ldx * 8));
   // any non-zero operand times the same as the real one: fill C with a constant
   std::vector<double> ones((size_t)ldx * ocols, 0.0);
   for (int64_t c = 0; c < ncols; ++c)
@@ -596,12 +602,13 @@ int rijk_ctx_autotune(rijk_ctx* ctx, int64_t ncols, int64_t sample_rows, int* be
     for (int rep = 0; rep < 2; ++rep) {  // first repetition warms up
       RIJK_CK(cudaEventRecord(a, st));
       rijk::launch_half_transform(g, ctx->dB, 0, np, static_cast<double*>(ctx->Cw.p), ldx, ocols, ncols,
-                                  static_cast<double*>(ctx->X.p), ldx, ldx * ocols, ctx->d_err, st);
+                                  static_cast<double*>(ctx->X.p), ldx, rijk::XMap{ncols, (int)ncols, 0, 0, 0, 0},
+                                  ctx->d_err, st);
       RIJK_CK(cudaEventRecord(b, st));
       RIJK_CK(cudaEventSynchronize(b));
       RIJK_CK(cudaEventElapsedTime(&t_ht, a, b));
       RIJK_CK(cudaEventRecord(a, st));
-      rijk::launch_k_rank_update(g, static_cast<double*>(ctx->X.p), ldx, ldx * ocols, np, 0, ncols, splits, 0,
+      rijk::launch_k_rank_update(g, static_cast<double*>(ctx->X.p), ldx, np, ncols, splits, 0,
                                  static_cast<double*>(ctx->Kpart.p), ctx->d_err, st);
       RIJK_CK(cudaEventRecord(b, st));
       RIJK_CK(cudaEventSynchronize(b));
@@ -1132,7 +1139,8 @@ int rijk_ao2mo(rijk_ctx* ctx, const double* eigv, int64_t num_state, int64_t row
     for (int64_t p0 = 0; p0 < g.naux; p0 += pchunk) {
       const int64_t np = std::min(pchunk, g.naux - p0);
       // X_p = B_p C[:, cols]  (FP64 DMMA half-transform)
-      rijk::launch_half_transform(g, ctx->dB, p0, np, Cc, ldx, ocols, ncol, X, ldx, ldx * ocols, ctx->d_err, st);
+      rijk::launch_half_transform(g, ctx->dB, p0, np, Cc, ldx, ocols, ncol, X, ldx, rijk::XMap::dense(ocols),
+                                  ctx->d_err, st);
       // Y_p = C[:, rows]^T X_p  (batched over p)
       for (int64_t b0 = 0; b0 < np; b0 += 65535) {
         const int64_t nb = std::min<int64_t>(65535, np - b0);

@@ -10,8 +10,10 @@
 //   32 columns of 32 contiguous doubles).  For an A-slot, A[m][k] = S[m][k]
 //   when trans == 0 and S[k][m] when trans == 1; for a B-slot, B[k][n] = S[k][n]
 //   when trans == 0 and S[n][k] when trans == 1.  ptr == nullptr stages zeros.
-//   kvalid(kt) is the number of k columns of step kt that can be non-zero
-//   (the rest is padding and its k4 steps are skipped).
+//   kvalid(kt) is the number of k columns of step kt that count; the slot's
+//   columns beyond it are ignored (skipped k4 steps, and zeros in place of the
+//   slot's contents in a partial k4 step), so they may hold anything finite
+//   or not.
 //
 // Warp roles: warps 0 .. WM*WN-1 compute, the last warp produces.  The producer
 // waits until a stage is released (empty mbarrier, one arrival per consumer
@@ -151,8 +153,9 @@ __device__ __forceinline__ bool dmma_consume(int ktiles, DmmaSmem<Cfg>& sm, doub
         bkst[j] = tr ? SLD : 1;
         bbase[j] = (Cfg::MT + slot) * SLOT_DOUBLES + c * bnst[j] + (lane & 3) * bkst[j];
       }
-      const int kk_lim = (kvalid(kt) + 3) / 4;
-      if (kk_lim == TS / 4 && fm_lim == Cfg::FM && fn_lim == Cfg::FN) {
+      const int kvl = kvalid(kt);
+      const int kk_lim = (kvl + 3) / 4;
+      if (kvl == TS && fm_lim == Cfg::FM && fn_lim == Cfg::FN) {
         // Common case: straight-line code, so the compiler can load the
         // fragments of step kk+1 while the DMMAs of step kk issue.
 #pragma unroll
@@ -174,19 +177,22 @@ __device__ __forceinline__ bool dmma_consume(int ktiles, DmmaSmem<Cfg>& sm, doub
             for (int fn = 0; fn < Cfg::FN; ++fn) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], af[fm], bf[fn]);
         }
       } else {
-        // Edge tiles: skip the k4 steps and fragments that only hold padding.
+        // Edge tiles: skip the k4 steps and fragments that only hold padding;
+        // k columns at or beyond kvalid of the last k4 step read as zero (a
+        // slot may hold other data there, not only zero padding).
 #pragma unroll 1
         for (int kk = 0; kk < kk_lim; ++kk) {
           double af[Cfg::FM], bf[Cfg::FN];
+          const bool kin = kk * 4 + (lane & 3) < kvl;
 #pragma unroll
           for (int fm = 0; fm < Cfg::FM; ++fm) {
             const int j = fm / FPA, i = fm % FPA;
-            af[fm] = fm < fm_lim ? sbase[abase[j] + (i * 8) * amst[j] + (kk * 4) * akst[j]] : 0.0;
+            af[fm] = (fm < fm_lim && kin) ? sbase[abase[j] + (i * 8) * amst[j] + (kk * 4) * akst[j]] : 0.0;
           }
 #pragma unroll
           for (int fn = 0; fn < Cfg::FN; ++fn) {
             const int j = fn / FPB, i = fn % FPB;
-            bf[fn] = fn < fn_lim ? sbase[bbase[j] + (i * 8) * bnst[j] + (kk * 4) * bkst[j]] : 0.0;
+            bf[fn] = (fn < fn_lim && kin) ? sbase[bbase[j] + (i * 8) * bnst[j] + (kk * 4) * bkst[j]] : 0.0;
           }
 #pragma unroll
           for (int fm = 0; fm < Cfg::FM; ++fm)
@@ -322,8 +328,9 @@ __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktile
       bkst[j] = tr ? SLD : 1;
       bbase[j] = (Cfg::MT + slot) * SLOT_DOUBLES + c * bnst[j] + (lane & 3) * bkst[j];
     }
-    const int kk_lim = (kvalid(kt) + 3) / 4;
-    const bool full = kk_lim == TS / 4 && fm_lim == Cfg::FM && fn_lim == Cfg::FN;
+    const int kvl = kvalid(kt);
+    const int kk_lim = (kvl + 3) / 4;
+    const bool full = kvl == TS && fm_lim == Cfg::FM && fn_lim == Cfg::FN;
     if constexpr (Cfg::WTM % TS == 0 && Cfg::WTN % TS == 0) {
       // the warp's A slots and B slots; orientations are warp-uniform per slot
       const int sa = warp_m0 / TS, sbs = warp_n0 / TS;
@@ -365,18 +372,20 @@ __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktile
           for (int fn = 0; fn < Cfg::FN; ++fn) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], af[fm], bf[fn]);
       }
     } else {
+      // edge tile: as in dmma_consume, k at or beyond kvalid reads as zero
 #pragma unroll 1
       for (int kk = 0; kk < kk_lim; ++kk) {
         double af[Cfg::FM], bf[Cfg::FN];
+        const bool kin = kk * 4 + (lane & 3) < kvl;
 #pragma unroll
         for (int fm = 0; fm < Cfg::FM; ++fm) {
           const int j = fm / FPA, i = fm % FPA;
-          af[fm] = fm < fm_lim ? sbase[abase[j] + (i * 8) * amst[j] + (kk * 4) * akst[j]] : 0.0;
+          af[fm] = (fm < fm_lim && kin) ? sbase[abase[j] + (i * 8) * amst[j] + (kk * 4) * akst[j]] : 0.0;
         }
 #pragma unroll
         for (int fn = 0; fn < Cfg::FN; ++fn) {
           const int j = fn / FPB, i = fn % FPB;
-          bf[fn] = fn < fn_lim ? sbase[bbase[j] + (i * 8) * bnst[j] + (kk * 4) * bkst[j]] : 0.0;
+          bf[fn] = (fn < fn_lim && kin) ? sbase[bbase[j] + (i * 8) * bnst[j] + (kk * 4) * bkst[j]] : 0.0;
         }
 #pragma unroll
         for (int fm = 0; fm < Cfg::FM; ++fm)

@@ -56,17 +56,38 @@ void launch_k_prepare_c(const Geom& g, const double* eigv, int64_t ld_eigv, int6
 // dense n x n (ld = n) -> padded ldc x ldc copy (zero padding)
 void launch_pad_square(const double* src, int64_t n, int64_t ldsrc, int64_t ldc, double* dst, cudaStream_t st);
 
-// X[p] = B_{p0+p} * W for p in [0, np): W is ldw x ncol (ncol multiple of 64),
-// X[p] is ldx x ncol column-major with ldx = round_up(n, 128), stride sxp.
-// Columns at or beyond ncol_valid of W are zero and their fragments are skipped.
+// Where the half-transform stores column c of X_p = B_p W (p counted from the
+// chunk's first aux row): at column dst(p, c) of X (leading dimension ldx), or
+// nowhere when dst is negative.  Columns [0, lim_a) go to block a with per-row
+// stride pstride_a; columns [coff_b, coff_b + lim_b) to block b, which starts at
+// column base_b, with stride pstride_b.
+struct XMap {
+  int64_t pstride_a;
+  int lim_a;
+  int coff_b, lim_b;
+  int64_t base_b, pstride_b;
+  // every W column of every aux row at stride ncol (X_p is an ldx x ncol block)
+  static XMap dense(int64_t ncol) { return {ncol, (int)ncol, 0, 0, 0, 0}; }
+  __host__ __device__ int64_t dst(int64_t p, int c) const {
+    if (c < lim_a) return p * pstride_a + c;
+    if (c >= coff_b && c < coff_b + lim_b) return base_b + p * pstride_b + (c - coff_b);
+    return -1;
+  }
+};
+
+// X_p = B_{p0+p} * W for p in [0, np): W is ldw x ncol (ncol a multiple of 64);
+// ldx = round_up(n, 128); the columns land where xm says.  Columns at or beyond
+// ncol_valid of W are zero and their fragments are skipped.
 void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
-                           int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, int64_t sxp, int* err,
+                           int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, const XMap& xm, int* err,
                            cudaStream_t st);
-// Kpart[split][q] (128x128 blocks q over block pairs) = sum over p in split,
-// columns [c0, c0+ncol) of X:  X_p X_p^T.  full = 0: pairs Ib<=Jb; 1: all pairs.
+// Kpart[split][q] (128x128 blocks q over block pairs) = sum over the aux rows p
+// of the split of X_p X_p^T, where X holds X_p's nw columns at columns
+// [p nw, (p + 1) nw) (leading dimension ldx; the 32 columns after the last row
+// must be readable).  full = 0: pairs Ib<=Jb; 1: all pairs.
 int k_rank_splits(const Geom& g, int64_t np, int full);
-void launch_k_rank_update(const Geom& g, const double* X, int64_t ldx, int64_t sxp, int64_t np, int64_t c0,
-                          int64_t ncol, int splits, int full, double* Kpart, int* err, cudaStream_t st);
+void launch_k_rank_update(const Geom& g, const double* X, int64_t ldx, int64_t np, int64_t nw, int splits, int full,
+                          double* Kpart, int* err, cudaStream_t st);
 // Kpart[split][q] = sum_p T_p B_{p0+p}  (dm form: T_p = B_p D)
 void launch_k_dm_update(const Geom& g, const double* T, int64_t ldt, int64_t stp, const double* B, int64_t p0,
                         int64_t np, int splits, int full, double* Kpart, int* err, cudaStream_t st);

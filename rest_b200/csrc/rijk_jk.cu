@@ -403,7 +403,7 @@ template <class Cfg>
 __global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_half_transform(const double* __restrict__ B, int64_t ldB, int64_t p0,
                                                                  int nrb, int ncb, const double* __restrict__ W,
                                                                  int64_t ldw, int n, int nt, int ncol_valid,
-                                                                 double* __restrict__ X, int64_t ldx, int64_t sxp,
+                                                                 double* __restrict__ X, int64_t ldx, XMap xm,
                                                                  int* err) {
   extern __shared__ __align__(128) double smem[];
   const int64_t bid = blockIdx.x;
@@ -418,35 +418,36 @@ __global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_half_transfor
   const int ktiles = I0 < nt ? nt : 0;
   const LastTileK kv{nt - 1, n - (nt - 1) * TS};
   if (!dmma_mainloop<Cfg>(sc, ktiles, smem, acc, err, n - I0 * TS, ncol_valid - col0, kv)) return;
-  double* Xp = X + pl * sxp + (int64_t)I0 * TS + (int64_t)col0 * ldx;
+  double* Xr = X + (int64_t)I0 * TS;
   dmma_for_each<Cfg>(acc, [&](int m, int c, double v0, double v1) {
-    Xp[m + (int64_t)c * ldx] = v0;
-    Xp[m + (int64_t)(c + 1) * ldx] = v1;
+    const int64_t d0 = xm.dst(pl, col0 + c), d1 = xm.dst(pl, col0 + c + 1);
+    if (d0 >= 0) Xr[m + d0 * ldx] = v0;
+    if (d1 >= 0) Xr[m + d1 * ldx] = v1;
   });
 }
 
 template <class Cfg>
 static void half_transform_cfg(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
-                               int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, int64_t sxp, int* err,
+                               int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, const XMap& xm, int* err,
                                cudaStream_t st) {
   cudaFuncSetAttribute(k_half_transform<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
   const int nrb = (int)(ldx / Cfg::BM);
   const int ncb = (int)(ncol / Cfg::BN);
   count_launch();
   k_half_transform<Cfg><<<(unsigned)(np * nrb * ncb), Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(
-      B, g.ldB, p0, nrb, ncb, W, ldw, (int)g.n, (int)g.nt, (int)ncol_valid, X, ldx, sxp, err);
+      B, g.ldB, p0, nrb, ncb, W, ldw, (int)g.n, (int)g.nt, (int)ncol_valid, X, ldx, xm, err);
 }
 
 void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
-                           int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, int64_t sxp, int* err,
+                           int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, const XMap& xm, int* err,
                            cudaStream_t st) {
   switch (g.ht_cfg) {
-    case 1: return half_transform_cfg<HtCfg1>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
-    case 2: return half_transform_cfg<HtCfg2>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
-    case 3: return half_transform_cfg<HtCfg3>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
-    case 4: return half_transform_cfg<HtCfg4>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
-    case 5: return half_transform_cfg<HtCfg5>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
-    default: return half_transform_cfg<HtCfg0>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, sxp, err, st);
+    case 1: return half_transform_cfg<HtCfg1>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, st);
+    case 2: return half_transform_cfg<HtCfg2>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, st);
+    case 3: return half_transform_cfg<HtCfg3>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, st);
+    case 4: return half_transform_cfg<HtCfg4>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, st);
+    case 5: return half_transform_cfg<HtCfg5>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, st);
+    default: return half_transform_cfg<HtCfg0>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, st);
   }
 }
 
@@ -503,45 +504,37 @@ __device__ __forceinline__ bool sub_block(int64_t bq, int full, int64_t nkb, int
   return full || Ib != Jb || hm * Cfg::BM < (hn + 1) * Cfg::BN;
 }
 
+// Operands of the rank update: this spin's half-transformed orbitals as one
+// matrix with column k = p * nw + i (aux row p of the chunk, orbital i), so the
+// contraction runs over k without padding between aux rows.
 struct RankSched {
   const double* X;
-  int64_t ldx, sxp;
-  int64_t p0;
-  int ctiles, c0t;  // column tiles per P, first column tile
+  int64_t ldx, k0;
   int64_t mrow0, nrow0;
   __device__ SlotSrc a(int kt, int mt) const {
-    const int64_t p = p0 + kt / ctiles;
-    const int ic = c0t + kt % ctiles;
-    return {X + p * sxp + mrow0 + mt * TS + (int64_t)ic * TS * ldx, ldx, 0};
+    return {X + mrow0 + mt * TS + (k0 + (int64_t)kt * TS) * ldx, ldx, 0};
   }
   __device__ SlotSrc b(int kt, int ntl) const {
-    const int64_t p = p0 + kt / ctiles;
-    const int ic = c0t + kt % ctiles;
-    return {X + p * sxp + nrow0 + ntl * TS + (int64_t)ic * TS * ldx, ldx, 1};
+    return {X + nrow0 + ntl * TS + (k0 + (int64_t)kt * TS) * ldx, ldx, 1};
   }
-};
-
-// Valid occupied columns of the last column tile of every P.
-struct RankK {
-  int ctiles, lastk;
-  __device__ int operator()(int kt) const { return (kt % ctiles) == ctiles - 1 ? lastk : TS; }
 };
 
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_rank_update(const double* __restrict__ X, int64_t ldx, int64_t sxp,
-                                                              int64_t np, int c0t, int ctiles, int lastk, int n,
-                                                              int splits, int full, int64_t nkb, int64_t pairs,
-                                                              double* __restrict__ Kpart, int* err) {
+__global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_rank_update(const double* __restrict__ X, int64_t ldx,
+                                                              int64_t np, int nw, int n, int splits, int full,
+                                                              int64_t nkb, int64_t pairs, double* __restrict__ Kpart,
+                                                              int* err) {
   extern __shared__ __align__(128) double smem[];
   const int sp = blockIdx.y;
   int64_t q, row0, col0, off;
   if (!sub_block<Cfg>(blockIdx.x, full, nkb, q, row0, col0, off)) return;
   const int64_t pa = np * sp / splits, pb = np * (sp + 1) / splits;
-  RankSched sc{X, ldx, sxp, pa, ctiles, c0t, row0, col0};
+  const int64_t kcount = (pb - pa) * nw;
+  RankSched sc{X, ldx, pa * nw, row0, col0};
   double acc[Cfg::FM][Cfg::FN][2];
-  const int ktiles = (int)((pb - pa) * ctiles);
-  if (!dmma_mainloop<Cfg>(sc, ktiles, smem, acc, err, n - (int)row0, n - (int)col0, RankK{ctiles, lastk}))
-    return;
+  const int ktiles = (int)((kcount + TS - 1) / TS);
+  const LastTileK kv{ktiles - 1, (int)(kcount - (int64_t)(ktiles - 1) * TS)};
+  if (!dmma_mainloop<Cfg>(sc, ktiles, smem, acc, err, n - (int)row0, n - (int)col0, kv)) return;
   double* out = Kpart + ((int64_t)sp * pairs + q) * (KB * KB) + off;
   dmma_for_each<Cfg>(acc, [&](int m, int c, double v0, double v1) {
     out[m + KB * c] = v0;
@@ -550,30 +543,27 @@ __global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_rank_update(c
 }
 
 template <class Cfg>
-static void rank_update_cfg(const Geom& g, const double* X, int64_t ldx, int64_t sxp, int64_t np, int64_t c0,
-                            int64_t ncol, int splits, int full, double* Kpart, int* err, cudaStream_t st) {
+static void rank_update_cfg(const Geom& g, const double* X, int64_t ldx, int64_t np, int64_t nw, int splits, int full,
+                            double* Kpart, int* err, cudaStream_t st) {
   cudaFuncSetAttribute(k_rank_update<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
   const int64_t nkb = cdiv(g.n, KB);
   const int64_t pairs = k_block_pairs(g, full);
-  const int c0t = (int)(c0 / TS);
-  const int ctiles = (int)cdiv(ncol, TS);
-  const int lastk = (int)(ncol - (ctiles - 1) * TS);
   constexpr int subs = (KB / Cfg::BM) * (KB / Cfg::BN);
   dim3 grid((unsigned)(pairs * subs), (unsigned)splits);
   count_launch();
-  k_rank_update<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(X, ldx, sxp, np, c0t, ctiles, lastk, (int)g.n,
-                                                                   splits, full, nkb, pairs, Kpart, err);
+  k_rank_update<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(X, ldx, np, (int)nw, (int)g.n, splits, full, nkb,
+                                                                   pairs, Kpart, err);
 }
 
-void launch_k_rank_update(const Geom& g, const double* X, int64_t ldx, int64_t sxp, int64_t np, int64_t c0,
-                          int64_t ncol, int splits, int full, double* Kpart, int* err, cudaStream_t st) {
+void launch_k_rank_update(const Geom& g, const double* X, int64_t ldx, int64_t np, int64_t nw, int splits, int full,
+                          double* Kpart, int* err, cudaStream_t st) {
   switch (g.rk_cfg) {
-    case 1: return rank_update_cfg<RkCfg1>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
-    case 2: return rank_update_cfg<RkCfg2>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
-    case 3: return rank_update_cfg<RkCfg3>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
-    case 4: return rank_update_cfg<RkCfg4>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
-    case 5: return rank_update_cfg<RkCfg5>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
-    default: return rank_update_cfg<RkCfg0>(g, X, ldx, sxp, np, c0, ncol, splits, full, Kpart, err, st);
+    case 1: return rank_update_cfg<RkCfg1>(g, X, ldx, np, nw, splits, full, Kpart, err, st);
+    case 2: return rank_update_cfg<RkCfg2>(g, X, ldx, np, nw, splits, full, Kpart, err, st);
+    case 3: return rank_update_cfg<RkCfg3>(g, X, ldx, np, nw, splits, full, Kpart, err, st);
+    case 4: return rank_update_cfg<RkCfg4>(g, X, ldx, np, nw, splits, full, Kpart, err, st);
+    case 5: return rank_update_cfg<RkCfg5>(g, X, ldx, np, nw, splits, full, Kpart, err, st);
+    default: return rank_update_cfg<RkCfg0>(g, X, ldx, np, nw, splits, full, Kpart, err, st);
   }
 }
 
@@ -602,6 +592,13 @@ struct KdmSched {
     if (kb <= nb) return {Bp + tile_pair_index(kb, nb) * TILE_ELEMS, TS, 0};
     return {Bp + tile_pair_index(nb, kb) * TILE_ELEMS, TS, 1};
   }
+};
+
+// Valid k columns of the last tile of every aux row (k tiles run row by row,
+// ctiles per row).
+struct RankK {
+  int ctiles, lastk;
+  __device__ int operator()(int kt) const { return (kt % ctiles) == ctiles - 1 ? lastk : TS; }
 };
 
 template <class Cfg>
