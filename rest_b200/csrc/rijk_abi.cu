@@ -37,7 +37,8 @@ struct rijk_ctx {
   bool have = false;
   int64_t naux_pad = 0;
   double* dB = nullptr;
-  size_t dB_bytes = 0;
+  size_t dB_bytes = 0;  // the current tensor's size
+  size_t dB_cap = 0;    // the allocation's size (it only grows: a smaller tensor reuses it)
   int* d_err = nullptr;   // device-side wait timeouts
   int* d_info = nullptr;  // Cholesky failing pivot
   DevBuf stage, W, w, Jpart, Cw, X, Kpart, din, dout, docc, mV, mLinv, mT, mLinvd, mOut, Cr, Y, Yp;
@@ -222,10 +223,10 @@ int alloc_tensor(rijk_ctx* ctx, int64_t n, int64_t naux) {
   Geom g = rijk::make_geom(n, naux);
   const int64_t naux_pad = round_up(naux, rijk::TS);
   const size_t bytes = (size_t)naux_pad * g.ldB * sizeof(double);
-  if (ctx->dB && ctx->dB_bytes != bytes) {
+  if (ctx->dB && ctx->dB_cap < bytes) {
     cudaFree(ctx->dB);
     ctx->dB = nullptr;
-    ctx->dB_bytes = 0;
+    ctx->dB_bytes = ctx->dB_cap = 0;
   }
   if (!ctx->dB) {
     cudaError_t e = cudaMalloc(&ctx->dB, bytes);
@@ -235,8 +236,9 @@ int alloc_tensor(rijk_ctx* ctx, int64_t n, int64_t naux) {
       ctx->have = false;
       return set_err(ctx, RIJK_ERR_NOMEM, "tensor allocation of " + std::to_string(bytes) + " bytes failed");
     }
-    ctx->dB_bytes = bytes;
+    ctx->dB_cap = bytes;
   }
+  ctx->dB_bytes = bytes;
   if (naux_pad > naux)
     RIJK_CK(cudaMemsetAsync(ctx->dB + naux * g.ldB, 0, (size_t)(naux_pad - naux) * g.ldB * sizeof(double),
                             ctx->stream));

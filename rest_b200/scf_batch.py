@@ -90,7 +90,7 @@ class BatchedRHF:
                  precision: str = "fp64", integrals: str = "auto", rebuild_every: int = 16,
                  switch_etot: float = 1e-7, switch_rho: float = 1e-5, eig_workers: int = 8,
                  graphs: bool = False, split_min_basis: int = 512, refine_eigs: bool = True,
-                 setup_workers: int = 8, host_blas_threads: int | None = 1):
+                 setup_workers: int = 8, host_blas_threads: int | None = 1, contexts: list | None = None):
         import torch
 
         if precision not in ("fp64", "mixed", "split"):
@@ -116,10 +116,15 @@ class BatchedRHF:
         self.graphs = graphs and precision == "fp64"
         self._graph = None
         self.host_blas_threads = host_blas_threads
+        # contexts lent by the caller (one per molecule, at least as many as
+        # molecules): their tensors are replaced here, and close() leaves them open
+        if contexts is not None and len(contexts) < len(mols):
+            raise ValueError("fewer contexts than molecules")
+        self._borrowed = contexts is not None
         with host_blas_limit(host_blas_threads):
-            self._setup(mols, basis, auxbas, device, metric, integrals, setup_workers)
+            self._setup(mols, basis, auxbas, device, metric, integrals, setup_workers, contexts)
 
-    def _setup(self, mols, basis, auxbas, device, metric, integrals, setup_workers):
+    def _setup(self, mols, basis, auxbas, device, metric, integrals, setup_workers, contexts):
         import torch
 
         t0 = time.perf_counter()
@@ -134,8 +139,8 @@ class BatchedRHF:
             torch.linalg.eigh(torch.eye(2, dtype=torch.float64, device=self.dev))
         tls = threading.local()
 
-        def one(mol):
-            """One molecule's contexts and integrals (host one-electron parts,
+        def one(i, mol):
+            """One molecule's context and integrals (host one-electron parts,
             device nuclear attraction, device three-centre integrals, metric and
             fit), on this thread's own stream; returns when its device work is done."""
             part = {"host_one_electron": 0.0, "contexts": 0.0, "device": 0.0}
@@ -150,7 +155,7 @@ class BatchedRHF:
                     integrals == "auto" and int(bas.l.max()) <= DEVICE_MAX_L_AO and int(aux.l.max()) <= DEVICE_MAX_L_AUX)
                 tk = int1e(mol, bas, "kinetic") if on_device else None
                 tb = time.perf_counter()
-                ctx = RIJK(device)
+                ctx = contexts[i] if contexts is not None else RIJK(device)
                 tc = time.perf_counter()
                 part["host_one_electron"] += tb - ta
                 part["contexts"] += tc - tb
@@ -168,19 +173,20 @@ class BatchedRHF:
                             ctx.build_rimatr_cholesky(v2, i3, n)
                     tls.stream.synchronize()
                 except BaseException:
-                    ctx.close()
+                    if contexts is None:
+                        ctx.close()
                     raise
                 part["device"] += time.perf_counter() - tc
             return ctx, n, h, s, part
 
         nw = max(1, min(setup_workers, len(mols)))
         if nw == 1:
-            outs = [one(m) for m in mols]
+            outs = [one(i, m) for i, m in enumerate(mols)]
         else:
             from concurrent.futures import ThreadPoolExecutor
 
             with ThreadPoolExecutor(nw) as pool:
-                futs = [pool.submit(one, m) for m in mols]
+                futs = [pool.submit(one, i, m) for i, m in enumerate(mols)]
                 outs, err = [], None
                 for f in futs:
                     try:
@@ -188,8 +194,9 @@ class BatchedRHF:
                     except BaseException as e:  # noqa: BLE001  (closed below, then re-raised)
                         err = err or e
             if err is not None:
-                for o in outs:
-                    o[0].close()
+                if contexts is None:
+                    for o in outs:
+                        o[0].close()
                 raise err
         # host time per phase, summed over the setup threads
         parts = {"host_one_electron": 0.0, "contexts": 0.0, "device": 0.0}
@@ -697,7 +704,10 @@ class BatchedRHF:
             self._pool.shutdown()
             self._pool = None
         for c in self.ctx:
-            c.close()
+            if self._borrowed:
+                c.pin_buffers(False)  # pinned for graph replay; the lender may load other tensors
+            else:
+                c.close()
         self.ctx = []
 
 
@@ -750,26 +760,39 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
     eig = {"refined": 0, "eigh": 0}
     parts = {}
     teardown = 0.0
-    for idx in groups:
-        b = BatchedRHF([mols[i] for i in idx], basis, auxbas, device=device, **kw)
-        try:
-            r = b.run(initial_densities=None if guesses is None else [guesses[i] for i in idx], **run_kw)
-        finally:
-            tt = time.perf_counter()
-            b.close()
-            torch.cuda.empty_cache()
-            teardown += time.perf_counter() - tt
-        setup += r.setup_s
-        scf += r.scf_s
-        for k in eig:
-            eig[k] += r.timings["eigensolves"][k]
-        for k, v in list(r.timings["setup_parts"].items()) + list(r.timings["scf_parts"].items()):
-            parts[k] = parts.get(k, 0.0) + v
-        for j, i in enumerate(idx):
-            energies[i], conv[i], iters[i] = r.energies[j], r.converged[j], r.iterations[j]
-            nfp64[i], nsplit[i] = r.timings["fp64_k_builds"][j], r.timings["split_k_builds"][j]
-            if dens:
-                dens[i] = r.densities[j]
+    # One set of contexts serves every group, largest molecules first: a context
+    # keeps its tensor allocation when a smaller tensor replaces it, so the
+    # later groups allocate nothing and only the last group tears down.
+    pool = []
+    try:
+        for idx in reversed(groups):
+            while len(pool) < len(idx):
+                pool.append(RIJK(device))
+            b = BatchedRHF([mols[i] for i in idx], basis, auxbas, device=device, contexts=pool[:len(idx)], **kw)
+            try:
+                r = b.run(initial_densities=None if guesses is None else [guesses[i] for i in idx], **run_kw)
+            finally:
+                tt = time.perf_counter()
+                b.close()
+                torch.cuda.empty_cache()
+                teardown += time.perf_counter() - tt
+            setup += r.setup_s
+            scf += r.scf_s
+            for k in eig:
+                eig[k] += r.timings["eigensolves"][k]
+            for k, v in list(r.timings["setup_parts"].items()) + list(r.timings["scf_parts"].items()):
+                parts[k] = parts.get(k, 0.0) + v
+            for j, i in enumerate(idx):
+                energies[i], conv[i], iters[i] = r.energies[j], r.converged[j], r.iterations[j]
+                nfp64[i], nsplit[i] = r.timings["fp64_k_builds"][j], r.timings["split_k_builds"][j]
+                if dens:
+                    dens[i] = r.densities[j]
+    finally:
+        tt = time.perf_counter()
+        for c in pool:
+            c.close()
+        torch.cuda.empty_cache()
+        teardown += time.perf_counter() - tt
     parts["teardown"] = teardown
     parts["groups"] = len(groups)
     parts["free_bytes_at_start"] = float(budget / memory_fraction)

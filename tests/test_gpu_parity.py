@@ -323,3 +323,28 @@ def test_every_tile_shape_gives_the_same_k(ctx, ht, rk):
         assert _maxdiff(kf, O.vk_full_fromdm_with_ri_v(ri3, [d], 1, 1.0)[0]) <= TOL
     finally:
         ctx.set_tiles(1, 1)
+
+
+def test_smaller_tensor_reuses_the_allocation(ctx):
+    """A context keeps its tensor allocation when a smaller tensor replaces a
+    larger one (the molecule-set driver reuses contexts, largest molecules
+    first): results equal a fresh load's, and the reported size is the new
+    tensor's."""
+    big = host_case(100, 400, 16, seed=31)
+    small = host_case(37, 150, 6, seed=32)
+    ctx.set_rimatr(big.rimatr, 100)
+    size_big = ctx.tensor_bytes()
+    ctx.set_rimatr(small.rimatr, 37)
+    size_small = ctx.tensor_bytes()
+    assert 0 < size_small < size_big
+    nt = -(-37 // 32)
+    assert size_small == (-(-150 // 32) * 32) * nt * (nt + 1) // 2 * 1024 * 8
+    assert np.array_equal(ctx.get_rimatr(), small.rimatr)
+    eig = np.zeros((37, 8), order="F")
+    eig[:, :6] = small.c_occ
+    occ = [np.r_[np.full(6, 2.0), np.zeros(2)]]
+    vj = ctx.vj_upper_with_rimatr_v([small.dm], 1, 1.0)[0]
+    vk = ctx.vk_upper_with_ri_v([eig], [5], occ, 1, -0.5)[0]
+    assert _maxdiff(vj, O.vj_upper_with_rimatr_v(small.rimatr, [small.dm], 1, 1.0)[0]) <= TOL
+    ri3 = O.ri3fn_from_rimatr(small.rimatr, 37)
+    assert _maxdiff(vk, O.vk_upper_with_ri_v(ri3, [eig], [5], occ, 1, -0.5)[0]) <= TOL
