@@ -760,14 +760,32 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
     eig = {"refined": 0, "eigh": 0}
     parts = {}
     teardown = 0.0
-    # One set of contexts serves every group, largest molecules first: a context
-    # keeps its tensor allocation when a smaller tensor replaces it, so the
-    # later groups allocate nothing and only the last group tears down.
-    pool = []
+    # One set of contexts serves the groups, largest molecules first: a context
+    # keeps its tensor and scratch allocations when a smaller molecule replaces
+    # its tensor, so a later group allocates nothing new.  What a pooled context
+    # holds is the estimate for the largest molecule it served; a group reuses
+    # the pool only while held plus new memory stays within the budget, else
+    # the pool is closed and the group starts afresh.
+    pool, held = [], []
     try:
         for idx in reversed(groups):
+            idx = sorted(idx, key=lambda i: -need[i])
+            keep = min(len(pool), len(idx))
+            cost = sum(max(held[j], need[idx[j]]) for j in range(keep)) + sum(need[i] for i in idx[keep:])
+            tt = time.perf_counter()
+            drop = pool[keep:] if cost <= budget else pool
+            for c in drop:
+                c.close()
+            if cost > budget:
+                pool, held = [], []
+            else:
+                pool, held = pool[:keep], held[:keep]
+            teardown += time.perf_counter() - tt
             while len(pool) < len(idx):
                 pool.append(RIJK(device))
+                held.append(0)
+            for j, i in enumerate(idx):
+                held[j] = max(held[j], need[i])
             b = BatchedRHF([mols[i] for i in idx], basis, auxbas, device=device, contexts=pool[:len(idx)], **kw)
             try:
                 r = b.run(initial_densities=None if guesses is None else [guesses[i] for i in idx], **run_kw)
