@@ -724,6 +724,18 @@ def device_bytes(n: int, naux: int, nocc: int, precision: str = "fp64") -> int:
     return tensor + scratch + split + 8 * n * n * 8
 
 
+def pool_reuse(held: list, needs: list, budget: float) -> int:
+    """How many pooled contexts a group keeps.  ``held``: the memory each pooled
+    context holds (the largest molecule it served), ``needs``: the group's
+    molecules, largest first, paired with the pool in order.  Reusing keeps
+    min(len(held), len(needs)) contexts, each then holding the larger of the
+    two, plus fresh contexts for the rest; if that exceeds ``budget`` the pool
+    is dropped (0) and the group starts afresh."""
+    keep = min(len(held), len(needs))
+    cost = sum(max(held[j], needs[j]) for j in range(keep)) + sum(needs[keep:])
+    return keep if cost <= budget else 0
+
+
 def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, device: int = 0,
                      metric: str = "cholesky", memory_fraction: float = 0.5, **kw) -> BatchResult:
     """Converge a molecule set in groups of at most ``group_size`` molecules of
@@ -770,16 +782,11 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
     try:
         for idx in reversed(groups):
             idx = sorted(idx, key=lambda i: -need[i])
-            keep = min(len(pool), len(idx))
-            cost = sum(max(held[j], need[idx[j]]) for j in range(keep)) + sum(need[i] for i in idx[keep:])
+            keep = pool_reuse(held, [need[i] for i in idx], budget)
             tt = time.perf_counter()
-            drop = pool[keep:] if cost <= budget else pool
-            for c in drop:
+            for c in pool[keep:]:
                 c.close()
-            if cost > budget:
-                pool, held = [], []
-            else:
-                pool, held = pool[:keep], held[:keep]
+            pool, held = pool[:keep], held[:keep]
             teardown += time.perf_counter() - tt
             while len(pool) < len(idx):
                 pool.append(RIJK(device))
