@@ -348,3 +348,34 @@ def test_smaller_tensor_reuses_the_allocation(ctx):
     assert _maxdiff(vj, O.vj_upper_with_rimatr_v(small.rimatr, [small.dm], 1, 1.0)[0]) <= TOL
     ri3 = O.ri3fn_from_rimatr(small.rimatr, 37)
     assert _maxdiff(vk, O.vk_upper_with_ri_v(ri3, [eig], [5], occ, 1, -0.5)[0]) <= TOL
+
+
+def test_vk_occupied_form_over_many_aux_chunks(monkeypatch):
+    """A 2 MiB scratch budget splits the aux rows into chunks of 31 (n=200,
+    o=33): each chunk's half-transformed orbitals sit back to back without
+    padding, the rank update's k tiles straddle aux rows, and its splits end
+    on partial k4 steps.  RHF and UHF K against the oracle."""
+    from rest_b200 import RIJK
+
+    monkeypatch.setenv("RIJK_SCRATCH_BYTES", str(2 << 20))
+    n, naux, nocc = 200, 800, 33
+    case = host_case(n, naux, nocc, seed=77)
+    c2, _ = _second_spin(case, 78)
+    ri3 = O.ri3fn_from_rimatr(case.rimatr, n)
+    e1 = np.zeros((n, nocc + 1), order="F")
+    e1[:, :nocc] = case.c_occ
+    e2 = np.zeros((n, nocc + 1), order="F")
+    e2[:, : c2.shape[1]] = c2
+    occ1 = np.r_[np.full(nocc, 2.0), 0.0]
+    occ2 = np.r_[np.full(c2.shape[1], 1.0), np.zeros(nocc + 1 - c2.shape[1])]
+    c = RIJK(0)
+    try:
+        c.set_rimatr(case.rimatr, n)
+        for spin, scale in ((1, -0.5), (2, -1.0)):
+            eig, homo, occ = [e1, e2][:spin], [nocc - 1, c2.shape[1] - 1][:spin], [occ1, occ2][:spin]
+            got = c.vk_upper_with_ri_v(eig, homo, occ, spin, scale)
+            ref = O.vk_upper_with_ri_v(ri3, eig, homo, occ, spin, scale)
+            for s in range(spin):
+                assert _maxdiff(got[s], ref[s]) <= TOL
+    finally:
+        c.close()
