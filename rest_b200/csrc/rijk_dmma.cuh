@@ -226,19 +226,25 @@ __device__ __forceinline__ void cp_async_wait() {
 
 template <class Cfg, class Sched>
 __device__ __forceinline__ void cpa_issue_stage(const Sched& sc, int kt, double* stage, uint8_t* flags) {
-  // 512 16-byte chunks per slot: chunk = column c (0..31) x row pair r2 (0..15)
+  // 512 16-byte chunks per slot: chunk = column c (0..31) x row pair r2 (0..15).
+  // Thread t copies chunks t + THREADS j: with THREADS a multiple of 16 they
+  // share the row pair t % 16 and step THREADS / 16 columns, so one base
+  // address per slot and constant strides cover them.
   constexpr int CHUNKS = 512;
+  static_assert(Cfg::THREADS % 16 == 0 && CHUNKS % Cfg::THREADS == 0, "chunk split");
+  constexpr int NJ = CHUNKS / Cfg::THREADS, CSTEP = Cfg::THREADS / 16;
+  const int c0 = threadIdx.x >> 4, r = (threadIdx.x & 15) * 2;
 #pragma unroll 1
   for (int s = 0; s < Cfg::SLOTS; ++s) {
     const SlotSrc src = (s < Cfg::MT) ? sc.a(kt, s) : sc.b(kt, s - Cfg::MT);
     if (threadIdx.x == 0) flags[s] = (uint8_t)src.trans;
     const double* base = src.ptr ? src.ptr : g_zero_tile;
     const int64_t ld = src.ptr ? src.ld : TS;
-    double* dst = stage + s * SLOT_DOUBLES;
-    for (int ch = threadIdx.x; ch < CHUNKS; ch += Cfg::THREADS) {
-      const int c = ch >> 4, r = (ch & 15) * 2;
-      cp_async16(dst + c * SLD + r, base + (int64_t)c * ld + r);
-    }
+    const double* g = base + (int64_t)c0 * ld + r;
+    const int64_t gstep = (int64_t)CSTEP * ld;
+    double* d = stage + s * SLOT_DOUBLES + c0 * SLD + r;
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) cp_async16(d + j * CSTEP * SLD, g + j * gstep);
   }
 }
 
