@@ -234,7 +234,7 @@ __device__ __forceinline__ void cpa_issue_stage(const Sched& sc, int kt, double*
   static_assert(Cfg::THREADS % 16 == 0 && CHUNKS % Cfg::THREADS == 0, "chunk split");
   constexpr int NJ = CHUNKS / Cfg::THREADS, CSTEP = Cfg::THREADS / 16;
   const int c0 = threadIdx.x >> 4, r = (threadIdx.x & 15) * 2;
-#pragma unroll 1
+#pragma unroll
   for (int s = 0; s < Cfg::SLOTS; ++s) {
     const SlotSrc src = (s < Cfg::MT) ? sc.a(kt, s) : sc.b(kt, s - Cfg::MT);
     if (threadIdx.x == 0) flags[s] = (uint8_t)src.trans;
