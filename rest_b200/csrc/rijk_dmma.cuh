@@ -315,25 +315,6 @@ __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktile
     const int st = kt % S;
     const double* sbase = sm.slots + st * Cfg::STAGE_DOUBLES;
     const uint8_t* fl = sm.flags + st * Cfg::SLOTS;
-    int abase[APS], amst[APS], akst[APS], bbase[BPS], bnst[BPS], bkst[BPS];
-#pragma unroll
-    for (int j = 0; j < APS; ++j) {
-      const int m = warp_m0 + j * TS;
-      const int slot = m / TS, r = m % TS + (lane >> 2);
-      const int tr = fl[slot];
-      amst[j] = tr ? SLD : 1;
-      akst[j] = tr ? 1 : SLD;
-      abase[j] = slot * SLOT_DOUBLES + r * amst[j] + (lane & 3) * akst[j];
-    }
-#pragma unroll
-    for (int j = 0; j < BPS; ++j) {
-      const int c0 = warp_n0 + j * TS;
-      const int slot = c0 / TS, c = c0 % TS + (lane >> 2);
-      const int tr = fl[Cfg::MT + slot];
-      bnst[j] = tr ? 1 : SLD;
-      bkst[j] = tr ? SLD : 1;
-      bbase[j] = (Cfg::MT + slot) * SLOT_DOUBLES + c * bnst[j] + (lane & 3) * bkst[j];
-    }
     const int kvl = kvalid(kt);
     const int kk_lim = (kvl + 3) / 4;
     const bool full = kvl == TS && fm_lim == Cfg::FM && fn_lim == Cfg::FN;
@@ -357,6 +338,26 @@ __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktile
           dmma_ktile_fixed<Cfg, true, true>(sbase, sa, sbs, lane, acc);
         continue;
       }
+    }
+    // general path: per-slot fragment bases and strides from the orientation flags
+    int abase[APS], amst[APS], akst[APS], bbase[BPS], bnst[BPS], bkst[BPS];
+#pragma unroll
+    for (int j = 0; j < APS; ++j) {
+      const int m = warp_m0 + j * TS;
+      const int slot = m / TS, r = m % TS + (lane >> 2);
+      const int tr = fl[slot];
+      amst[j] = tr ? SLD : 1;
+      akst[j] = tr ? 1 : SLD;
+      abase[j] = slot * SLOT_DOUBLES + r * amst[j] + (lane & 3) * akst[j];
+    }
+#pragma unroll
+    for (int j = 0; j < BPS; ++j) {
+      const int c0 = warp_n0 + j * TS;
+      const int slot = c0 / TS, c = c0 % TS + (lane >> 2);
+      const int tr = fl[Cfg::MT + slot];
+      bnst[j] = tr ? 1 : SLD;
+      bkst[j] = tr ? SLD : 1;
+      bbase[j] = (Cfg::MT + slot) * SLOT_DOUBLES + c * bnst[j] + (lane & 3) * bkst[j];
     }
     if (full) {
 #pragma unroll
