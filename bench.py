@@ -660,10 +660,15 @@ def molecule_set_in_child(device: int, nmol: int) -> dict:
     import torch
 
     torch.cuda.empty_cache()  # this process's cached blocks go back to the device for the child
-    out = subprocess.run([sys.executable, os.path.abspath(__file__), "--molecule-set-only", str(nmol),
-                          "--device", str(device)], capture_output=True, text=True, timeout=1800)
+    try:
+        out = subprocess.run([sys.executable, os.path.abspath(__file__), "--molecule-set-only", str(nmol),
+                              "--device", str(device)], capture_output=True, text=True, timeout=1800)
+    except subprocess.TimeoutExpired:
+        return {"error": "molecule-set child process timed out after 1800 s"}
     if out.returncode != 0:
-        raise RuntimeError("molecule-set measurement failed:\n" + out.stderr[-4000:])
+        # the headline line still prints; this config reports why it has no numbers
+        print(out.stderr[-4000:], file=sys.stderr)
+        return {"error": "molecule-set child process failed: " + (out.stderr.strip().splitlines() or ["?"])[-1]}
     res = json.loads(out.stdout.strip().splitlines()[-1])
     res["process"] = "measured in a fresh child process"
     return res
