@@ -251,9 +251,12 @@ __device__ __forceinline__ void cpa_issue_stage(const Sched& sc, int kt, double*
 // One full k-tile (32 k) of a warp whose A slots (consecutive, from slot_a) all
 // have orientation TA and whose B slots (consecutive, from slot_b) all have
 // orientation TB: every fragment address is the warp's base plus an immediate.
-template <class Cfg, bool TA, bool TB>
+// PARTIAL: only fragments fm < fm_lim, fn < fn_lim are loaded and multiplied
+// (the warp's tile straddles the valid rows or columns); the k-tile is full.
+template <class Cfg, bool TA, bool TB, bool PARTIAL = false>
 __device__ __forceinline__ void dmma_ktile_fixed(const double* __restrict__ sbase, int slot_a, int slot_b, int lane,
-                                                 double (&acc)[Cfg::FM][Cfg::FN][2]) {
+                                                 double (&acc)[Cfg::FM][Cfg::FN][2], int fm_lim = Cfg::FM,
+                                                 int fn_lim = Cfg::FN) {
   constexpr int AMST = TA ? SLD : 1, AKST = TA ? 1 : SLD;
   constexpr int BNST = TB ? 1 : SLD, BKST = TB ? SLD : 1;
   constexpr int APS = Cfg::WTM >= TS ? Cfg::WTM / TS : 1;
@@ -266,14 +269,15 @@ __device__ __forceinline__ void dmma_ktile_fixed(const double* __restrict__ sbas
     double af[Cfg::FM], bf[Cfg::FN];
 #pragma unroll
     for (int fm = 0; fm < Cfg::FM; ++fm)
-      af[fm] = sa[(fm / FPA) * SLOT_DOUBLES + ((fm % FPA) * 8) * AMST + (kk * 4) * AKST];
+      if (!PARTIAL || fm < fm_lim) af[fm] = sa[(fm / FPA) * SLOT_DOUBLES + ((fm % FPA) * 8) * AMST + (kk * 4) * AKST];
 #pragma unroll
     for (int fn = 0; fn < Cfg::FN; ++fn)
-      bf[fn] = sb[(fn / FPB) * SLOT_DOUBLES + ((fn % FPB) * 8) * BNST + (kk * 4) * BKST];
+      if (!PARTIAL || fn < fn_lim) bf[fn] = sb[(fn / FPB) * SLOT_DOUBLES + ((fn % FPB) * 8) * BNST + (kk * 4) * BKST];
 #pragma unroll
     for (int fm = 0; fm < Cfg::FM; ++fm)
 #pragma unroll
-      for (int fn = 0; fn < Cfg::FN; ++fn) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], af[fm], bf[fn]);
+      for (int fn = 0; fn < Cfg::FN; ++fn)
+        if (!PARTIAL || (fm < fm_lim && fn < fn_lim)) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], af[fm], bf[fn]);
   }
 }
 
@@ -337,6 +341,21 @@ __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktile
         else
           dmma_ktile_fixed<Cfg, true, true>(sbase, sa, sbs, lane, acc);
         continue;
+      }
+      if constexpr (Cfg::THREADS == 128 && Cfg::FM * Cfg::FN == 16 && 3 * Cfg::SMEM_BYTES <= 227 * 1024) {
+        if (kvl == TS && uniform) {
+          // full k-tile, warp tile straddling the valid rows or columns (the
+          // 4-warp 64x64 shapes only: the variant costs registers)
+          if (!ta && !tb)
+            dmma_ktile_fixed<Cfg, false, false, true>(sbase, sa, sbs, lane, acc, fm_lim, fn_lim);
+          else if (ta && !tb)
+            dmma_ktile_fixed<Cfg, true, false, true>(sbase, sa, sbs, lane, acc, fm_lim, fn_lim);
+          else if (!ta && tb)
+            dmma_ktile_fixed<Cfg, false, true, true>(sbase, sa, sbs, lane, acc, fm_lim, fn_lim);
+          else
+            dmma_ktile_fixed<Cfg, true, true, true>(sbase, sa, sbs, lane, acc, fm_lim, fn_lim);
+          continue;
+        }
       }
     }
     // general path: per-slot fragment bases and strides from the orientation flags

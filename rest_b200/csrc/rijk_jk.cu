@@ -372,6 +372,9 @@ using HtCfg5 = DmmaCfg<2, 4, 2, 2, 2, true>;  // 64 x 128, 4 warps of 32 x 64, c
 // for the shape with 32 x 64 warp tiles (up to 255 registers).
 template <class Cfg>
 constexpr int min_ctas() {
+  // 4-warp 64x64 shapes whose shared memory lets three CTAs share an SM ask
+  // for registers that let them (<= 170 per thread)
+  if (Cfg::THREADS == 128 && Cfg::FM * Cfg::FN == 16 && 3 * Cfg::SMEM_BYTES <= 227 * 1024) return 3;
   return (Cfg::THREADS >= 256 || Cfg::FM * Cfg::FN >= 32) ? 2 : 1;
 }
 
