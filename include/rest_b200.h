@@ -54,7 +54,10 @@ int rijk_ctx_create(int device, rijk_ctx** out);
 int rijk_ctx_destroy(rijk_ctx* ctx);
 const char* rijk_ctx_last_error(const rijk_ctx* ctx);
 const char* rijk_status_string(int status);
-/* Sizes of the loaded tensor (0 if none) and device bytes it occupies. */
+/* Sizes of the loaded tensor (0 if none) and device bytes it occupies.  A
+ * context keeps its tensor allocation when a smaller tensor replaces a larger
+ * one (a set of molecules can reuse one context, largest first); tensor_bytes
+ * is the loaded tensor's size, which may be less than the context holds. */
 int rijk_ctx_info(const rijk_ctx* ctx, int64_t* num_basis, int64_t* num_auxbas, int64_t* tensor_bytes);
 /* The context's CUDA stream (a cudaStream_t). */
 void* rijk_ctx_stream(rijk_ctx* ctx);
