@@ -43,7 +43,9 @@ enum rijk_status {
   RIJK_ERR_NO_TENSOR = 4,  /* no fitted tensor loaded in the context               */
   RIJK_ERR_TIMEOUT = 5,    /* a device-side wait ran out of its time budget         */
   RIJK_ERR_NOMEM = 6,      /* device allocation failed                              */
-  RIJK_ERR_NONFINITE = 7,  /* NaN/Inf found in an input                             */
+  RIJK_ERR_NONFINITE = 7,  /* NaN/Inf in a density, orbital or occupation element a
+                              build reads (checked on the device, reported by the
+                              next synchronising call)                             */
   RIJK_ERR_TOO_LARGE = 8   /* size beyond a documented maximum                      */
 };
 
@@ -105,6 +107,17 @@ int rijk_ctx_autotune(rijk_ctx* ctx, int64_t ncols, int64_t sample_rows, int* be
  * capturing those calls into a CUDA graph, so that the graph's pointers stay
  * valid for as long as it is replayed. */
 int rijk_ctx_pin_buffers(rijk_ctx* ctx, int pinned);
+/* No counterpart in REST (its CPU build has no device-side waits).  Every
+ * device-side wait in this context's kernels gives up after `nanoseconds` of
+ * the GPU's global timer (0 = the default of 2 s; otherwise 10 ms to 600 s);
+ * the next synchronising call then returns RIJK_ERR_TIMEOUT and the context
+ * stays usable. */
+int rijk_ctx_set_wait_budget(rijk_ctx* ctx, int64_t nanoseconds);
+/* Runs one bounded wait on a barrier that nothing completes (one CTA, no copy
+ * in flight), so that a caller can check that a device-side wait that runs out
+ * is reported as RIJK_ERR_TIMEOUT, without any fault, and that the context
+ * stays usable.  Returns RIJK_ERR_TIMEOUT when the path works. */
+int rijk_ctx_selftest_timeout(rijk_ctx* ctx);
 int rijk_ctx_profile(rijk_ctx* ctx, int enable);
 int rijk_ctx_profile_read(rijk_ctx* ctx, double* ms, int64_t* launches);
 /* Wait for the work enqueued on `stream` (NULL = the context's stream) and
@@ -215,9 +228,13 @@ int rijk_vk_upper_lowrank_split_dev(rijk_ctx* ctx, const double* d_V, int64_t ld
  * every GPU loading the library holds until exit; sizes needing more
  * (2 spin ldB + spin N doubles: n <= 2016 for spin 1 and n <= 1408 for
  * spin 2 at N = 4n) return RIJK_ERR_TOO_LARGE.  The first call on a device
- * looks the array's address up (cudaGetSymbolAddress); make that first call
- * before any stream capture.  All calls share the array: calls that overlap on
- * the GPU race and must be serialised by the caller. */
+ * looks the array's address up (cudaGetSymbolAddress) and caches it by device
+ * ordinal; make that first call before any stream capture.  The current device
+ * at the call must be the device the pointers and the stream belong to, and the
+ * library must not be used across a cudaDeviceReset of that device.  All calls
+ * share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller.  An error already pending in the CUDA runtime when the call
+ * starts is returned as RIJK_ERR_CUDA and left pending. */
 #define RIJK_NOALLOC_SCRATCH_BYTES (32ull << 20)
 int rijk_vj_upper_noalloc(const double* d_tensor, int64_t row_stride, int64_t num_basis, int64_t num_auxbas,
                           const double* d_dm, int spin_channel, double scaling_factor, int dm_mode, double* d_vj,

@@ -12,8 +12,10 @@ functions only print), and REST itself (Rust, with the unvendored crates
 ``rest_tensors`` / ``rest_libcint``) cannot be built here.  The restatement is
 therefore checked against analytic identities, against a second independent
 formulation inside this file (full ``ri3fn`` layout vs packed ``rimatr``,
-V^-1/2 metric vs Cholesky metric), and against REST's example energies through
-``oracle/gto_oracle.py``.
+V^-1/2 metric vs Cholesky metric), and against REST's published example energy
+(pentacene RI-HF, ``examples/PEN/RIHF/rest.out``): ``oracle/scf_ctx.py`` runs
+the SCF loop on these formulas and ``tests/test_scf_oracle.py`` compares it
+with the values in ``tests/golden/pen_rihf.json``.
 
 Storage conventions follow REST (column-major everywhere):
 

@@ -69,6 +69,8 @@ SIGNATURES = {
     "rijk_ctx_profile": (C.c_int, [_ctxp, C.c_int]),
     "rijk_ctx_set_tiles": (C.c_int, [_ctxp, C.c_int, C.c_int]),
     "rijk_ctx_pin_buffers": (C.c_int, [_ctxp, C.c_int]),
+    "rijk_ctx_set_wait_budget": (C.c_int, [_ctxp, C.c_int64]),
+    "rijk_ctx_selftest_timeout": (C.c_int, [_ctxp]),
     "rijk_ctx_autotune": (
         C.c_int,
         [_ctxp, C.c_int64, C.c_int64, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp],

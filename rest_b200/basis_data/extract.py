@@ -40,4 +40,6 @@ def main(pool: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/basis-set-pool")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python -m rest_b200.basis_data.extract <REST checkout>/basis-set-pool")
+    main(sys.argv[1])

@@ -198,6 +198,8 @@ int sync_and_check(rijk_ctx* ctx, cudaStream_t st) {
   RIJK_CK(cudaMemcpy(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (h != 0) {
     RIJK_CK(cudaMemset(ctx->d_err, 0, sizeof(int)));
+    if (h == rijk::DEV_NONFINITE)
+      return set_err(ctx, RIJK_ERR_NONFINITE, "a density, orbital or occupation element read was NaN or Inf");
     return set_err(ctx, RIJK_ERR_TIMEOUT, "a device-side wait exceeded its time budget");
   }
   return RIJK_OK;
@@ -325,7 +327,7 @@ int vj_dev(rijk_ctx* ctx, const double* d_dm, int spin, double scale, int mode, 
   double* Jp = static_cast<double*>(ctx->Jpart.p);
   {
     ProfScope ps(ctx, RIJK_PROF_J_OTHER, st);
-    rijk::launch_j_weights(g, d_dm, spin, mode, W, st);
+    rijk::launch_j_weights(g, d_dm, spin, mode, W, ctx->d_err, st);
   }
   {
     ProfScope ps(ctx, RIJK_PROF_J_PASS1, st);
@@ -359,7 +361,8 @@ int vk_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int
   double* Cw = static_cast<double*>(ctx->Cw.p);
   {
     ProfScope ps(ctx, RIJK_PROF_K_OTHER, st);
-    rijk::launch_k_prepare_c(g, d_eigv, g.n, g.n * num_state, d_occ, num_state, nw, spin, ldx, ocols, Cw, st);
+    rijk::launch_k_prepare_c(g, d_eigv, g.n, g.n * num_state, d_occ, num_state, nw, spin, ldx, ocols, Cw, ctx->d_err,
+                             st);
   }
   // X holds, per spin, the chunk's X_p back to back without padding (column
   // p nw + i), spin beta after spin alpha, and 32 spare columns for the rank
@@ -411,7 +414,7 @@ int vk_dm_dev(rijk_ctx* ctx, const double* d_dm, int spin, double scale, int ful
   for (int s = 0; s < spin; ++s) {
     {
       ProfScope ps(ctx, RIJK_PROF_K_OTHER, st);
-      rijk::launch_pad_square(d_dm + s * g.n * g.n, g.n, g.n, ldx, Dp, st);
+      rijk::launch_pad_square(d_dm + s * g.n * g.n, g.n, g.n, ldx, Dp, ctx->d_err, st);
     }
     for (int64_t p0 = 0; p0 < g.naux; p0 += pchunk) {
       const int64_t np = std::min(pchunk, g.naux - p0);
@@ -507,12 +510,13 @@ int rijk_ctx_create(int device, rijk_ctx** out) {
     if (v > (1 << 20)) c->scratch_budget = (size_t)v;
   }
   keep_pool_memory(device);
-  // the timeout flag and the Cholesky pivot share one allocation (d_err owns it)
+  // the error flag, the Cholesky pivot and the wait budget share one
+  // allocation (d_err owns it; layout in rijk_common.cuh, ERR_WORDS)
   bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaMalloc(&c->d_err, 2 * sizeof(int)) == cudaSuccess;
+            cudaMalloc(&c->d_err, rijk::ERR_WORDS * sizeof(int)) == cudaSuccess;
   if (ok) {
     c->d_info = c->d_err + 1;
-    ok = cudaMemsetAsync(c->d_err, 0, 2 * sizeof(int), c->stream) == cudaSuccess &&
+    ok = cudaMemsetAsync(c->d_err, 0, rijk::ERR_WORDS * sizeof(int), c->stream) == cudaSuccess &&
          cudaStreamSynchronize(c->stream) == cudaSuccess;
   }
   if (!ok) {
@@ -563,6 +567,25 @@ int rijk_ctx_pin_buffers(rijk_ctx* ctx, int pinned) {
   if (!ctx) return RIJK_ERR_ARG;
   ctx->pinned = pinned != 0;
   return RIJK_OK;
+}
+
+int rijk_ctx_set_wait_budget(rijk_ctx* ctx, int64_t nanoseconds) {
+  if (!ctx) return RIJK_ERR_ARG;
+  if (nanoseconds != 0 && (nanoseconds < 10000000 || nanoseconds > 600000000000LL))
+    return set_err(ctx, RIJK_ERR_ARG, "wait budget must be 0 (default) or between 10 ms and 600 s");
+  RIJK_CK(cudaSetDevice(ctx->device));
+  const uint64_t v = (uint64_t)nanoseconds;
+  RIJK_CK(cudaMemcpyAsync(ctx->d_err + 2, &v, sizeof(v), cudaMemcpyHostToDevice, ctx->stream));
+  RIJK_CK(cudaStreamSynchronize(ctx->stream));
+  return RIJK_OK;
+}
+
+int rijk_ctx_selftest_timeout(rijk_ctx* ctx) {
+  if (!ctx) return RIJK_ERR_ARG;
+  RIJK_CK(cudaSetDevice(ctx->device));
+  rijk::launch_wait_selftest(ctx->d_err, ctx->stream);
+  RIJK_TRY(after_launch(ctx, "wait self-test"));
+  return sync_and_check(ctx, ctx->stream);
 }
 
 int rijk_ctx_set_tiles(rijk_ctx* ctx, int half_transform_cfg, int update_cfg) {
@@ -999,7 +1022,7 @@ int rijk_density_matrix(rijk_ctx* ctx, const double* eigv, int64_t num_basis, in
     RIJK_TRY(ensure(ctx, ctx->Cw, (size_t)ld * kc * 8));
     double* Cw = static_cast<double*>(ctx->Cw.p);
     rijk::launch_k_prepare_c(g, din + s * n * num_state, n, 0, static_cast<double*>(ctx->docc.p) + s * num_state, 0,
-                             nw, 1, ld, kc, Cw, ctx->stream);
+                             nw, 1, ld, kc, Cw, ctx->d_err, ctx->stream);
     rijk::launch_dgemm(ld, ld, kc, 1.0, Cw, ld, 0, Cw, ld, 1, 0.0, dout + s * ld * ld, ld, 0, 0, 1, 0, 0, 0,
                        ctx->d_err, ctx->stream);
     RIJK_TRY(after_launch(ctx, "density"));
@@ -1098,7 +1121,7 @@ int rijk_vk_upper_occ_split_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num
     RIJK_TRY(ensure(ctx, ctx->Cw, (size_t)ldx * oc * 8));
     double* Cw = static_cast<double*>(ctx->Cw.p);
     rijk::launch_k_prepare_c(g, d_eigv + (size_t)s * g.n * num_state, g.n, 0, d_occupation + (size_t)s * num_state, 0,
-                             nw, 1, ldx, oc, Cw, st);
+                             nw, 1, ldx, oc, Cw, ctx->d_err, st);
     RIJK_TRY(rijk_vk_upper_lowrank_split_dev(ctx, Cw, ldx, nw[0], nw[0], scaling_factor, 0, d_vk + s * g.npair, st));
   }
   return RIJK_OK;

@@ -2,6 +2,7 @@
 // three-centre tensor, error flag, bounded mbarrier waits, bulk copies.
 #pragma once
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 namespace rijk {
@@ -48,10 +49,28 @@ enum Status : int {
 enum DevErr : int {
   DEV_OK = 0,
   DEV_WAIT_TIMEOUT = 1,
+  DEV_NONFINITE = 2,
 };
 
-// A wait on an mbarrier gives up after this many nanoseconds of %globaltimer.
+// The error word a kernel receives is the first of four ints a context owns:
+// [0] the device-side error flag, [1] the Cholesky failing pivot, [2..3] the
+// context's wait budget in nanoseconds (uint64; 0 = WAIT_LIMIT_NS).
+constexpr int ERR_WORDS = 4;
+
+// A wait on an mbarrier gives up after this many nanoseconds of %globaltimer
+// unless the context sets another budget.
 constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s
+
+__device__ __forceinline__ uint64_t wait_budget_ns(const int* err) {
+  if (!err) return WAIT_LIMIT_NS;
+  const uint64_t b = *reinterpret_cast<const volatile uint64_t*>(err + 2);
+  return b ? b : WAIT_LIMIT_NS;
+}
+
+// Records a non-finite input value (first error wins).
+__device__ __forceinline__ void flag_nonfinite(int* err, double v) {
+  if (err && !isfinite(v)) atomicCAS(err, DEV_OK, DEV_NONFINITE);
+}
 
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;
@@ -90,13 +109,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait: returns false (and records DEV_WAIT_TIMEOUT) if the phase did
-// not complete within WAIT_LIMIT_NS.
+// not complete within the context's wait budget (WAIT_LIMIT_NS by default).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
+  const uint64_t limit = wait_budget_ns(err);
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (globaltimer_ns() - t0 > WAIT_LIMIT_NS) {
+    if (globaltimer_ns() - t0 > limit) {
       if (err) atomicCAS(err, DEV_OK, DEV_WAIT_TIMEOUT);
       return false;
     }

@@ -37,7 +37,10 @@ void launch_unpack_rimatr(const Geom& g, const double* src, int64_t np, double* 
 // --- J ------------------------------------------------------------------------
 // mode 0: full n*n dot (vj_upper_with_ri_v); mode 1: packed-upper formula
 // (vj_upper_with_rimatr_v).  dm: nspin matrices n*n column-major, stride n*n.
-void launch_j_weights(const Geom& g, const double* dm, int nspin, int mode, double* W, cudaStream_t st);
+// One CTA waits (bounded by the context's budget) on an mbarrier that nothing
+// completes, and records DEV_WAIT_TIMEOUT: the timeout path without a fault.
+void launch_wait_selftest(int* err, cudaStream_t st);
+void launch_j_weights(const Geom& g, const double* dm, int nspin, int mode, double* W, int* err, cudaStream_t st);
 // w[s*naux + P] = sum_k B[P,k] W[s*ldB + k]
 void launch_j_pass1(const Geom& g, const double* B, const double* W, int nspin, double* w, cudaStream_t st);
 // number of P-splits pass 2 uses (scratch = splits * nspin * ldB doubles)
@@ -52,9 +55,10 @@ void launch_j_finalize(const Geom& g, const double* Jpart, int nspin, int splits
 // Cw[s] (ldc x ocols, column-major, zero padded) = C_s[:, :nw_s] * sqrt(occ_s)
 void launch_k_prepare_c(const Geom& g, const double* eigv, int64_t ld_eigv, int64_t stride_eigv,
                         const double* occ, int64_t stride_occ, const int64_t* nw, int nspin, int64_t ldc,
-                        int64_t ocols, double* Cw, cudaStream_t st);
+                        int64_t ocols, double* Cw, int* err, cudaStream_t st);
 // dense n x n (ld = n) -> padded ldc x ldc copy (zero padding)
-void launch_pad_square(const double* src, int64_t n, int64_t ldsrc, int64_t ldc, double* dst, cudaStream_t st);
+void launch_pad_square(const double* src, int64_t n, int64_t ldsrc, int64_t ldc, double* dst, int* err,
+                       cudaStream_t st);
 
 // Where the half-transform stores column c of X_p = B_p W (p counted from the
 // chunk's first aux row): at column dst(p, c) of X (leading dimension ldx), or

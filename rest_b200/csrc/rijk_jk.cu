@@ -93,6 +93,27 @@ void launch_unpack_rimatr(const Geom& g, const double* src, int64_t np, double* 
 }
 
 // ============================================================================
+// failure detection
+// ============================================================================
+// Thread 0 initialises an mbarrier that expects one arrival and then waits on
+// its first phase, which nothing completes.  The bounded wait gives up after
+// the context's budget and records DEV_WAIT_TIMEOUT; no copy is in flight and
+// no other thread depends on the barrier, so the CTA simply returns.
+__global__ void k_wait_selftest(int* err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+    mbar_wait_bounded(&bar, 0, err);
+  }
+}
+
+void launch_wait_selftest(int* err, cudaStream_t st) {
+  count_launch();
+  k_wait_selftest<<<1, 32, 0, st>>>(err);
+}
+
+// ============================================================================
 // J
 // ============================================================================
 // W[s*ldB + k]: the density folded onto the stored tile elements so that
@@ -102,7 +123,7 @@ void launch_unpack_rimatr(const Geom& g, const double* src, int64_t np, double* 
 //   mode 1 (packed formula, :2513-2527): off-diagonal tiles 2 D[mu,nu] (mu < nu),
 //          diagonal tiles D[min, max], which sums to 2 sum_{mu<=nu} - sum_diag.
 __global__ void __launch_bounds__(256) k_j_weights(int64_t n, int64_t ldB, const double* __restrict__ dm, int nspin,
-                                                   int mode, double* __restrict__ W) {
+                                                   int mode, double* __restrict__ W, int* err) {
   const int64_t total = (int64_t)nspin * ldB;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t s = e / ldB, k = e - s * ldB;
@@ -119,16 +140,17 @@ __global__ void __launch_bounds__(256) k_j_weights(int64_t n, int64_t ldB, const
         const int64_t i = mu < nu ? mu : nu, j = mu < nu ? nu : mu;
         v = mode == 0 ? D[mu + n * nu] : D[i + n * j];
       }
+      flag_nonfinite(err, v);
     }
     W[e] = v;
   }
 }
 
-void launch_j_weights(const Geom& g, const double* dm, int nspin, int mode, double* W, cudaStream_t st) {
+void launch_j_weights(const Geom& g, const double* dm, int nspin, int mode, double* W, int* err, cudaStream_t st) {
   const int64_t total = nspin * g.ldB;
   const unsigned blocks = (unsigned)std::min<int64_t>(cdiv(total, 256), 148 * 16);
   count_launch();
-  k_j_weights<<<blocks, 256, 0, st>>>(g.n, g.ldB, dm, nspin, mode, W);
+  k_j_weights<<<blocks, 256, 0, st>>>(g.n, g.ldB, dm, nspin, mode, W, err);
 }
 
 __device__ __forceinline__ double2 ld_stream(const double2* p) { return __ldcs(p); }
@@ -313,7 +335,8 @@ void launch_j_finalize(const Geom& g, const double* Jpart, int nspin, int splits
 __global__ void __launch_bounds__(256) k_prepare_c(int64_t n, const double* __restrict__ eigv, int64_t ld_eigv,
                                                    int64_t stride_eigv, const double* __restrict__ occ,
                                                    int64_t stride_occ, int64_t nw0, int64_t nw1, int64_t coff1,
-                                                   int nspin, int64_t ldc, int64_t ocols, double* __restrict__ Cw) {
+                                                   int nspin, int64_t ldc, int64_t ocols, double* __restrict__ Cw,
+                                                   int* err) {
   const int64_t total = ldc * ocols;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t row = e % ldc, col = e / ldc;
@@ -327,36 +350,46 @@ __global__ void __launch_bounds__(256) k_prepare_c(int64_t n, const double* __re
       s = 1;
       i = col - coff1;
     }
-    if (s >= 0 && row < n) v = eigv[s * stride_eigv + row + ld_eigv * i] * sqrt(occ[s * stride_occ + i]);
+    if (s >= 0 && row < n) {
+      const double o = occ[s * stride_occ + i];
+      v = eigv[s * stride_eigv + row + ld_eigv * i] * sqrt(o);
+      flag_nonfinite(err, v);  // NaN/Inf orbitals or occupations (and negative occupations)
+    }
     Cw[e] = v;
   }
 }
 
 void launch_k_prepare_c(const Geom& g, const double* eigv, int64_t ld_eigv, int64_t stride_eigv, const double* occ,
                         int64_t stride_occ, const int64_t* nw, int nspin, int64_t ldc, int64_t ocols, double* Cw,
-                        cudaStream_t st) {
+                        int* err, cudaStream_t st) {
   const int64_t coff1 = round_up(nw[0], TS);
   const int64_t total = ldc * ocols;
   const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), 148 * 16));
   count_launch();
   k_prepare_c<<<blocks, 256, 0, st>>>(g.n, eigv, ld_eigv, stride_eigv, occ, stride_occ, nw[0], nspin == 2 ? nw[1] : 0,
-                                      coff1, nspin, ldc, ocols, Cw);
+                                      coff1, nspin, ldc, ocols, Cw, err);
 }
 
 __global__ void __launch_bounds__(256) k_pad_square(const double* __restrict__ src, int64_t n, int64_t ldsrc,
-                                                    int64_t ldc, double* __restrict__ dst) {
+                                                    int64_t ldc, double* __restrict__ dst, int* err) {
   const int64_t total = ldc * ldc;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t r = e % ldc, c = e / ldc;
-    dst[e] = (r < n && c < n) ? src[r + ldsrc * c] : 0.0;
+    double v = 0.0;
+    if (r < n && c < n) {
+      v = src[r + ldsrc * c];
+      flag_nonfinite(err, v);
+    }
+    dst[e] = v;
   }
 }
 
-void launch_pad_square(const double* src, int64_t n, int64_t ldsrc, int64_t ldc, double* dst, cudaStream_t st) {
+void launch_pad_square(const double* src, int64_t n, int64_t ldsrc, int64_t ldc, double* dst, int* err,
+                       cudaStream_t st) {
   const int64_t total = ldc * ldc;
   const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), 148 * 16));
   count_launch();
-  k_pad_square<<<blocks, 256, 0, st>>>(src, n, ldsrc, ldc, dst);
+  k_pad_square<<<blocks, 256, 0, st>>>(src, n, ldsrc, ldc, dst, err);
 }
 
 // ---- half-transform: X_p = B_p W ------------------------------------------

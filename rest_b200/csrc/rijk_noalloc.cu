@@ -17,9 +17,16 @@
 // host threads) race on it and must be ordered by the caller.  Each call
 // overwrites every scratch element it reads, so nothing needs clearing
 // between calls.
+//
+// The array's device address is looked up once per device ordinal and cached
+// for the life of the process.  The device that is current when the call is
+// made must be the one the pointers belong to, and the library must not be
+// used across a cudaDeviceReset of that device (the reset unloads the module,
+// and the cached address would then point at released memory).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "../../include/rest_b200.h"
@@ -71,17 +78,28 @@ extern "C" int rijk_vj_upper_noalloc(const double* d_tensor, int64_t row_stride,
   const int64_t need = jp_off + spin_channel * g.ldB;
   if (need > (int64_t)kScratchDoubles) return RIJK_ERR_TOO_LARGE;
   if (row_stride != g.ldB) return RIJK_ERR_ARG;
+  // An error left pending by the caller's own work is not this call's to
+  // clear: report it and leave it for the caller's check.
+  if (cudaPeekAtLastError() != cudaSuccess) return RIJK_ERR_CUDA;
   double* s = nullptr;
   const int st = scratch_on_current_device(&s);
   if (st != RIJK_OK) return st;
+  // Pass 2 splits the aux rows over as many partial sums as the allocating
+  // path uses, as far as the array has room for them (the same split count
+  // gives the same summation order).
+  const int64_t room = ((int64_t)kScratchDoubles - jp_off) / (spin_channel * g.ldB);
+  const int splits = (int)std::max<int64_t>(1, std::min<int64_t>(rijk::j_pass2_splits(g), room));
   cudaStream_t cs = static_cast<cudaStream_t>(stream);
   double* W = s;
   double* w = s + w_off;
   double* Jp = s + jp_off;
-  rijk::launch_j_weights(g, d_dm, spin_channel, dm_mode, W, cs);
+  rijk::launch_j_weights(g, d_dm, spin_channel, dm_mode, W, nullptr, cs);
+  if (cudaGetLastError() != cudaSuccess) return RIJK_ERR_CUDA;
   rijk::launch_j_pass1(g, d_tensor, W, spin_channel, w, cs);
-  rijk::launch_j_pass2(g, d_tensor, w, spin_channel, 1, Jp, cs);
-  rijk::launch_j_finalize(g, Jp, spin_channel, 1, scaling_factor, 0, d_vj, cs);
+  if (cudaGetLastError() != cudaSuccess) return RIJK_ERR_CUDA;
+  rijk::launch_j_pass2(g, d_tensor, w, spin_channel, splits, Jp, cs);
+  if (cudaGetLastError() != cudaSuccess) return RIJK_ERR_CUDA;
+  rijk::launch_j_finalize(g, Jp, spin_channel, splits, scaling_factor, 0, d_vj, cs);
   if (cudaGetLastError() != cudaSuccess) return RIJK_ERR_CUDA;
   return RIJK_OK;
 }

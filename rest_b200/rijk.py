@@ -107,6 +107,15 @@ class RIJK:
         """Freeze the context's device memory (for CUDA graph capture of *_dev calls)."""
         self._check(lib().rijk_ctx_pin_buffers(self._h, int(bool(pinned))))
 
+    def set_wait_budget(self, nanoseconds: int = 0):
+        """Budget of every device-side wait of this context (0 = default 2 s)."""
+        self._check(lib().rijk_ctx_set_wait_budget(self._h, int(nanoseconds)))
+
+    def selftest_timeout(self):
+        """Run one bounded wait that nothing completes; raises RijkError with
+        status RIJK_ERR_TIMEOUT when the timeout path works."""
+        self._check(lib().rijk_ctx_selftest_timeout(self._h))
+
     def set_tiles(self, half_transform_cfg: int, update_cfg: int):
         self._check(lib().rijk_ctx_set_tiles(self._h, int(half_transform_cfg), int(update_cfg)))
 

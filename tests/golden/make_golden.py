@@ -88,7 +88,9 @@ def water() -> dict:
 
 
 def main():
-    rest = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <REST checkout>")
+    rest = Path(sys.argv[1])
     (HERE / "pen_rihf.json").write_text(json.dumps(pen(rest), indent=1))
     (HERE / "water_rihf.json").write_text(json.dumps(water(), indent=1))
     print("wrote", HERE / "pen_rihf.json", HERE / "water_rihf.json")

@@ -379,3 +379,57 @@ def test_vk_occupied_form_over_many_aux_chunks(monkeypatch):
                 assert _maxdiff(got[s], ref[s]) <= TOL
     finally:
         c.close()
+
+
+def _k_occ_from_rimatr(rimatr, n, c, occ):
+    """Oracle occupied-form K (REST vk_upper_with_ri_v_sync, scf_io/mod.rs:2758-2834)
+    straight from rimatr, one aux row at a time: X = B_P C, K += X occ X^T."""
+    ii, jj = O.upper_pairs(n)
+    k = np.zeros((n, n))
+    bp = np.zeros((n, n))
+    for p in range(rimatr.shape[1]):
+        bp[ii, jj] = rimatr[:, p]
+        bp[jj, ii] = rimatr[:, p]
+        x = bp @ c
+        k += (x * occ) @ x.T
+    return k[ii, jj]
+
+
+@pytest.mark.parametrize("scratch", [None, 50 << 20])
+def test_benched_shape_n1200_aux_slab_against_oracle(monkeypatch, scratch):
+    """The benchmark's shape (n=1200, nocc=200) element-wise against the oracle.
+
+    The first 96 aux rows of the n=1200, N=4800 sweep tensor (the same NumPy
+    draw as the full tensor's rows) are loaded as rimatr.  At n=1200 the last
+    row block of every B_P holds 48 of 64 rows and at nocc=200 the last column
+    block of the half-transform holds 8 of 64 orbitals, so the straddling
+    warp tiles of the DMMA mainloop run on every aux row.  With a 50 MiB
+    scratch budget the 96 rows split into chunks of 25 (4 chunks, the last one
+    ragged).  RHF J (a2) and K (a3), and UHF K with a second spin of 150
+    orbitals, must equal the oracle within 1e-10 per element."""
+    from rest_b200 import RIJK
+
+    if scratch is not None:
+        monkeypatch.setenv("RIJK_SCRATCH_BYTES", str(scratch))
+    n, naux, nocc = 1200, 4800, 200
+    case = host_case(n, naux, nocc, seed=2024, rows=(0, 96))
+    assert case.rimatr.shape == (n * (n + 1) // 2, 96)
+    rng = np.random.default_rng(12)
+    c2 = np.asfortranarray(np.linalg.qr(rng.standard_normal((n, 150)))[0])
+    c = RIJK(0)
+    try:
+        c.set_rimatr(case.rimatr, n)
+        j = c.vj_upper_with_rimatr_v([case.dm], 1, 1.0)[0]
+        assert _maxdiff(j, O.vj_upper_with_rimatr_v(case.rimatr, [case.dm], 1, 1.0)[0]) <= TOL
+        occ1 = np.full(nocc, 2.0)
+        k = c.vk_upper_with_ri_v([case.c_occ], [nocc - 1], [occ1], 1, -0.5)[0]
+        k_ref = _k_occ_from_rimatr(case.rimatr, n, case.c_occ, occ1)
+        assert _maxdiff(k, -0.5 * k_ref) <= TOL
+        e2 = np.zeros((n, nocc), order="F")
+        e2[:, :150] = c2
+        occ2 = np.r_[np.ones(150), np.zeros(nocc - 150)]
+        ku = c.vk_upper_with_ri_v([case.c_occ, e2], [nocc - 1, 149], [0.5 * occ1, occ2], 2, -1.0)
+        assert _maxdiff(ku[0], -0.5 * k_ref) <= TOL
+        assert _maxdiff(ku[1], -_k_occ_from_rimatr(case.rimatr, n, c2, np.ones(150))) <= TOL
+    finally:
+        c.close()

@@ -59,13 +59,43 @@ def test_noalloc_matches_allocating_entry_point(ctx, n, naux, spin, mode):
         assert float((out - ref).abs().max()) <= TOL
 
 
-def test_noalloc_rejects_sizes_beyond_its_scratch(ctx):
+def test_noalloc_calls_allocate_no_device_memory(ctx):
+    """The property the entry point exists for: after the first call (which
+    only looks up the array's address), ten more calls leave the device's free
+    memory exactly where it was."""
     import torch
 
+    n, naux = 200, 800
+    case = host_case(n, naux, 33, seed=5)
+    ctx.set_rimatr(case.rimatr, n)
     d_tensor, ld = ctx.tensor_ptr()
+    dm = torch.tensor(case.dm.T.ravel(), dtype=torch.float64, device="cuda")
+    out = torch.empty(n * (n + 1) // 2, dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    assert _noalloc(d_tensor, ld, n, naux, dm.data_ptr(), 1, 1.0, 1, out.data_ptr(), st) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(10):
+        assert _noalloc(d_tensor, ld, n, naux, dm.data_ptr(), 1, 1.0, 1, out.data_ptr(), st) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
+def _tile_stride(n):
+    nt = -(-n // 32)
+    return nt * (nt + 1) // 2 * 1024
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    """Size and stride checks return before any launch, so any non-null
+    device pointer serves here (no tensor needs to be loaded)."""
+    import torch
+
     x = torch.zeros(8, dtype=torch.float64, device="cuda")
+    d_tensor, ld = x.data_ptr(), _tile_stride(37)
     # n = 2017 at N = 4n needs more than the 32 MiB array (checked before any launch)
-    assert _noalloc(d_tensor, ld, 2017, 4 * 2017, x.data_ptr(), 1, 1.0, 1, x.data_ptr(), 0) == 8
-    assert _noalloc(d_tensor, ld, 1409, 4 * 1409, x.data_ptr(), 2, 1.0, 1, x.data_ptr(), 0) == 8
+    assert _noalloc(d_tensor, _tile_stride(2017), 2017, 4 * 2017, x.data_ptr(), 1, 1.0, 1, x.data_ptr(), 0) == 8
+    assert _noalloc(d_tensor, _tile_stride(1409), 1409, 4 * 1409, x.data_ptr(), 2, 1.0, 1, x.data_ptr(), 0) == 8
     # a row stride that does not match the tile-packed layout of the given sizes
     assert _noalloc(d_tensor, ld + 1024, 37, 150, x.data_ptr(), 1, 1.0, 1, x.data_ptr(), 0) == 1
