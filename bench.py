@@ -508,6 +508,8 @@ def measure_alkanes(device: int, sizes=(10, 20, 40)) -> list:
     from rest_b200.scf_batch import BatchedRHF
 
     crit = dict(acc_etot=1e-8, acc_rho=1e-6, acc_eev=1e-6, max_cycle=100)
+    golden = json.load(open(os.path.join(ROOT, "tests", "golden", "oracle_energies.json")))
+    oracle = {a["carbons"]: a["energy"] for a in golden["alkanes"]}
     out = []
     for nc in sizes:
         mol = alkane(nc)
@@ -526,6 +528,9 @@ def measure_alkanes(device: int, sizes=(10, 20, 40)) -> list:
                          "scf_s": r.scf_s, "setup_s": r.setup_s, "fp64_k_builds": r.timings["fp64_k_builds"][0],
                          "split_k_builds": r.timings["split_k_builds"][0]}
         rec["mixed_minus_fp64_energy"] = rec["mixed"]["energy"] - rec["fp64"]["energy"]
+        if nc in oracle:  # FP64 CPU oracle energy (1e-10 Eh, committed fixture)
+            rec["fp64_minus_oracle_energy"] = rec["fp64"]["energy"] - oracle[nc]
+            rec["mixed_minus_oracle_energy"] = rec["mixed"]["energy"] - oracle[nc]
         rec["scf_speedup_mixed_vs_fp64"] = rec["fp64"]["scf_s"] / rec["mixed"]["scf_s"]
         out.append(rec)
     return out
@@ -540,15 +545,19 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
 
     from rest_b200 import RIJK
     from rest_b200.basis import int1e
-    from rest_b200.geometry import water_cluster
+    from rest_b200.geometry import water_cluster, water_cluster_set_spec
     from rest_b200.guess import LearnedGuess
     from rest_b200.scf import SCF, ScfOptions
     from rest_b200.scf_batch import run_molecule_set
 
     crit = dict(acc_etot=1e-8, acc_rho=1e-6, acc_eev=1e-6, max_cycle=100)
-    rng = np.random.default_rng(2024)
-    ks = rng.integers(1, 17, nmol)
-    mols = [water_cluster(int(k), seed=50000 + i) for i, k in enumerate(ks)]
+    spec = water_cluster_set_spec(nmol, seed=2024)
+    mols = [water_cluster(k, s) for k, s in spec]
+    # FP64 oracle energies of a fixed subset of the set (converged on the CPU
+    # oracle to 1e-10 Eh once, committed as a fixture; nothing runs the oracle here)
+    golden = json.load(open(os.path.join(ROOT, "tests", "golden", "oracle_energies.json")))
+    oracle_sub = {e["index"]: e["energy"] for e in golden["water_set"]["entries"]
+                  if e["index"] < nmol and tuple(spec[e["index"]]) == (e["k"], e["seed"])}
     run_molecule_set(mols[:4], "def2-SVP", "def2-SVP-JKFIT", group_size=4, precision="mixed", device=device, **crit)
     # the guess model is loaded (weights read and uploaded, kernels loaded) once,
     # outside the timed runs, as a model is before serving; its time is reported
@@ -572,6 +581,10 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
         res[tag] = {"molecules_per_s": nmol / wall, "wall_s": wall, "setup_s": r.setup_s, "scf_s": r.scf_s,
                     "iterations_mean": float(np.mean(r.iterations)), "converged": int(sum(r.converged)),
                     "guess_s": extra, "eigensolves": r.timings["eigensolves"],
+                    "fp64_k_builds": int(sum(r.timings["fp64_k_builds"])),
+                    "split_k_builds": int(sum(r.timings["split_k_builds"])),
+                    "max_abs_energy_error_vs_oracle": float(max(abs(r.energies[i] - e) for i, e in oracle_sub.items()))
+                    if oracle_sub else None,
                     "setup_parts_s": r.timings["setup_parts"]}
         return r
 
@@ -617,6 +630,10 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
         res[tag]["speedup_vs_plain_fp64"] = res[tag]["molecules_per_s"] / plain
     res["set"] = f"{nmol} water clusters (H2O)_k, k uniform in 1..16 (seeded), def2-SVP / def2-SVP-JKFIT, " \
                  f"RHF to 1e-8 Eh, groups of {group}, device Cholesky metric"
+    res["oracle_subset"] = (f"clusters {sorted(oracle_sub)} (k = {[spec[i][0] for i in sorted(oracle_sub)]}): "
+                            "FP64 CPU oracle energies converged to 1e-10 Eh, tests/golden/oracle_energies.json")
+    res["split_k_builds_note"] = ("the mixed arms run split-precision K only for molecules of at least "
+                                  "split_min_basis basis functions; clusters below it take FP64 builds")
     return res
 
 
@@ -687,7 +704,7 @@ def main():
     ap.add_argument("--no-scf", action="store_true", help="skip the water SCF timing")
     ap.add_argument("--no-apps", action="store_true",
                     help="skip the application configs (device tensor build, alkanes, molecule set)")
-    ap.add_argument("--set-size", type=int, default=64, help="molecules in the batched water-cluster set")
+    ap.add_argument("--set-size", type=int, default=512, help="molecules in the batched water-cluster set")
     ap.add_argument("--molecule-set-only", type=int, default=0, metavar="NMOL",
                     help="measure only the molecule-set config with NMOL molecules and print its JSON")
     ap.add_argument("--device", type=int, default=0, help="device of --molecule-set-only")

@@ -37,6 +37,17 @@ def water_cluster(k: int, seed: int) -> Molecule:
     return Molecule.from_angstrom(symbols, np.array(coords))
 
 
+def water_cluster_set_spec(nmol: int, seed: int = 2024, kmax: int = 16) -> list:
+    """(k, seed) of each cluster of the seeded molecule set: k uniform in
+    1..kmax drawn from ``seed``, cluster i placed with seed 50000 + i."""
+    ks = np.random.default_rng(seed).integers(1, kmax + 1, nmol)
+    return [(int(k), 50000 + i) for i, k in enumerate(ks)]
+
+
+def water_cluster_set(nmol: int, seed: int = 2024, kmax: int = 16) -> list:
+    return [water_cluster(k, s) for k, s in water_cluster_set_spec(nmol, seed, kmax)]
+
+
 def alkane_coords(nc: int, cc: float = 1.54, ch: float = 1.09):
     """(symbols, coords in A) of all-trans C_nH_{2n+2}.
 
