@@ -25,7 +25,7 @@ from ._abi import RijkError, lib
 
 ANG = 0.5291772083  # Bohr radius in Angstrom used by REST (src/constants/mod.rs:85)
 DATA = Path(__file__).resolve().parent / "basis_data"
-Z_OF = {"H": 1, "He": 2, "Li": 3, "Be": 4, "B": 5, "C": 6, "N": 7, "O": 8, "F": 9, "Ne": 10}
+Z_OF = {"H": 1, "He": 2, "Li": 3, "Be": 4, "B": 5, "C": 6, "N": 7, "O": 8, "F": 9, "Ne": 10, "Cu": 29}
 LMAX = 6
 
 

@@ -1,5 +1,5 @@
 """Extract the basis sets the configs use from REST's basis-set-pool into one
-compact JSON per basis (elements H, C, N, O; exponents, coefficients, l).
+compact JSON per basis (elements H, C, N, O, Cu; exponents, coefficients, l).
 
 The pool is Basis Set Exchange data shipped with REST
 (basis-set-pool/<name>/<El>.json); this script is how the committed files in
@@ -12,7 +12,7 @@ import sys
 from pathlib import Path
 
 SETS = ["STO-3G", "def2-SVP", "def2-SVP-JKFIT", "def2-SV(P)-JKFIT"]
-ELEMENTS = ["H", "C", "N", "O"]
+ELEMENTS = ["H", "C", "N", "O", "Cu"]
 
 
 def main(pool: str) -> None:

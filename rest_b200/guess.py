@@ -456,6 +456,22 @@ class LearnedGuess:
         y = self.net.forward(x).cpu().numpy().astype(np.float64)
         return self.norm.blocks(y, ps.kind)
 
+    def write_rest_init_guess(self, mol, path, ovlp: np.ndarray | None = None) -> bool:
+        """Hands the predicted density to REST's own guess path: writes the
+        ``init_guess`` HDF5 file REST reads with ``external_init_guess = true``
+        and ``guessfile_type = "hdf5"`` (src/initial_guess/mod.rs:17-26, :71-83),
+        in REST's AO order.  Returns False (and writes nothing) when the
+        prediction fails its electron-count check, so that REST keeps its own
+        guess."""
+        from .chkfile import write_init_guess
+
+        d = self.density(mol, ovlp=ovlp)
+        if d is None:
+            return False
+        # REST's closed-shell density is the total density (occupation 2), as here
+        write_init_guess(path, [d], shells=mol.shells(self.basis))
+        return True
+
     def density(self, mol, ovlp: np.ndarray | None = None, tol: float = 0.05):
         sh = mol.shells(self.basis)
         ps = pair_features(mol)

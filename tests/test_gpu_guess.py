@@ -151,3 +151,24 @@ def test_committed_guess_cuts_scf_iterations_on_held_out_clusters():
     assert all(ref.converged) and all(lrn.converged)
     assert np.mean(lrn.iterations) < np.mean(ref.iterations)
     assert np.max(np.abs(np.array(lrn.energies) - np.array(ref.energies))) < 1e-6
+
+
+def test_learned_density_handed_to_rest_as_init_guess(tmp_path):
+    """The learned density written as REST's init_guess file (REST's AO order)
+    reads back as the same density and holds the cluster's electrons."""
+    from rest_b200.basis import int1e
+    from rest_b200.chkfile import H5Reader, read_init_guess, rest_ao_order
+
+    guess = LearnedGuess.load()
+    mol = water_cluster(5, seed=77)
+    sh = mol.shells(guess.basis)
+    s = int1e(mol, sh, "ovlp")
+    path = tmp_path / "init_guess.chk"
+    assert guess.write_rest_init_guess(mol, path, ovlp=s)
+    d = guess.density(mol, ovlp=s)
+    back = read_init_guess(path, sh.nfun, 1, shells=sh)[0]
+    assert np.array_equal(back, d)
+    raw = H5Reader.open(path).dataset("init_guess")
+    perm = rest_ao_order(sh)
+    assert np.array_equal(raw.T, d[np.ix_(perm, perm)])  # column-major, REST's AO order
+    assert abs(float(np.sum(back * s)) - mol.nelec) < 1e-8
