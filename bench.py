@@ -573,7 +573,7 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
         extra = 0.0
         if kw.pop("learned", False):
             t1 = time.perf_counter()
-            dens = [guess.density(m, ovlp=int1e(m, m.shells("def2-SVP"), "ovlp")) for m in mols]
+            dens = [guess.density(m, ovlp=int1e(m, m.shells("def2-SVP"), "ovlp"), on_device=True) for m in mols]
             extra = time.perf_counter() - t1
             kw["initial_densities"] = dens
         r = run_molecule_set(mols, "def2-SVP", "def2-SVP-JKFIT", group_size=group, device=device, **kw, **crit)

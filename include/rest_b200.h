@@ -93,6 +93,7 @@ enum rijk_prof_class {
  * override the defaults at context creation. */
 #define RIJK_TILE_CFGS 6
 int rijk_ctx_set_tiles(rijk_ctx* ctx, int half_transform_cfg, int update_cfg);
+int rijk_ctx_get_tiles(const rijk_ctx* ctx, int* half_transform_cfg, int* update_cfg);
 /* Autotuner: times every CTA shape of the half-transform and of the rank
  * update on sample_rows aux rows (<= 0: 512) of the loaded tensor with ncols
  * occupied columns, keeps the fastest of each and returns them; ms (if
@@ -217,6 +218,47 @@ int rijk_vk_upper_occ_split_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num
 int rijk_vk_upper_lowrank_split_dev(rijk_ctx* ctx, const double* d_V, int64_t ld_v, int64_t ncols, int64_t npos,
                                     double scaling_factor, int accumulate, double* d_vk, void* stream);
 
+/* ---- grouped build over a molecule set ----------------------------------------- */
+/* No single counterpart in REST: REST builds J and K one SCF at a time
+ * (vj_upper_with_rimatr_v_sync + vk_upper_with_ri_v_sync, src/scf_io/mod.rs:
+ * 2490-2561, 2758-2834); a group runs that build for many molecules (one
+ * context each, tensors loaded) in six launches for all of them, the two
+ * tensor-core phases as persistent kernels over work items (molecule, aux row,
+ * tile).  nocc[m]: doubly occupied orbitals of molecule m.  The CTA shapes are
+ * 0, 1 or 4 of rijk_ctx_set_tiles (the caller's autotuner picks them).  The
+ * group owns the scratch of all molecules (one allocation at creation); its
+ * contexts must stay loaded and unchanged while it exists. */
+typedef struct rijk_group rijk_group;
+int rijk_group_create(rijk_ctx* const* ctxs, int count, const int64_t* nocc, int half_transform_cfg, int update_cfg,
+                      rijk_group** out);
+int rijk_group_destroy(rijk_group* group);
+/* For every molecule m with d_active[m] != 0 (device int array):
+ *   out_m = J(D_m) + k_scale K(C_m),  D_m = 2 C_m C_m^T over the nocc[m] columns,
+ * written full and symmetric (n_m x n_m) at d_out + m out_mol with row stride ldo;
+ * C_m(mu, i) = d_C[m c_mol + mu c_row + i c_col].  J is REST's rimatr J (a2),
+ * K the occupied-orbital K (a3, occupation 2; k_scale = -0.5 for RHF).
+ * Enqueued on `stream` without synchronising: the pointers may be captured in a
+ * CUDA graph and the active flags changed between replays. */
+int rijk_group_jk_occ_dev(rijk_group* group, const double* d_C, int64_t c_mol, int64_t c_row, int64_t c_col,
+                          double k_scale, const int* d_active, double* d_out, int64_t out_mol, int64_t ldo,
+                          void* stream);
+/* Wait for `stream` and report a device-side timeout of the group's kernels. */
+int rijk_group_synchronize(rijk_group* group, void* stream);
+
+/* ---- batched symmetric eigensolver (FP64) ------------------------------------- */
+/* The Fock diagonalisation of REST's SCF (diagonalize_hamiltonian,
+ * src/scf_io/mod.rs:1843-1873, LAPACK dspgvx) for a batch of matrices already in
+ * standard form (the batched driver forms X^T F X on the device).  d_a: batch
+ * row-major ld x ld symmetric matrices (overwritten); matrix b uses its leading
+ * d_nvalid[b] rows and columns (device int32).  Outputs: d_w (batch x ld)
+ * eigenvalues ascending, then pad_value for the padding; d_v (batch x ld x ld,
+ * row-major) eigenvectors as columns, unit vectors for the padding; d_work:
+ * batch x ld x ld doubles; d_info[b] = 1 where an eigenvalue did not converge in
+ * 30 QL sweeps (0 otherwise).  ld <= 768, else RIJK_ERR_TOO_LARGE.  One CTA per
+ * matrix: Householder tridiagonalisation, explicit Q, implicit-shift QL. */
+int rijk_eigh_batched_dev(double* d_a, int64_t ld, const int32_t* d_nvalid, int64_t batch, double pad_value,
+                          double* d_w, double* d_v, double* d_work, int32_t* d_info, void* stream);
+
 /* ---- J without any device allocation ----------------------------------------- */
 /* No counterpart in REST.  Same result as rijk_vj_upper_dev for callers that
  * cannot let a library call cudaMalloc (their device memory is owned by another
@@ -313,6 +355,18 @@ int rijk_mlp_masked_mse(const float* y, const float* t, const float* mask, int64
 int rijk_mlp_adam(float* w, uint16_t* w_bf16, const float* g, float* m, float* v, int64_t count, double lr,
                   double beta1, double beta2, double eps, int64_t step, void* stream);
 int rijk_mlp_to_bf16(const float* src, uint16_t* dst, int64_t count, void* stream);
+/* Density assembly of the learned guess (no counterpart in REST).  y: the
+ * network output, npairs_ordered x 196 FP32 (standardised 14 x 14 local blocks,
+ * row-major); t_mean, t_std: 4 x 196 (per element-pair kind = 2 type(A) +
+ * type(B)); upairs: 4 int32 per unordered atom pair A <= B within the cutoff
+ * (A, B, row of (A, B) in y, row of (B, A) in y); per atom its first AO, element
+ * type (0, 1), AO count (<= 14) and water index; rot: per water and element the
+ * 14 x 14 rotation G of that element's AO block into the water's frame.  Writes
+ * dm (num_basis^2, device): D_AB = 1/2 (G_A P_AB G_B^T |frame of A's water +
+ * G_A P_BA^T G_B^T |frame of B's water), D_BA = D_AB^T, zero beyond the cutoff. */
+int rijk_guess_assemble(const float* y, const float* t_mean, const float* t_std, const int32_t* upairs,
+                        int64_t npairs, const int32_t* atom_first, const int32_t* atom_type, const int32_t* atom_nfun,
+                        const int32_t* atom_water, const double* rot, int64_t num_basis, double* dm, void* stream);
 
 /* ---- MO-basis three-centre tensor -------------------------------------------- */
 /* generate_ri3mo_rayon / ao2mo_rayon (src/scf_io/mod.rs:2331-2359, :3270-3307):

@@ -68,8 +68,16 @@ SIGNATURES = {
     "rijk_kernel_launches": (C.c_int64, []),
     "rijk_ctx_profile": (C.c_int, [_ctxp, C.c_int]),
     "rijk_ctx_set_tiles": (C.c_int, [_ctxp, C.c_int, C.c_int]),
+    "rijk_ctx_get_tiles": (C.c_int, [_ctxp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "rijk_ctx_pin_buffers": (C.c_int, [_ctxp, C.c_int]),
     "rijk_ctx_set_wait_budget": (C.c_int, [_ctxp, C.c_int64]),
+    "rijk_group_create": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "rijk_group_destroy": (C.c_int, [C.c_void_p]),
+    "rijk_group_jk_occ_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_double,
+                                        C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p]),
+    "rijk_group_synchronize": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "rijk_eigh_batched_dev": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_double, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "rijk_ctx_selftest_timeout": (C.c_int, [_ctxp]),
     "rijk_ctx_autotune": (
         C.c_int,
@@ -153,6 +161,9 @@ SIGNATURES = {
          C.c_double, C.c_double, C.c_int64, C.c_void_p],
     ),
     "rijk_mlp_to_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
+    "rijk_guess_assemble": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                      C.c_void_p]),
 }
 
 

@@ -588,6 +588,13 @@ int rijk_ctx_selftest_timeout(rijk_ctx* ctx) {
   return sync_and_check(ctx, ctx->stream);
 }
 
+int rijk_ctx_get_tiles(const rijk_ctx* ctx, int* half_transform_cfg, int* update_cfg) {
+  if (!ctx || !half_transform_cfg || !update_cfg) return RIJK_ERR_ARG;
+  *half_transform_cfg = ctx->ht_cfg;
+  *update_cfg = ctx->rk_cfg;
+  return RIJK_OK;
+}
+
 int rijk_ctx_set_tiles(rijk_ctx* ctx, int half_transform_cfg, int update_cfg) {
   if (!ctx || half_transform_cfg < 0 || half_transform_cfg >= RIJK_TILE_CFGS || update_cfg < 0 ||
       update_cfg >= RIJK_TILE_CFGS)
@@ -1180,6 +1187,170 @@ int rijk_ao2mo(rijk_ctx* ctx, const double* eigv, int64_t num_state, int64_t row
     }
   }
   return sync_and_check(ctx, st);
+}
+
+// ---- grouped build over a molecule set -------------------------------------------
+}  // extern "C"
+
+struct rijk_group {
+  int device = 0;
+  int count = 0;
+  rijk::GroupPlan plan{};
+  void* mem = nullptr;  // descriptors, prefix sums, error words and every molecule's scratch
+  int* d_err = nullptr;
+  int sms = 148;
+  std::string last;
+};
+
+extern "C" {
+
+int rijk_group_create(rijk_ctx* const* ctxs, int count, const int64_t* nocc, int half_transform_cfg, int update_cfg,
+                      rijk_group** out) {
+  if (!ctxs || !nocc || !out || count <= 0) return RIJK_ERR_ARG;
+  *out = nullptr;
+  if (half_transform_cfg != 0 && half_transform_cfg != 1 && half_transform_cfg != 4) return RIJK_ERR_ARG;
+  if (update_cfg != 0 && update_cfg != 1 && update_cfg != 4) return RIJK_ERR_ARG;
+  const int device = ctxs[0] ? ctxs[0]->device : -1;
+  for (int m = 0; m < count; ++m) {
+    if (!ctxs[m] || !ctxs[m]->have || ctxs[m]->device != device) return RIJK_ERR_ARG;
+    if (nocc[m] <= 0 || nocc[m] > ctxs[m]->g.n) return RIJK_ERR_ARG;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) return RIJK_ERR_CUDA;
+  const int BM = rijk::group_cta_rows(half_transform_cfg), BN = rijk::group_cta_cols(half_transform_cfg);
+  const int subs = rijk::group_rank_subs(update_cfg);
+  std::vector<rijk::GroupMol> mols(count);
+  std::vector<int64_t> pre[6];
+  int64_t tot[6] = {0, 0, 0, 0, 0, 0};
+  // byte layout: descriptors | 6 prefix arrays | error words | per-molecule scratch
+  size_t off = round_up((int64_t)count * sizeof(rijk::GroupMol), 256);
+  const size_t pre_off = off;
+  off += round_up(6 * (int64_t)count * 8, 256);
+  const size_t err_off = off;
+  off += 256;
+  std::vector<size_t> mol_off(count);
+  for (int m = 0; m < count; ++m) {
+    const Geom& g = ctxs[m]->g;
+    rijk::GroupMol& d = mols[m];
+    d.B = ctxs[m]->dB;
+    d.ldB = g.ldB;
+    d.n = (int)g.n;
+    d.nt = (int)g.nt;
+    d.naux = (int)g.naux;
+    d.nocc = (int)nocc[m];
+    d.ldx = round_up(g.n, 128);
+    d.ocols = (int)round_up(nocc[m], std::max(BN, 64));
+    d.jsplits = (int)std::max<int64_t>(1, std::min<int64_t>(8, g.naux / 256));
+    d.ksplits = (int)std::max<int64_t>(1, std::min<int64_t>(16, cdiv(g.naux * nocc[m], 32768)));
+    d.nkb = cdiv(g.n, 128);
+    d.pairs = d.nkb * (d.nkb + 1) / 2;
+    d.npair = g.npair;
+    const int64_t counts[6] = {d.ldx * d.ocols + g.ldB, g.naux, g.naux * (d.ldx / BM) * (d.ocols / BN),
+                               (int64_t)d.ksplits * d.pairs * subs, (int64_t)d.jsplits * cdiv(g.ldB / 2, 256),
+                               g.npair};
+    for (int ph = 0; ph < 6; ++ph) {
+      pre[ph].push_back(tot[ph]);
+      tot[ph] += counts[ph];
+    }
+    mol_off[m] = off;
+    off += round_up(d.ldx * d.ocols * 8, 256) + round_up(g.ldB * 8, 256) + round_up(g.naux * 8, 256) +
+           round_up((int64_t)d.jsplits * g.ldB * 8, 256) + round_up((g.naux * nocc[m] + rijk::TS) * d.ldx * 8, 256) +
+           round_up((int64_t)d.ksplits * d.pairs * 128 * 128 * 8, 256);
+  }
+  void* mem = nullptr;
+  if (cudaMalloc(&mem, off) != cudaSuccess) {
+    cudaGetLastError();
+    return RIJK_ERR_NOMEM;
+  }
+  char* base = static_cast<char*>(mem);
+  for (int m = 0; m < count; ++m) {
+    rijk::GroupMol& d = mols[m];
+    const Geom& g = ctxs[m]->g;
+    char* q = base + mol_off[m];
+    auto take = [&](int64_t bytes) {
+      char* r = q;
+      q += round_up(bytes, 256);
+      return reinterpret_cast<double*>(r);
+    };
+    d.Cw = take(d.ldx * d.ocols * 8);
+    d.W = take(g.ldB * 8);
+    d.w = take(g.naux * 8);
+    d.Jpart = take((int64_t)d.jsplits * g.ldB * 8);
+    d.X = take((g.naux * d.nocc + rijk::TS) * d.ldx * 8);
+    d.Kpart = take((int64_t)d.ksplits * d.pairs * 128 * 128 * 8);
+  }
+  std::vector<int64_t> pre_flat;
+  for (int ph = 0; ph < 6; ++ph) pre_flat.insert(pre_flat.end(), pre[ph].begin(), pre[ph].end());
+  bool ok = cudaMemcpy(base, mols.data(), count * sizeof(rijk::GroupMol), cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(base + pre_off, pre_flat.data(), pre_flat.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemset(base + err_off, 0, 256) == cudaSuccess;
+  // X's spare columns are read (masked) by the rank update's last k tile
+  for (int m = 0; ok && m < count; ++m)
+    ok = cudaMemset(mols[m].X, 0, (size_t)(mols[m].naux * (int64_t)mols[m].nocc + rijk::TS) * mols[m].ldx * 8) ==
+         cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    cudaFree(mem);
+    return RIJK_ERR_CUDA;
+  }
+  rijk_group* gr = new rijk_group();
+  gr->device = device;
+  gr->count = count;
+  gr->mem = mem;
+  gr->d_err = reinterpret_cast<int*>(base + err_off);
+  gr->plan.mols = reinterpret_cast<rijk::GroupMol*>(base);
+  gr->plan.count = count;
+  for (int ph = 0; ph < 6; ++ph) {
+    gr->plan.pre[ph] = reinterpret_cast<int64_t*>(base + pre_off) + (int64_t)ph * count;
+    gr->plan.total[ph] = tot[ph];
+  }
+  gr->plan.ht_cfg = half_transform_cfg;
+  gr->plan.rk_cfg = update_cfg;
+  int sms = 148;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+    cudaGetLastError();
+    sms = 148;
+  }
+  gr->sms = sms;
+  *out = gr;
+  return RIJK_OK;
+}
+
+int rijk_group_destroy(rijk_group* g) {
+  if (!g) return RIJK_OK;
+  cudaSetDevice(g->device);
+  cudaDeviceSynchronize();
+  if (g->mem) cudaFree(g->mem);
+  delete g;
+  return RIJK_OK;
+}
+
+int rijk_group_jk_occ_dev(rijk_group* g, const double* d_C, int64_t c_mol, int64_t c_row, int64_t c_col,
+                          double k_scale, const int* d_active, double* d_out, int64_t out_mol, int64_t ldo,
+                          void* stream) {
+  if (!g || !d_C || !d_active || !d_out || ldo <= 0) return RIJK_ERR_ARG;
+  if (cudaSetDevice(g->device) != cudaSuccess) return RIJK_ERR_CUDA;
+  rijk::launch_group(g->plan, d_C, c_mol, c_row, c_col, k_scale, d_out, out_mol, ldo, d_active, g->d_err, g->sms,
+                     static_cast<cudaStream_t>(stream));
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g->last = std::string("group build: ") + cudaGetErrorString(e);
+    return RIJK_ERR_CUDA;
+  }
+  return RIJK_OK;
+}
+
+int rijk_group_synchronize(rijk_group* g, void* stream) {
+  if (!g) return RIJK_ERR_ARG;
+  if (cudaSetDevice(g->device) != cudaSuccess) return RIJK_ERR_CUDA;
+  if (cudaStreamSynchronize(static_cast<cudaStream_t>(stream)) != cudaSuccess) return RIJK_ERR_CUDA;
+  int h = 0;
+  if (cudaMemcpy(&h, g->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return RIJK_ERR_CUDA;
+  if (h != 0) {
+    cudaMemset(g->d_err, 0, sizeof(int));
+    g->last = "a device-side wait exceeded its time budget";
+    return RIJK_ERR_TIMEOUT;
+  }
+  return RIJK_OK;
 }
 
 double rijk_energy_contraction(const double* a, const double* b, int64_t npair) {

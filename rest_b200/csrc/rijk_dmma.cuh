@@ -209,6 +209,40 @@ __device__ __forceinline__ bool dmma_consume(int ktiles, DmmaSmem<Cfg>& sm, doub
 }
 
 // ---------------------------------------------------------------------------
+// Remainder columns (cp.async scheme, 4-warp 64 x 64 CTAs).  When the B
+// operand's valid columns end XF * 8 or fewer columns past a multiple of 64,
+// the CTAs of the last full column block also compute those columns, so that
+// no CTA streams the A operand for a nearly empty output tile.  Per k-step the
+// 32 x (8 XF) block of B is staged into the padding words of the stage's slots
+// (element (k, n) of it at slot n / 4, column 4 (k / 4) + n % 4, word 32 + k % 4:
+// 16-byte runs of two k, and conflict-free fragment loads), and warp (wm, wn)
+// multiplies it by the A fragments of rows wm * 32 + wn * 16 .. + 15, which it
+// holds already: two extra DMMAs per k4 step and extra fragment.
+// ---------------------------------------------------------------------------
+template <int XF>
+struct ExtraCols {
+  double acc[2][XF > 0 ? XF : 1][2];  // rows (wn * 2 + e) * 8 + lane / 4 of the warp tile
+  bool on = false;                    // this CTA computes the remainder columns
+};
+
+// Per-lane offset (in doubles, inside a stage) of extra fragment j for k4 step 0.
+__device__ __forceinline__ int extra_off(int j, int lane) {
+  const int l4 = lane >> 2;
+  return (2 * j + (l4 >> 2)) * SLOT_DOUBLES + (l4 & 3) * SLD + 32 + (lane & 3);
+}
+
+template <int XF>
+__device__ __forceinline__ void extra_k4(const double* __restrict__ sbase, int kk, int lane, double a0, double a1,
+                                         bool v0, bool v1, bool kin, ExtraCols<XF>& x) {
+#pragma unroll
+  for (int j = 0; j < XF; ++j) {
+    const double b = kin ? sbase[extra_off(j, lane) + kk * 4 * SLD] : 0.0;
+    if (v0) dmma_m8n8k4(x.acc[0][j][0], x.acc[0][j][1], a0, b);
+    if (v1) dmma_m8n8k4(x.acc[1][j][0], x.acc[1][j][1], a1, b);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Second staging scheme, selected per CTA shape (Cfg::STAGES < 0 never; the
 // template flag below): every thread copies 16-byte chunks with cp.async into
 // the same padded slots, cp.async groups track the stages, one CTA barrier per
@@ -224,8 +258,9 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <class Cfg, class Sched>
-__device__ __forceinline__ void cpa_issue_stage(const Sched& sc, int kt, double* stage, uint8_t* flags) {
+template <class Cfg, int XF = 0, class Sched>
+__device__ __forceinline__ void cpa_issue_stage(const Sched& sc, int kt, double* stage, uint8_t* flags,
+                                                bool extra = false) {
   // 512 16-byte chunks per slot: chunk = column c (0..31) x row pair r2 (0..15).
   // Thread t copies chunks t + THREADS j: with THREADS a multiple of 16 they
   // share the row pair t % 16 and step THREADS / 16 columns, so one base
@@ -246,6 +281,21 @@ __device__ __forceinline__ void cpa_issue_stage(const Sched& sc, int kt, double*
 #pragma unroll
     for (int j = 0; j < NJ; ++j) cp_async16(d + j * CSTEP * SLD, g + j * gstep);
   }
+  if constexpr (XF > 0) {
+    static_assert(Cfg::THREADS == 128 && 2 * XF <= Cfg::SLOTS, "remainder staging");
+    if (extra) {
+      // 16-byte chunk id = column nn (0 .. 8 XF - 1) x row pair r2 (k = 2 r2, 2 r2 + 1)
+      const SlotSrc xs = sc.x(kt);
+#pragma unroll
+      for (int i = 0; i < XF; ++i) {
+        const int id = threadIdx.x + 128 * i;
+        const int nn = id >> 4, r2 = id & 15;
+        const double* g = xs.ptr + (int64_t)nn * xs.ld + 2 * r2;
+        double* d = stage + (nn >> 2) * SLOT_DOUBLES + (4 * (r2 >> 1) + (nn & 3)) * SLD + 32 + 2 * (r2 & 1);
+        cp_async16(d, g);
+      }
+    }
+  }
 }
 
 // One full k-tile (32 k) of a warp whose A slots (consecutive, from slot_a) all
@@ -253,10 +303,10 @@ __device__ __forceinline__ void cpa_issue_stage(const Sched& sc, int kt, double*
 // orientation TB: every fragment address is the warp's base plus an immediate.
 // PARTIAL: only fragments fm < fm_lim, fn < fn_lim are loaded and multiplied
 // (the warp's tile straddles the valid rows or columns); the k-tile is full.
-template <class Cfg, bool TA, bool TB, bool PARTIAL = false>
+template <class Cfg, bool TA, bool TB, bool PARTIAL = false, int XF = 0>
 __device__ __forceinline__ void dmma_ktile_fixed(const double* __restrict__ sbase, int slot_a, int slot_b, int lane,
                                                  double (&acc)[Cfg::FM][Cfg::FN][2], int fm_lim = Cfg::FM,
-                                                 int fn_lim = Cfg::FN) {
+                                                 int fn_lim = Cfg::FN, ExtraCols<XF>* x = nullptr, int wn = 0) {
   constexpr int AMST = TA ? SLD : 1, AKST = TA ? 1 : SLD;
   constexpr int BNST = TB ? 1 : SLD, BKST = TB ? SLD : 1;
   constexpr int APS = Cfg::WTM >= TS ? Cfg::WTM / TS : 1;
@@ -278,23 +328,39 @@ __device__ __forceinline__ void dmma_ktile_fixed(const double* __restrict__ sbas
 #pragma unroll
       for (int fn = 0; fn < Cfg::FN; ++fn)
         if (!PARTIAL || (fm < fm_lim && fn < fn_lim)) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], af[fm], bf[fn]);
+    if constexpr (XF > 0) {
+      if (x->on) {
+        const double a0 = wn ? af[2] : af[0], a1 = wn ? af[3] : af[1];
+        extra_k4<XF>(sbase, kk, lane, a0, a1, !PARTIAL || 2 * wn < fm_lim, !PARTIAL || 2 * wn + 1 < fm_lim, true,
+                     *x);
+      }
+    }
   }
 }
 
-template <class Cfg, class Sched, class KValid>
+template <class Cfg, int XF = 0, class Sched, class KValid>
 __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktiles, void* smem_base,
                                                       double (&acc)[Cfg::FM][Cfg::FN][2], int mvalid, int nvalid,
-                                                      const KValid& kvalid) {
+                                                      const KValid& kvalid, ExtraCols<XF>* x = nullptr) {
   DmmaSmem<Cfg> sm(smem_base);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int i = 0; i < Cfg::FM; ++i)
 #pragma unroll
     for (int j = 0; j < Cfg::FN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  bool xon = false;
+  if constexpr (XF > 0) {
+    xon = x->on;
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+      for (int j = 0; j < XF; ++j) x->acc[e][j][0] = x->acc[e][j][1] = 0.0;
+  }
   constexpr int S = Cfg::STAGES;
 #pragma unroll
   for (int s = 0; s < S - 1; ++s) {
-    if (s < ktiles) cpa_issue_stage<Cfg>(sc, s, sm.slots + s * Cfg::STAGE_DOUBLES, sm.flags + s * Cfg::SLOTS);
+    if (s < ktiles)
+      cpa_issue_stage<Cfg, XF>(sc, s, sm.slots + s * Cfg::STAGE_DOUBLES, sm.flags + s * Cfg::SLOTS, xon);
     cp_async_commit();
   }
   const bool compute = warp < Cfg::CWARPS;
@@ -312,7 +378,8 @@ __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktile
     {
       const int nk = kt + S - 1;
       const int ns = nk % S;
-      if (nk < ktiles) cpa_issue_stage<Cfg>(sc, nk, sm.slots + ns * Cfg::STAGE_DOUBLES, sm.flags + ns * Cfg::SLOTS);
+      if (nk < ktiles)
+        cpa_issue_stage<Cfg, XF>(sc, nk, sm.slots + ns * Cfg::STAGE_DOUBLES, sm.flags + ns * Cfg::SLOTS, xon);
       cp_async_commit();
     }
     if (idle) continue;
@@ -331,15 +398,16 @@ __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktile
       for (int j = 1; j < APS; ++j) uniform = uniform && ((fl[sa + j] != 0) == ta);
 #pragma unroll
       for (int j = 1; j < BPS; ++j) uniform = uniform && ((fl[Cfg::MT + sbs + j] != 0) == tb);
+      const int wn = warp % Cfg::WN;
       if (full && uniform) {
         if (!ta && !tb)
-          dmma_ktile_fixed<Cfg, false, false>(sbase, sa, sbs, lane, acc);
+          dmma_ktile_fixed<Cfg, false, false, false, XF>(sbase, sa, sbs, lane, acc, Cfg::FM, Cfg::FN, x, wn);
         else if (ta && !tb)
-          dmma_ktile_fixed<Cfg, true, false>(sbase, sa, sbs, lane, acc);
+          dmma_ktile_fixed<Cfg, true, false, false, XF>(sbase, sa, sbs, lane, acc, Cfg::FM, Cfg::FN, x, wn);
         else if (!ta && tb)
-          dmma_ktile_fixed<Cfg, false, true>(sbase, sa, sbs, lane, acc);
+          dmma_ktile_fixed<Cfg, false, true, false, XF>(sbase, sa, sbs, lane, acc, Cfg::FM, Cfg::FN, x, wn);
         else
-          dmma_ktile_fixed<Cfg, true, true>(sbase, sa, sbs, lane, acc);
+          dmma_ktile_fixed<Cfg, true, true, false, XF>(sbase, sa, sbs, lane, acc, Cfg::FM, Cfg::FN, x, wn);
         continue;
       }
       if constexpr (Cfg::THREADS == 128 && Cfg::FM * Cfg::FN == 16 && 3 * Cfg::SMEM_BYTES <= 227 * 1024) {
@@ -347,13 +415,13 @@ __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktile
           // full k-tile, warp tile straddling the valid rows or columns (the
           // 4-warp 64x64 shapes only: the variant costs registers)
           if (!ta && !tb)
-            dmma_ktile_fixed<Cfg, false, false, true>(sbase, sa, sbs, lane, acc, fm_lim, fn_lim);
+            dmma_ktile_fixed<Cfg, false, false, true, XF>(sbase, sa, sbs, lane, acc, fm_lim, fn_lim, x, wn);
           else if (ta && !tb)
-            dmma_ktile_fixed<Cfg, true, false, true>(sbase, sa, sbs, lane, acc, fm_lim, fn_lim);
+            dmma_ktile_fixed<Cfg, true, false, true, XF>(sbase, sa, sbs, lane, acc, fm_lim, fn_lim, x, wn);
           else if (!ta && tb)
-            dmma_ktile_fixed<Cfg, false, true, true>(sbase, sa, sbs, lane, acc, fm_lim, fn_lim);
+            dmma_ktile_fixed<Cfg, false, true, true, XF>(sbase, sa, sbs, lane, acc, fm_lim, fn_lim, x, wn);
           else
-            dmma_ktile_fixed<Cfg, true, true, true>(sbase, sa, sbs, lane, acc, fm_lim, fn_lim);
+            dmma_ktile_fixed<Cfg, true, true, true, XF>(sbase, sa, sbs, lane, acc, fm_lim, fn_lim, x, wn);
           continue;
         }
       }
@@ -396,6 +464,12 @@ __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktile
         for (int fm = 0; fm < Cfg::FM; ++fm)
 #pragma unroll
           for (int fn = 0; fn < Cfg::FN; ++fn) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], af[fm], bf[fn]);
+        if constexpr (XF > 0) {
+          if (xon) {
+            const int wn = warp % Cfg::WN;
+            extra_k4<XF>(sbase, kk, lane, wn ? af[2] : af[0], wn ? af[3] : af[1], true, true, true, *x);
+          }
+        }
       }
     } else {
       // edge tile: as in dmma_consume, k at or beyond kvalid reads as zero
@@ -418,6 +492,13 @@ __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktile
 #pragma unroll
           for (int fn = 0; fn < Cfg::FN; ++fn)
             if (fm < fm_lim && fn < fn_lim) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], af[fm], bf[fn]);
+        if constexpr (XF > 0) {
+          if (xon) {
+            const int wn = warp % Cfg::WN;
+            extra_k4<XF>(sbase, kk, lane, wn ? af[2] : af[0], wn ? af[3] : af[1], 2 * wn < fm_lim,
+                         2 * wn + 1 < fm_lim, kin, *x);
+          }
+        }
       }
     }
   }
@@ -428,13 +509,16 @@ __device__ __forceinline__ bool dmma_mainloop_cpasync(const Sched& sc, int ktile
 // Whole CTA: set up the barriers, split into producer and consumers.  Only
 // consumer threads return true (and hold results); the producer returns false.
 // Cfg::CPASYNC selects the cp.async staging above instead.
-template <class Cfg, class Sched, class KValid = DefaultKValid>
+template <class Cfg, class Sched, class KValid = DefaultKValid, int XF = 0>
 __device__ __forceinline__ bool dmma_mainloop(const Sched& sc, int ktiles, void* smem_base,
                                               double (&acc)[Cfg::FM][Cfg::FN][2], int* err, int mvalid = 1 << 30,
-                                              int nvalid = 1 << 30, const KValid& kvalid = KValid()) {
+                                              int nvalid = 1 << 30, const KValid& kvalid = KValid(),
+                                              ExtraCols<XF>* x = nullptr) {
   if constexpr (Cfg::CPASYNC) {
     (void)err;
-    return dmma_mainloop_cpasync<Cfg>(sc, ktiles, smem_base, acc, mvalid, nvalid, kvalid);
+    return dmma_mainloop_cpasync<Cfg, XF>(sc, ktiles, smem_base, acc, mvalid, nvalid, kvalid, x);
+  } else {
+    static_assert(XF == 0, "remainder columns need the cp.async scheme");
   }
   DmmaSmem<Cfg> sm(smem_base);
   const int warp = threadIdx.x >> 5;

@@ -124,6 +124,42 @@ void launch_rank_tc(const Geom& g, const TcGeom& t, const void* Xhi, const void*
 void launch_rank_tc_finalize(const Geom& g, const TcGeom& t, const float* part, int splits, double scale,
                              int accumulate, double* out, cudaStream_t st);
 
+// --- grouped build over a molecule set ---------------------------------------
+// One molecule of a group (device-resident descriptor).
+struct GroupMol {
+  const double* B;  // tile-packed tensor of the molecule's context
+  int64_t ldB;
+  int n, nt, naux, nocc;
+  double* Cw;       // sqrt(2) C, ldx x ocols, column-major
+  int64_t ldx;
+  int ocols;        // a multiple of the half-transform CTA width
+  double* W;        // J weights (ldB)
+  double* w;        // J scalars (naux)
+  double* Jpart;    // jsplits x ldB
+  int jsplits;
+  double* X;        // ldx x (naux nocc + 32)
+  double* Kpart;    // ksplits x pairs x 128 x 128
+  int ksplits;
+  int64_t nkb, pairs, npair;
+};
+// Work enumeration of the six phases: pre[phase] (device, count entries) are
+// the prefix sums of each molecule's items, total[phase] their sum.
+struct GroupPlan {
+  GroupMol* mols;
+  int count;
+  int64_t* pre[6];
+  int64_t total[6];
+  int ht_cfg, rk_cfg;
+};
+int group_cta_rows(int cfg);
+int group_cta_cols(int cfg);
+int group_rank_subs(int cfg);
+// out[m] (ldo-strided, full and symmetric) = J(2 C_m C_m^T) + k_scale K(C_m) for
+// every molecule m with active[m] != 0; molecule m's orbitals C(mu, i) at
+// C0[m c_mol + mu c_row + i c_col] (occupation 2 for i < nocc).
+void launch_group(const GroupPlan& gp, const double* C0, int64_t c_mol, int64_t c_row, int64_t c_col, double k_scale,
+                  double* out0, int64_t out_mol, int64_t ldo, const int* active, int* err, int sms, cudaStream_t st);
+
 // --- ri3mo ---------------------------------------------------------------------
 // out (ldo x ncp, zero padded) = C[:, c0 : c0 + nc]
 void launch_gather_cols(const double* C, int64_t n, int64_t ldc_in, int64_t c0, int64_t nc, int64_t ldo, int64_t ncp,

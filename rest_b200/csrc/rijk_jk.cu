@@ -416,6 +416,7 @@ struct HalfTransformSched {
   const double* W;
   int64_t ldw;
   int nt, I0, col0;
+  int xcol0;  // first remainder column (CTAs of the last full column block)
   __device__ SlotSrc a(int kt, int mt) const {
     const int I = I0 + mt, J = kt;
     if (I >= nt) return {nullptr, TS, 0};
@@ -425,6 +426,7 @@ struct HalfTransformSched {
   __device__ SlotSrc b(int kt, int ntl) const {
     return {W + (int64_t)kt * TS + (int64_t)(col0 + ntl * TS) * ldw, ldw, 0};
   }
+  __device__ SlotSrc x(int kt) const { return {W + (int64_t)kt * TS + (int64_t)xcol0 * ldw, ldw, 0}; }
 };
 
 // Only the rows of the last k tile below n can be non-zero.
@@ -435,12 +437,14 @@ struct LastTileK {
 
 // Grid: blockIdx.x = cb + ncb * (rb + nrb * p), so that the column blocks of
 // one row block run back to back and share its B tiles in L2.
-template <class Cfg>
+// XF > 0: the CTAs of the last column block (cb == ncb - 1) also compute the
+// XF * 8 remainder columns from xcol0 on (see ExtraCols).
+template <class Cfg, int XF = 0>
 __global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_half_transform(const double* __restrict__ B, int64_t ldB, int64_t p0,
                                                                  int nrb, int ncb, const double* __restrict__ W,
                                                                  int64_t ldw, int n, int nt, int ncol_valid,
                                                                  double* __restrict__ X, int64_t ldx, XMap xm,
-                                                                 int* err) {
+                                                                 int* err, int xcol0) {
   extern __shared__ __align__(128) double smem[];
   const int64_t bid = blockIdx.x;
   const int cb = (int)(bid % ncb);
@@ -448,30 +452,75 @@ __global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_half_transfor
   const int64_t pl = rest / nrb;
   const int I0 = (int)(rest % nrb) * Cfg::MT;
   const int col0 = cb * Cfg::BN;
-  HalfTransformSched sc{B + (p0 + pl) * ldB, W, ldw, nt, I0, col0};
+  HalfTransformSched sc{B + (p0 + pl) * ldB, W, ldw, nt, I0, col0, xcol0};
   double acc[Cfg::FM][Cfg::FN][2];
+  ExtraCols<XF> xc;
+  xc.on = XF > 0 && cb == ncb - 1;
   // Row blocks entirely below n hold zeros only: skip their k-loop.
   const int ktiles = I0 < nt ? nt : 0;
   const LastTileK kv{nt - 1, n - (nt - 1) * TS};
-  if (!dmma_mainloop<Cfg>(sc, ktiles, smem, acc, err, n - I0 * TS, ncol_valid - col0, kv)) return;
+  if (!dmma_mainloop<Cfg, HalfTransformSched, LastTileK, XF>(sc, ktiles, smem, acc, err, n - I0 * TS,
+                                                             ncol_valid - col0, kv, &xc))
+    return;
   double* Xr = X + (int64_t)I0 * TS;
   dmma_for_each<Cfg>(acc, [&](int m, int c, double v0, double v1) {
     const int64_t d0 = xm.dst(pl, col0 + c), d1 = xm.dst(pl, col0 + c + 1);
     if (d0 >= 0) Xr[m + d0 * ldx] = v0;
     if (d1 >= 0) Xr[m + d1 * ldx] = v1;
   });
+  if constexpr (XF > 0) {
+    if (xc.on) {
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      const int wm = warp / Cfg::WN, wn = warp % Cfg::WN;
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+#pragma unroll
+        for (int j = 0; j < XF; ++j) {
+          const int m = wm * Cfg::WTM + (wn * 2 + e) * 8 + (lane >> 2);
+          const int c = xcol0 + 8 * j + 2 * (lane & 3);
+          const int64_t d0 = c < ncol_valid ? xm.dst(pl, c) : -1, d1 = c + 1 < ncol_valid ? xm.dst(pl, c + 1) : -1;
+          if (d0 >= 0) Xr[m + d0 * ldx] = xc.acc[e][j][0];
+          if (d1 >= 0) Xr[m + d1 * ldx] = xc.acc[e][j][1];
+        }
+    }
+  }
+}
+
+template <class Cfg, int XF = 0>
+static void half_transform_launch(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W,
+                                  int64_t ldw, int ncb, int64_t ncol_valid, double* X, int64_t ldx, const XMap& xm,
+                                  int* err, int xcol0, cudaStream_t st) {
+  cudaFuncSetAttribute(k_half_transform<Cfg, XF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)Cfg::SMEM_BYTES);
+  const int nrb = (int)(ldx / Cfg::BM);
+  count_launch();
+  k_half_transform<Cfg, XF><<<(unsigned)(np * nrb * ncb), Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(
+      B, g.ldB, p0, nrb, ncb, W, ldw, (int)g.n, (int)g.nt, (int)ncol_valid, X, ldx, xm, err, xcol0);
 }
 
 template <class Cfg>
 static void half_transform_cfg(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
                                int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, const XMap& xm, int* err,
                                cudaStream_t st) {
-  cudaFuncSetAttribute(k_half_transform<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
-  const int nrb = (int)(ldx / Cfg::BM);
-  const int ncb = (int)(ncol / Cfg::BN);
-  count_launch();
-  k_half_transform<Cfg><<<(unsigned)(np * nrb * ncb), Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(
-      B, g.ldB, p0, nrb, ncb, W, ldw, (int)g.n, (int)g.nt, (int)ncol_valid, X, ldx, xm, err);
+  half_transform_launch<Cfg>(g, B, p0, np, W, ldw, (int)(ncol / Cfg::BN), ncol_valid, X, ldx, xm, err, 0, st);
+}
+
+// The default shape: when the valid columns end at most 16 past a multiple of
+// 64, the last full column block also computes those remainder columns (one or
+// two extra fragments) instead of a block of CTAs for them alone.
+template <>
+void half_transform_cfg<HtCfg1>(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W,
+                                int64_t ldw, int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx,
+                                const XMap& xm, int* err, cudaStream_t st) {
+  const int64_t full = ncol_valid / HtCfg1::BN, rem = ncol_valid - full * HtCfg1::BN;
+  const int xcol0 = (int)(full * HtCfg1::BN);
+  if (full >= 1 && rem > 0 && rem <= 8)
+    return half_transform_launch<HtCfg1, 1>(g, B, p0, np, W, ldw, (int)full, ncol_valid, X, ldx, xm, err, xcol0,
+                                            st);
+  if (full >= 1 && rem > 8 && rem <= 16)
+    return half_transform_launch<HtCfg1, 2>(g, B, p0, np, W, ldw, (int)full, ncol_valid, X, ldx, xm, err, xcol0,
+                                            st);
+  half_transform_launch<HtCfg1>(g, B, p0, np, W, ldw, (int)(ncol / HtCfg1::BN), ncol_valid, X, ldx, xm, err, 0, st);
 }
 
 void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
@@ -717,6 +766,258 @@ void launch_k_finalize(const Geom& g, const double* Kpart, int splits, int full,
   count_launch();
   k_k_finalize<<<blocks, 256, 0, st>>>(g.n, g.npair, Kpart, splits, full, nkb, pairs, scale, accumulate, out_kind,
                                        out);
+}
+
+// ============================================================================
+// Grouped build over a set of molecules (one launch per phase for all of them)
+// ============================================================================
+// A molecule set's SCFs advance together; REST's per-molecule build
+// (vk_upper_with_ri_v_sync, src/scf_io/mod.rs:2758-2834, with the J of
+// vj_upper_with_rimatr_v_sync, :2490-2561) runs here for every molecule of a
+// group at once.  Each phase enumerates work items over all molecules --
+// (molecule, element), (molecule, aux row), (molecule, aux row, row block,
+// column block), (molecule, K sub-block, split) -- and decodes the molecule
+// from per-phase prefix sums in device memory.  The two tensor-core phases are
+// persistent: a grid of SMs x resident CTAs walks the items.  Molecules whose
+// active flag is 0 are skipped, so a captured graph serves every iteration.
+
+__device__ __forceinline__ int group_find(const int64_t* __restrict__ pre, int count, int64_t w) {
+  int lo = 0, hi = count - 1;  // largest m with pre[m] <= w
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= w)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// Phase 1: Cw = sqrt(2) C (ldx x ocols, zero padded) and the J weights W from
+// D = 2 C C^T folded onto the tile layout (REST's a2 weights: off-diagonal
+// tiles 2 D, diagonal tiles D; D symmetric).
+__global__ void __launch_bounds__(256) k_grp_prepare(const GroupMol* __restrict__ mols, const int64_t* __restrict__ pre,
+                                                     int count, int64_t total, const double* __restrict__ C0,
+                                                     int64_t c_mol, int64_t c_row, int64_t c_col,
+                                                     const int* __restrict__ active) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int m = group_find(pre, count, e);
+    if (!active[m]) continue;
+    const GroupMol& g = mols[m];
+    const double* C = C0 + m * c_mol;
+    const int64_t t = e - pre[m];
+    const int64_t ncw = g.ldx * g.ocols;
+    if (t < ncw) {
+      const int64_t row = t % g.ldx, col = t / g.ldx;
+      g.Cw[t] = (row < g.n && col < g.nocc) ? 1.4142135623730951 * C[row * c_row + col * c_col] : 0.0;
+    } else {
+      const int64_t k = t - ncw;
+      const int64_t tile = k >> 10;
+      const int rc = (int)(k & 1023), r = rc & 31, c = rc >> 5;
+      const int64_t J = tri_root(tile), I = tile - J * (J + 1) / 2;
+      const int64_t mu = I * TS + r, nu = J * TS + c;
+      double v = 0.0;
+      if (mu < g.n && nu < g.n) {
+        const int64_t i = mu < nu ? mu : nu, j = mu < nu ? nu : mu;
+        for (int o = 0; o < g.nocc; ++o) v = fma(C[i * c_row + o * c_col], C[j * c_row + o * c_col], v);
+        v *= (I < J ? 4.0 : 2.0);
+      }
+      g.W[k] = v;
+    }
+  }
+}
+
+// Phase 2: w_P = B_P . W, one CTA per (molecule, aux row).
+__global__ void __launch_bounds__(256) k_grp_pass1(const GroupMol* __restrict__ mols, const int64_t* __restrict__ pre,
+                                                   int count, const int* __restrict__ active) {
+  const int m = group_find(pre, count, blockIdx.x);
+  if (!active[m]) return;
+  const GroupMol& g = mols[m];
+  const int64_t P = blockIdx.x - pre[m];
+  const double2* b = reinterpret_cast<const double2*>(g.B + P * g.ldB);
+  const double2* w0 = reinterpret_cast<const double2*>(g.W);
+  const int64_t nq = g.ldB / 2;
+  double s[1] = {0.0}, s2 = 0.0;
+  for (int64_t q = threadIdx.x; q < nq; q += 256) {
+    const double2 x = ld_stream(b + q);
+    const double2 a = __ldg(w0 + q);
+    s[0] = fma(x.x, a.x, s[0]);
+    s2 = fma(x.y, a.y, s2);
+  }
+  s[0] += s2;
+  block_reduce_store<1>(s, g.w + P, g.naux);
+}
+
+// Phase 3 (persistent): X_P = B_P Cw for every (molecule, aux row, row block, column block).
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_grp_half(const GroupMol* __restrict__ mols,
+                                                                            const int64_t* __restrict__ pre, int count,
+                                                                            int64_t total, const int* __restrict__ active,
+                                                                            int* err) {
+  extern __shared__ __align__(128) double smem[];
+  for (int64_t it = blockIdx.x; it < total; it += gridDim.x) {
+    const int m = group_find(pre, count, it);
+    if (!active[m]) continue;  // uniform over the CTA
+    const GroupMol& g = mols[m];
+    const int nrb = (int)(g.ldx / Cfg::BM), ncb = g.ocols / Cfg::BN;
+    const int64_t bid = it - pre[m];
+    const int cb = (int)(bid % ncb);
+    const int64_t rest = bid / ncb;
+    const int64_t pl = rest / nrb;
+    const int I0 = (int)(rest % nrb) * Cfg::MT;
+    const int col0 = cb * Cfg::BN;
+    HalfTransformSched sc{g.B + pl * g.ldB, g.Cw, g.ldx, g.nt, I0, col0, 0};
+    double acc[Cfg::FM][Cfg::FN][2];
+    const int ktiles = I0 < g.nt ? g.nt : 0;
+    const LastTileK kv{g.nt - 1, g.n - (g.nt - 1) * TS};
+    __syncthreads();  // the previous item's warps are done with the stages
+    if (dmma_mainloop<Cfg>(sc, ktiles, smem, acc, err, g.n - I0 * TS, g.nocc - col0, kv)) {
+      double* Xr = g.X + (int64_t)I0 * TS;
+      const int64_t nw = g.nocc;
+      dmma_for_each<Cfg>(acc, [&](int mm, int c, double v0, double v1) {
+        const int64_t c0 = col0 + c;
+        if (c0 < nw) Xr[mm + (pl * nw + c0) * g.ldx] = v0;
+        if (c0 + 1 < nw) Xr[mm + (pl * nw + c0 + 1) * g.ldx] = v1;
+      });
+    }
+  }
+}
+
+// Phase 4 (persistent): Kpart = sum_p X_p X_p^T per (molecule, upper K sub-block, split).
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_grp_rank(const GroupMol* __restrict__ mols,
+                                                                            const int64_t* __restrict__ pre, int count,
+                                                                            int64_t total, const int* __restrict__ active,
+                                                                            int* err) {
+  extern __shared__ __align__(128) double smem[];
+  constexpr int subs = (KB / Cfg::BM) * (KB / Cfg::BN);
+  for (int64_t it = blockIdx.x; it < total; it += gridDim.x) {
+    const int m = group_find(pre, count, it);
+    if (!active[m]) continue;
+    const GroupMol& g = mols[m];
+    const int64_t local = it - pre[m];
+    const int64_t nsub = g.pairs * subs;
+    const int sp = (int)(local / nsub);
+    int64_t q, row0, col0, off;
+    if (!sub_block<Cfg>(local % nsub, 0, g.nkb, q, row0, col0, off)) continue;
+    const int64_t pa = (int64_t)g.naux * sp / g.ksplits, pb = (int64_t)g.naux * (sp + 1) / g.ksplits;
+    const int64_t kcount = (pb - pa) * g.nocc;
+    RankSched sc{g.X, g.ldx, pa * g.nocc, row0, col0};
+    double acc[Cfg::FM][Cfg::FN][2];
+    const int ktiles = (int)((kcount + TS - 1) / TS);
+    const LastTileK kv{ktiles - 1, (int)(kcount - (int64_t)(ktiles - 1) * TS)};
+    __syncthreads();
+    if (dmma_mainloop<Cfg>(sc, ktiles, smem, acc, err, g.n - (int)row0, g.n - (int)col0, kv)) {
+      double* out = g.Kpart + ((int64_t)sp * g.pairs + q) * (KB * KB) + off;
+      dmma_for_each<Cfg>(acc, [&](int mm, int c, double v0, double v1) {
+        out[mm + KB * c] = v0;
+        out[mm + KB * (c + 1)] = v1;
+      });
+    }
+  }
+}
+
+// Phase 5: Jpart[split] = sum_p B[p, :] w_p per (molecule, 512-pair chunk of the row, split).
+__global__ void __launch_bounds__(256) k_grp_pass2(const GroupMol* __restrict__ mols, const int64_t* __restrict__ pre,
+                                                   int count, const int* __restrict__ active) {
+  const int m = group_find(pre, count, blockIdx.x);
+  if (!active[m]) return;
+  const GroupMol& g = mols[m];
+  const int64_t nq = g.ldB / 2;
+  const int64_t nqb = (nq + 255) / 256;
+  const int64_t local = blockIdx.x - pre[m];
+  const int sp = (int)(local / nqb);
+  const int64_t q = (local % nqb) * 256 + threadIdx.x;
+  if (q >= nq) return;
+  const int64_t p0 = (int64_t)g.naux * sp / g.jsplits, p1 = (int64_t)g.naux * (sp + 1) / g.jsplits;
+  const double2* b = reinterpret_cast<const double2*>(g.B) + q;
+  double2 a = make_double2(0.0, 0.0);
+  for (int64_t p = p0; p < p1; ++p) {
+    const double2 x = ld_stream(b + p * nq);
+    const double wp = __ldg(g.w + p);
+    a.x = fma(x.x, wp, a.x);
+    a.y = fma(x.y, wp, a.y);
+  }
+  reinterpret_cast<double2*>(g.Jpart + (int64_t)sp * g.ldB)[q] = a;
+}
+
+// Phase 6: out[i, j] = out[j, i] = J_ij + k_scale K_ij (splits summed in order).
+__global__ void __launch_bounds__(256) k_grp_finalize(const GroupMol* __restrict__ mols, const int64_t* __restrict__ pre,
+                                                      int count, int64_t total, double* __restrict__ out0,
+                                                      int64_t out_mol, int64_t ldo, double k_scale,
+                                                      const int* __restrict__ active) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int m = group_find(pre, count, e);
+    if (!active[m]) continue;
+    const GroupMol& g = mols[m];
+    const int64_t t = e - pre[m];
+    const int64_t j = tri_root(t), i = t - j * (j + 1) / 2;
+    const int64_t k = tile_pair_index(i / TS, j / TS) * TILE_ELEMS + (i % TS) + TS * (j % TS);
+    double vj = 0.0;
+    for (int sp = 0; sp < g.jsplits; ++sp) vj += g.Jpart[(int64_t)sp * g.ldB + k];
+    const int64_t Ib = i / KB, Jb = j / KB;
+    const int64_t q = Jb * (Jb + 1) / 2 + Ib;
+    const int64_t off = (i % KB) + (int64_t)KB * (j % KB);
+    double vk = 0.0;
+    for (int sp = 0; sp < g.ksplits; ++sp) vk += g.Kpart[((int64_t)sp * g.pairs + q) * (KB * KB) + off];
+    const double v = vj + k_scale * vk;
+    double* o = out0 + m * out_mol;
+    o[i * ldo + j] = v;
+    o[j * ldo + i] = v;
+  }
+}
+
+int group_ctas_per_sm(int cfg) { return cfg == 1 ? 3 : 2; }
+
+template <class Cfg>
+static void grp_half_cfg(const GroupMol* mols, const int64_t* pre, int count, int64_t total, const int* active,
+                         int* err, int sms, cudaStream_t st) {
+  cudaFuncSetAttribute(k_grp_half<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)sms * min_ctas<Cfg>()));
+  count_launch();
+  k_grp_half<Cfg><<<(unsigned)grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(mols, pre, count, total, active, err);
+}
+
+template <class Cfg>
+static void grp_rank_cfg(const GroupMol* mols, const int64_t* pre, int count, int64_t total, const int* active,
+                         int* err, int sms, cudaStream_t st) {
+  cudaFuncSetAttribute(k_grp_rank<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)sms * min_ctas<Cfg>()));
+  count_launch();
+  k_grp_rank<Cfg><<<(unsigned)grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(mols, pre, count, total, active, err);
+}
+
+int group_cta_rows(int cfg) { return cfg == 4 ? 128 : 64; }
+int group_cta_cols(int cfg) { return 64; }
+int group_rank_subs(int cfg) { return cfg == 4 ? 2 : 4; }
+
+void launch_group(const GroupPlan& gp, const double* C0, int64_t c_mol, int64_t c_row, int64_t c_col, double k_scale,
+                  double* out0, int64_t out_mol, int64_t ldo, const int* active, int* err, int sms, cudaStream_t st) {
+  const int n = gp.count;
+  {
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(gp.total[0], 256), 148 * 16));
+    count_launch();
+    k_grp_prepare<<<blocks, 256, 0, st>>>(gp.mols, gp.pre[0], n, gp.total[0], C0, c_mol, c_row, c_col, active);
+  }
+  count_launch();
+  k_grp_pass1<<<(unsigned)gp.total[1], 256, 0, st>>>(gp.mols, gp.pre[1], n, active);
+  switch (gp.ht_cfg) {
+    case 0: grp_half_cfg<HtCfg0>(gp.mols, gp.pre[2], n, gp.total[2], active, err, sms, st); break;
+    case 4: grp_half_cfg<HtCfg4>(gp.mols, gp.pre[2], n, gp.total[2], active, err, sms, st); break;
+    default: grp_half_cfg<HtCfg1>(gp.mols, gp.pre[2], n, gp.total[2], active, err, sms, st); break;
+  }
+  switch (gp.rk_cfg) {
+    case 0: grp_rank_cfg<RkCfg0>(gp.mols, gp.pre[3], n, gp.total[3], active, err, sms, st); break;
+    case 4: grp_rank_cfg<RkCfg4>(gp.mols, gp.pre[3], n, gp.total[3], active, err, sms, st); break;
+    default: grp_rank_cfg<RkCfg1>(gp.mols, gp.pre[3], n, gp.total[3], active, err, sms, st); break;
+  }
+  count_launch();
+  k_grp_pass2<<<(unsigned)gp.total[4], 256, 0, st>>>(gp.mols, gp.pre[4], n, active);
+  {
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(gp.total[5], 256), 148 * 16));
+    count_launch();
+    k_grp_finalize<<<blocks, 256, 0, st>>>(gp.mols, gp.pre[5], n, gp.total[5], out0, out_mol, ldo, k_scale, active);
+  }
 }
 
 }  // namespace rijk

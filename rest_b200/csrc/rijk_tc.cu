@@ -19,12 +19,23 @@
 // of a (R x 64) block at byte offset (k8 * R/8 + r8) * 128, row r%8 of it at
 // (r%8) * 16.  The descriptor's stride between core matrices along the rows is
 // then 128 bytes (SBO) and along K is R/8 * 128 bytes (LBO).  Each pipeline
-// stage is a handful of large contiguous bulk copies (TMA engine, no multicast).
+// stage is a handful of contiguous bulk copies (TMA engine, no multicast).
+//
+// The split tensor keeps only the upper 128 x 128 squares (I <= J) of each
+// symmetric B_P, as the FP64 tensor keeps only its upper 32 x 32 tiles.  A
+// square below the diagonal is read from its mirror: the same core matrices,
+// seen with the rows and K exchanged, are the MN-major canonical layout (each
+// core matrix is 8 K-rows of 16 bytes along M), which the MMA takes with the
+// A-major bit of the instruction descriptor set.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "rijk_common.cuh"
 #include "rijk_internal.h"
@@ -58,11 +69,12 @@ __device__ __forceinline__ uint64_t smem_desc(const void* p, uint32_t lbo, uint3
 }
 
 // kind::f16 instruction descriptor: BF16 A and B, FP32 D, both K-major.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool neg_b) {
-  return (1u << 4)                    // D format F32
-         | (1u << 7)                  // A format BF16
-         | (1u << 10)                 // B format BF16
-         | ((neg_b ? 1u : 0u) << 14)  // negate B
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool neg_b, bool a_mn_major = false) {
+  return (1u << 4)                        // D format F32
+         | (1u << 7)                      // A format BF16
+         | (1u << 10)                     // B format BF16
+         | ((neg_b ? 1u : 0u) << 14)      // negate B
+         | ((a_mn_major ? 1u : 0u) << 15)  // A is MN-major (else K-major)
          | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
@@ -116,43 +128,62 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// One tiled tensor copy (TMA, this GPU's memory, no multicast) of a 3-D box.
+__device__ __forceinline__ void tma_load_3d(void* smem_dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(smem_dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
 __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
   hi = __double2bfloat16(x);
   lo = __double2bfloat16(x - (double)__bfloat162float(hi));
 }
 
 // ---- layout producers --------------------------------------------------------
-// Bs[P][mb][kb] (hi and lo planes): the full symmetric B_P (n_pad x n_pad, rows
-// mu, K = kappa) from the FP64 tile-packed tensor.
-__global__ void __launch_bounds__(256) k_split_tensor(const double* __restrict__ B, int64_t ldB, int64_t n, int nt,
-                                                      int nmb, int nkb, int64_t p0, int64_t np,
-                                                      __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
-  const int64_t per_p = (int64_t)nmb * nkb * BLOCK_ELEMS;
+// Square (I <= J) of B_P is number J (J + 1) / 2 + I, two (128 x 64) K-major
+// blocks (K halves j = 0, 1): rows mu = 128 I + r, K kappa = 128 J + 64 j + k.
+__host__ __device__ __forceinline__ int64_t sq_index(int64_t I, int64_t J) { return J * (J + 1) / 2 + I; }
+
+// Bs[P][square][j] (hi and lo planes) from the FP64 tile-packed tensor; the
+// diagonal squares hold both triangles, entries beyond n are zero.
+__global__ void __launch_bounds__(256) k_split_tensor(const double* __restrict__ B, int64_t ldB, int64_t n, int nmb,
+                                                      int64_t p0, int64_t np, __nv_bfloat16* __restrict__ hi,
+                                                      __nv_bfloat16* __restrict__ lo) {
+  const int64_t nsq = (int64_t)nmb * (nmb + 1) / 2;
+  const int64_t per_p = nsq * 2 * BLOCK_ELEMS;
   const int64_t total = np * per_p;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t pl = e / per_p;
     const int64_t rem = e - pl * per_p;
     const int64_t blk = rem / BLOCK_ELEMS;
     const int o = (int)(rem - blk * BLOCK_ELEMS);
-    const int mb = (int)(blk / nkb), kb = (int)(blk % nkb);
+    const int64_t sq = blk >> 1;
+    const int j = (int)(blk & 1);
+    int64_t J = (int64_t)((sqrt(8.0 * (double)sq + 1.0) - 1.0) * 0.5);
+    while (J * (J + 1) / 2 > sq) --J;
+    while ((J + 1) * (J + 2) / 2 <= sq) ++J;
+    const int64_t I = sq - J * (J + 1) / 2;
     // invert core_off for R = 128
     const int within = o & 63, core = o >> 6;
     const int r = ((core % (TC_M / 8)) << 3) | (within >> 3);
     const int k = ((core / (TC_M / 8)) << 3) | (within & 7);
-    const int64_t mu = (int64_t)mb * TC_M + r, ka = (int64_t)kb * TC_KB + k;
+    const int64_t mu = I * TC_M + r, ka = J * TC_M + j * TC_KB + k;
     double x = 0.0;
     if (mu < n && ka < n) {
-      const int64_t I = mu / TS, J = ka / TS;
+      const int64_t ti = mu / TS, tj = ka / TS;
       const double* Bp = B + (p0 + pl) * ldB;
-      x = I <= J ? Bp[tile_pair_index(I, J) * TILE_ELEMS + (mu % TS) + TS * (ka % TS)]
-                 : Bp[tile_pair_index(J, I) * TILE_ELEMS + (ka % TS) + TS * (mu % TS)];
+      x = ti <= tj ? Bp[tile_pair_index(ti, tj) * TILE_ELEMS + (mu % TS) + TS * (ka % TS)]
+                   : Bp[tile_pair_index(tj, ti) * TILE_ELEMS + (ka % TS) + TS * (mu % TS)];
     }
     __nv_bfloat16 h, l;
     split_bf16(x, h, l);
     hi[e] = h;
     lo[e] = l;
   }
-  (void)nt;
 }
 
 // Vs[kb] (hi, lo): columns of V (n x ncols, column-major, ld) as the B operand
@@ -192,12 +223,23 @@ struct HalfTcP {
   static_assert((size_t)STAGES * STAGE_BYTES + 1024 + 256 <= SMEM, "stage budget");
 };
 
+// K step kb of row block mb reads square (mb, kb / 2) when mb <= kb / 2, else
+// the mirror square (kb / 2, mb) seen MN-major: its 16 groups of 8 rows mu
+// (one 1 KB run of the 8 core matrices of K half kb % 2 each) land at 1 KB
+// strides, so the MN-major descriptor has 128-byte K-group and 1 KB M-group
+// strides.
+// With use_tm the mirrored half is one tiled tensor copy per plane: the plane
+// seen as rows of 1024 BF16 (one group of 8 rows of a square, all 16 of its K
+// groups), as dims {256, 4, rows}; the box {256, 2, 16} at (0, 2 j, 16 square)
+// is K half j of the square's 16 row groups, landing at 1 KB per group.
 template <int NPAD>
 __global__ void __launch_bounds__(192, 1)
     k_half_tc_persistent(const __nv_bfloat16* __restrict__ Bhi, const __nv_bfloat16* __restrict__ Blo, int nmb,
                          int nkb, const __nv_bfloat16* __restrict__ Vhi, const __nv_bfloat16* __restrict__ Vlo,
                          int nib, int64_t ntiles, __nv_bfloat16* __restrict__ Xhi, __nv_bfloat16* __restrict__ Xlo,
-                         int* err) {
+                         int* err, const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
+                         int use_tm, int64_t p0) {
+  const int64_t nsq = (int64_t)nmb * (nmb + 1) / 2;
   using C = HalfTcP<NPAD>;
   constexpr int S = C::STAGES;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -230,32 +272,52 @@ __global__ void __launch_bounds__(192, 1)
   bool ok = true;
 
   if (warp == 0) {
-    if (lane == 0) {
-      for (int64_t lt = 0; lt < my_tiles && ok; ++lt) {
-        const int64_t tile = blockIdx.x + lt * G;
-        const int64_t pl = tile / nmb;
-        const int mb = (int)(tile % nmb);
-        for (int kb = 0; kb < nkb && ok; ++kb) {
-          const int64_t g = lt * nkb + kb;
-          const int s = (int)(g % S);
-          if (g >= S) ok = mbar_wait_bounded(&empty[s], (uint32_t)(((g / S) - 1) & 1), err);
-          if (!ok) break;
-          uint8_t* st = smem + s * C::STAGE_BYTES;
-          mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
-          const int64_t boff = ((pl * nmb + mb) * (int64_t)nkb + kb) * BLOCK_ELEMS;
-          bulk_g2s(st, Bhi + boff, BLOCK_BYTES, &full[s]);
-          bulk_g2s(st + BLOCK_BYTES, Blo + boff, BLOCK_BYTES, &full[s]);
-          const int64_t voff = (int64_t)kb * NPAD * TC_KB;
-          bulk_g2s(st + 2 * BLOCK_BYTES, Vhi + voff, C::V_BYTES, &full[s]);
-          bulk_g2s(st + 2 * BLOCK_BYTES + C::V_BYTES, Vlo + voff, C::V_BYTES, &full[s]);
+    // The whole warp stages: lane 0 waits for the slot and arms the barrier,
+    // then the copies are issued one per lane (a mirrored square is 32 runs
+    // of 1 KB, hi and lo).
+    for (int64_t lt = 0; lt < my_tiles && ok; ++lt) {
+      const int64_t tile = blockIdx.x + lt * G;
+      const int64_t pl = tile / nmb;
+      const int mb = (int)(tile % nmb);
+      for (int kb = 0; kb < nkb && ok; ++kb) {
+        const int64_t g = lt * nkb + kb;
+        const int s = (int)(g % S);
+        if (lane == 0 && g >= S) ok = mbar_wait_bounded(&empty[s], (uint32_t)(((g / S) - 1) & 1), err);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) break;
+        uint8_t* st = smem + s * C::STAGE_BYTES;
+        if (lane == 0) mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
+        __syncwarp();
+        const int Kb = kb >> 1, j = kb & 1;
+        if (mb <= Kb) {
+          const int64_t boff = ((pl * nsq + sq_index(mb, Kb)) * 2 + j) * BLOCK_ELEMS;
+          if (lane == 0) bulk_g2s(st, Bhi + boff, BLOCK_BYTES, &full[s]);
+          if (lane == 1) bulk_g2s(st + BLOCK_BYTES, Blo + boff, BLOCK_BYTES, &full[s]);
+        } else if (use_tm) {
+          const int z = (int)(((p0 + pl) * nsq + sq_index(Kb, mb)) * 16);
+          if (lane == 0) tma_load_3d(st, &tm_hi, 0, 2 * j, z, &full[s]);
+          if (lane == 1) tma_load_3d(st + BLOCK_BYTES, &tm_lo, 0, 2 * j, z, &full[s]);
+        } else {
+          const int64_t sbase = (pl * nsq + sq_index(Kb, mb)) * 2 * BLOCK_ELEMS + (int64_t)(8 * j) * 64;
+          const int run = lane & 15;  // M group of 8 rows: run `run` of 1 KB
+          const int64_t src = sbase + (int64_t)(run >> 3) * BLOCK_ELEMS + (int64_t)((run & 7) * (TC_M / 8)) * 64;
+          if (lane < 16)
+            bulk_g2s(st + run * 1024, Bhi + src, 1024, &full[s]);
+          else
+            bulk_g2s(st + BLOCK_BYTES + run * 1024, Blo + src, 1024, &full[s]);
         }
+        const int64_t voff = (int64_t)kb * NPAD * TC_KB;
+        if (lane == 2) bulk_g2s(st + 2 * BLOCK_BYTES, Vhi + voff, C::V_BYTES, &full[s]);
+        if (lane == 3) bulk_g2s(st + 2 * BLOCK_BYTES + C::V_BYTES, Vlo + voff, C::V_BYTES, &full[s]);
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t idesc = idesc_bf16(TC_M, NPAD, false);
+      constexpr uint32_t idesc_k = idesc_bf16(TC_M, NPAD, false);
+      constexpr uint32_t idesc_mn = idesc_bf16(TC_M, NPAD, false, true);
       for (int64_t lt = 0; lt < my_tiles && ok; ++lt) {
         const int b = (int)(lt & 1);
+        const int mb = (int)((blockIdx.x + lt * G) % nmb);
         if (lt >= 2) ok = mbar_wait_bounded(&acc_empty[b], (uint32_t)(((lt / 2) - 1) & 1), err);
         if (!ok) break;
         tc_fence_after();
@@ -267,11 +329,16 @@ __global__ void __launch_bounds__(192, 1)
           if (!ok) break;
           tc_fence_after();
           const uint8_t* st = smem + s * C::STAGE_BYTES;
+          const bool mirror = mb > (kb >> 1);
+          const uint32_t idesc = mirror ? idesc_mn : idesc_k;
+          // K-major: K groups 2 KB apart, row groups 128 B; MN-major mirror:
+          // K groups 128 B apart (LBO), row groups 1 KB (SBO)
+          const uint32_t a_lbo = mirror ? 128u : (TC_M / 8) * 128u, a_sbo = mirror ? 1024u : 128u;
 #pragma unroll
           for (int ks = 0; ks < TC_KB / 16; ++ks) {
-            const uint32_t ak = 2 * ks * (TC_M / 8) * 128, vk = 2 * ks * (NPAD / 8) * 128;
-            const uint64_t dah = smem_desc(st + ak, (TC_M / 8) * 128, 128);
-            const uint64_t dal = smem_desc(st + BLOCK_BYTES + ak, (TC_M / 8) * 128, 128);
+            const uint32_t ak = mirror ? 2 * ks * 128 : 2 * ks * (TC_M / 8) * 128, vk = 2 * ks * (NPAD / 8) * 128;
+            const uint64_t dah = smem_desc(st + ak, a_lbo, a_sbo);
+            const uint64_t dal = smem_desc(st + BLOCK_BYTES + ak, a_lbo, a_sbo);
             const uint64_t dvh = smem_desc(st + 2 * BLOCK_BYTES + vk, (NPAD / 8) * 128, 128);
             const uint64_t dvl = smem_desc(st + 2 * BLOCK_BYTES + C::V_BYTES + vk, (NPAD / 8) * 128, 128);
             const uint32_t acc0 = (kb > 0 || ks > 0) ? 1u : 0u;
@@ -473,19 +540,23 @@ TcGeom make_tc_geom(const Geom& g, int ncols) {
   return t;
 }
 
-int64_t tc_tensor_elems(const Geom& g) {
-  return g.naux * (int64_t)cdiv_t(g.n, TC_M) * cdiv_t(g.n, TC_KB) * BLOCK_ELEMS;
+// BF16 elements per aux row of one plane: the upper 128 x 128 squares
+static int64_t tc_row_elems(const Geom& g) {
+  const int64_t nmb = cdiv_t(g.n, TC_M);
+  return nmb * (nmb + 1) / 2 * 2 * BLOCK_ELEMS;
 }
+
+int64_t tc_tensor_elems(const Geom& g) { return g.naux * tc_row_elems(g); }
 
 void launch_split_tensor(const Geom& g, const double* B, int64_t p0, int64_t np, void* hi, void* lo,
                          cudaStream_t st) {
-  const int nmb = (int)cdiv_t(g.n, TC_M), nkb = (int)cdiv_t(g.n, TC_KB);
-  const int64_t per_p = (int64_t)nmb * nkb * BLOCK_ELEMS;
+  const int nmb = (int)cdiv_t(g.n, TC_M);
+  const int64_t per_p = tc_row_elems(g);
   auto* h = static_cast<__nv_bfloat16*>(hi) + p0 * per_p;
   auto* l = static_cast<__nv_bfloat16*>(lo) + p0 * per_p;
   const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv_t(np * per_p, 256), 148 * 32));
   count_launch();
-  k_split_tensor<<<blocks, 256, 0, st>>>(B, g.ldB, g.n, (int)g.nt, nmb, nkb, p0, np, h, l);
+  k_split_tensor<<<blocks, 256, 0, st>>>(B, g.ldB, g.n, nmb, p0, np, h, l);
 }
 
 void launch_split_cols(const Geom& g, const TcGeom& t, const double* V, int64_t ldv, int ncols, void* hi, void* lo,
@@ -507,20 +578,56 @@ static int sm_count() {
   return n;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// Map of one split plane for the mirrored reads (see k_half_tc_persistent).
+static bool mirror_map(CUtensorMap* m, const void* plane, int64_t rows) {
+  auto enc = tensor_map_encoder();
+  if (!enc || rows <= 0 || rows > (int64_t)INT32_MAX) return false;
+  const cuuint64_t dims[3] = {256, 4, (cuuint64_t)rows};
+  const cuuint64_t strides[2] = {512, 2048};  // bytes, dims 1 and 2
+  const cuuint32_t box[3] = {256, 2, 16};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(plane), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int NPAD>
 static void half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
                     const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st) {
   using C = HalfTcP<NPAD>;
   cudaFuncSetAttribute(k_half_tc_persistent<NPAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-  const int64_t per_p = (int64_t)t.nmb * t.nkb * BLOCK_ELEMS;
+  const int64_t per_p = tc_row_elems(g);
   const int64_t ntiles = np * t.nmb;
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, sm_count()));
+  // the maps cover the whole split tensor (g.naux rows of squares), from p = 0
+  const int64_t rows = g.naux * (int64_t)t.nmb * (t.nmb + 1) / 2 * 16;
+  CUtensorMap mhi, mlo;
+  const bool tm = mirror_map(&mhi, Bhi, rows) && mirror_map(&mlo, Blo, rows);
+  if (!tm) {
+    memset(&mhi, 0, sizeof(mhi));
+    memset(&mlo, 0, sizeof(mlo));
+  }
   count_launch();
   k_half_tc_persistent<NPAD><<<grid, 192, C::SMEM, st>>>(
       static_cast<const __nv_bfloat16*>(Bhi) + p0 * per_p, static_cast<const __nv_bfloat16*>(Blo) + p0 * per_p,
       t.nmb, t.nkb, static_cast<const __nv_bfloat16*>(Vhi), static_cast<const __nv_bfloat16*>(Vlo), t.nib, ntiles,
-      static_cast<__nv_bfloat16*>(Xhi), static_cast<__nv_bfloat16*>(Xlo), err);
-  (void)g;
+      static_cast<__nv_bfloat16*>(Xhi), static_cast<__nv_bfloat16*>(Xlo), err, mhi, mlo, tm ? 1 : 0, p0);
 }
 
 void launch_half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,

@@ -92,3 +92,33 @@ def refine(A, V, nvalid, steps: int = 4, tol_off: float = 1e-10, tol_orth: float
     lam = torch.gather(lam, 1, order)
     V = torch.gather(V, 2, order[:, None, :].expand(B, nm, nm))
     return lam, V, ok, off
+
+
+def eigh_batched(A, nvalid, pad_value: float = 1.0e6):
+    """All eigenpairs of the symmetric matrices A (B x nm x nm, FP64, device) with
+    the library's batched solver (rijk_eigh_batched_dev: Householder
+    tridiagonalisation and implicit QL, one CTA per matrix).  Matrix b uses its
+    leading nvalid[b] rows and columns; the padding gets eigenvalue pad_value and
+    unit vectors.  Returns (lam ascending, V with vectors as columns, ok per
+    matrix); A is not modified."""
+    import ctypes as C
+
+    import torch
+
+    from ._abi import RijkError, lib
+
+    B, nm, _ = A.shape
+    dev = A.device
+    a = A.contiguous().clone()
+    nv = torch.as_tensor(list(nvalid), dtype=torch.int32, device=dev)
+    lam = torch.empty(B, nm, dtype=A.dtype, device=dev)
+    V = torch.empty(B, nm, nm, dtype=A.dtype, device=dev)
+    work = torch.empty(B, nm, nm, dtype=A.dtype, device=dev)
+    info = torch.empty(B, dtype=torch.int32, device=dev)
+    st = lib().rijk_eigh_batched_dev(C.c_void_p(a.data_ptr()), nm, C.c_void_p(nv.data_ptr()), B, float(pad_value),
+                                     C.c_void_p(lam.data_ptr()), C.c_void_p(V.data_ptr()),
+                                     C.c_void_p(work.data_ptr()), C.c_void_p(info.data_ptr()),
+                                     C.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    if st != 0:
+        raise RijkError(st, "batched eigensolver")
+    return lam, V, info == 0

@@ -211,6 +211,27 @@ def local_blocks(mol, sh, D: np.ndarray, ps: PairSet):
     return T.reshape(len(ps.pairs), -1), M.reshape(len(ps.pairs), -1)
 
 
+def assembly_inputs(mol, sh, ps: PairSet):
+    """Host arrays of the device assembly (rijk_guess_assemble): unordered pairs
+    (A, B, row of (A, B), row of (B, A)), per-atom first AO / type / AO count /
+    water, and per water and element the 14 x 14 block rotation."""
+    rot = Rotator(mol, sh)
+    na = len(mol.symbols)
+    nw = na // 3
+    R = np.zeros((nw, 2, BLOCK, BLOCK))
+    for t, g in rot.rot.items():
+        R[:, t, :g.shape[1], :g.shape[2]] = g
+    first = np.array([rot.layout[a][0] for a in range(na)], dtype=np.int32)
+    nfun = np.array([rot.layout[a][1] for a in range(na)], dtype=np.int32)
+    A, B = ps.pairs[:, 0].astype(np.int64), ps.pairs[:, 1].astype(np.int64)
+    key = A * na + B
+    order = np.argsort(key)
+    sel = np.nonzero(A <= B)[0]
+    back = order[np.searchsorted(key[order], B[sel] * na + A[sel])]
+    up = np.stack([A[sel], B[sel], sel, back], axis=1).astype(np.int32)
+    return up, first, rot.typ.astype(np.int32), nfun, (np.arange(na) // 3).astype(np.int32), R
+
+
 def assemble_density(mol, sh, ps: PairSet, blocks: np.ndarray) -> np.ndarray:
     """Rotate predicted local blocks back, D_AB = G_A B G_B^T, and average the
     (A, B) and (B, A)^T predictions; pairs beyond the cutoff stay zero."""
@@ -390,8 +411,8 @@ def training_arrays(samples, basis: str = "def2-SVP"):
         ps = pair_features(mol)
         t, m = local_blocks(mol, sh, D, ps)
         F.append(ps.feats)
-        T.append(t)
-        M.append(m)
+        T.append(t.astype(np.float32))  # the network trains in FP32 / BF16
+        M.append(m.astype(np.float32))
         K.append(ps.kind)
     return np.concatenate(F), np.concatenate(T), np.concatenate(M), np.concatenate(K)
 
@@ -449,12 +470,33 @@ class LearnedGuess:
         Path(path).parent.mkdir(parents=True, exist_ok=True)
         np.savez_compressed(path, **st)
 
-    def predict_blocks(self, ps: PairSet) -> np.ndarray:
+    def _forward(self, ps: PairSet):
         import torch
 
         x = self.net.to_bf16(torch.tensor(self.norm.feats(ps.feats), dtype=torch.float32, device=self.net.dev))
-        y = self.net.forward(x).cpu().numpy().astype(np.float64)
+        return self.net.forward(x)
+
+    def predict_blocks(self, ps: PairSet) -> np.ndarray:
+        y = self._forward(ps).cpu().numpy().astype(np.float64)
         return self.norm.blocks(y, ps.kind)
+
+    def assemble_device(self, mol, sh, ps: PairSet, y):
+        """The AO density from the network output y (device, standardised)
+        with the library's assembly kernel; a device tensor (n x n, FP64)."""
+        import torch
+
+        dev = self.net.dev
+        if not hasattr(self, "_tstats"):
+            self._tstats = (torch.tensor(self.norm.t_mean, dtype=torch.float32, device=dev),
+                            torch.tensor(self.norm.t_std, dtype=torch.float32, device=dev))
+        up, first, typ, nfun, water, rot = (torch.as_tensor(a, device=dev) for a in assembly_inputs(mol, sh, ps))
+        rot = rot.to(torch.float64)
+        n = sh.nfun
+        D = torch.empty(n, n, dtype=torch.float64, device=dev)
+        tm, ts = self._tstats
+        _ck(lib().rijk_guess_assemble(_p(y), _p(tm), _p(ts), _p(up), up.shape[0], _p(first), _p(typ), _p(nfun),
+                                      _p(water), _p(rot), n, _p(D), self.net.stream), "guess_assemble")
+        return D
 
     def write_rest_init_guess(self, mol, path, ovlp: np.ndarray | None = None) -> bool:
         """Hands the predicted density to REST's own guess path: writes the
@@ -472,13 +514,18 @@ class LearnedGuess:
         write_init_guess(path, [d], shells=mol.shells(self.basis))
         return True
 
-    def density(self, mol, ovlp: np.ndarray | None = None, tol: float = 0.05):
+    def density(self, mol, ovlp: np.ndarray | None = None, tol: float = 0.05, on_device: bool = False):
+        """Predicted AO density (host array, or device tensor with on_device),
+        or None when its electron count tr(D S) is off by more than ``tol``."""
+        import torch
+
         sh = mol.shells(self.basis)
         ps = pair_features(mol)
-        D = assemble_density(mol, sh, ps, self.predict_blocks(ps))
+        D = self.assemble_device(mol, sh, ps, self._forward(ps))
         if ovlp is not None:
-            ne = float(np.sum(D * ovlp))
+            S = ovlp if torch.is_tensor(ovlp) else torch.as_tensor(np.asarray(ovlp), device=D.device)
+            ne = float((D * S).sum())
             if not np.isfinite(ne) or abs(ne - mol.nelec) > tol * mol.nelec:
                 return None
             D *= mol.nelec / ne
-        return D
+        return D if on_device else D.cpu().numpy()

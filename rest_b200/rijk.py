@@ -119,6 +119,18 @@ class RIJK:
     def set_tiles(self, half_transform_cfg: int, update_cfg: int):
         self._check(lib().rijk_ctx_set_tiles(self._h, int(half_transform_cfg), int(update_cfg)))
 
+    def tiles(self):
+        """(half-transform shape, update shape) currently selected."""
+        h, u = C.c_int(), C.c_int()
+        self._check(lib().rijk_ctx_get_tiles(self._h, C.byref(h), C.byref(u)))
+        return h.value, u.value
+
+    def shape(self):
+        """(num_basis, num_auxbas) of the loaded tensor (0, 0 when none)."""
+        n, naux = C.c_int64(), C.c_int64()
+        self._check(lib().rijk_ctx_info(self._h, C.byref(n), C.byref(naux), None))
+        return n.value, naux.value
+
     def autotune(self, ncols: int, sample_rows: int = 0):
         """Time every CTA shape on this tensor, keep the fastest; returns
         (half_cfg, update_cfg, {cfg: (half_ms, update_ms)})."""
@@ -332,6 +344,70 @@ class RIJK:
         out = np.empty(spin_channel * n * n)
         self._check(lib().rijk_density_matrix(self._h, _ptr(c), n, num_state, hm, _ptr(occ), spin_channel, _ptr(out)))
         return [out[s * n * n:(s + 1) * n * n].reshape(n, n, order="F") for s in range(spin_channel)]
+
+
+GROUP_CFGS = (0, 1, 4)  # CTA shapes the grouped build is compiled for
+
+
+_GROUP_TILES = {}  # (num_basis, num_auxbas, nocc) -> chosen shapes, for this process
+
+
+def group_tiles(ctx: "RIJK", nocc: int, sample_rows: int = 256):
+    """The project's autotuner applied to a group: times every CTA shape on
+    ``ctx``'s tensor (rijk_ctx_autotune) and keeps the fastest of those the
+    grouped build supports, for the half-transform and for the rank update.
+    The choice is kept per molecule shape for the rest of the process, so that
+    repeated runs take the same summation order, and ``ctx``'s own shapes are
+    left as they were."""
+    key = (*ctx.shape(), int(nocc))
+    if key not in _GROUP_TILES:
+        before = ctx.tiles()
+        _, _, ms = ctx.autotune(int(nocc), int(sample_rows))
+        ctx.set_tiles(*before)
+        _GROUP_TILES[key] = (min(GROUP_CFGS, key=lambda c: ms[c][0]), min(GROUP_CFGS, key=lambda c: ms[c][1]))
+    return _GROUP_TILES[key]
+
+
+class RIJKGroup:
+    """A molecule set's J/K built together (rijk_group_*): one launch per phase
+    for every molecule of ``ctxs`` (tensors loaded, left unchanged while the
+    group exists)."""
+
+    def __init__(self, ctxs, nocc, half_transform_cfg: int = 1, update_cfg: int = 1):
+        self._ctxs = list(ctxs)  # keep the contexts alive
+        arr = (C.c_void_p * len(self._ctxs))(*[c.handle.value for c in self._ctxs])
+        occ = (C.c_int64 * len(self._ctxs))(*[int(o) for o in nocc])
+        h = C.c_void_p()
+        st = lib().rijk_group_create(arr, len(self._ctxs), occ, int(half_transform_cfg), int(update_cfg),
+                                     C.byref(h))
+        if st != 0:
+            raise RijkError(st, "cannot create the molecule group")
+        self._h = h
+        self.tiles = (int(half_transform_cfg), int(update_cfg))
+
+    def jk_occ_dev(self, d_C: int, c_mol: int, c_row: int, c_col: int, k_scale: float, d_active: int, d_out: int,
+                   out_mol: int, ldo: int, stream: int = 0):
+        st = lib().rijk_group_jk_occ_dev(self._h, C.c_void_p(d_C), int(c_mol), int(c_row), int(c_col),
+                                         float(k_scale), C.c_void_p(d_active), C.c_void_p(d_out), int(out_mol),
+                                         int(ldo), C.c_void_p(stream or None))
+        if st != 0:
+            raise RijkError(st, "grouped J/K build failed")
+
+    def synchronize(self, stream: int = 0):
+        st = lib().rijk_group_synchronize(self._h, C.c_void_p(stream or None))
+        if st != 0:
+            raise RijkError(st, "grouped J/K build failed")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().rijk_group_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 (interpreter shutdown)
+            pass
 
 
 def energy_contraction(a_upper: np.ndarray, b_upper: np.ndarray) -> float:

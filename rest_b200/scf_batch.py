@@ -49,8 +49,8 @@ import numpy as np
 
 from .basis import DEVICE_MAX_L_AO, DEVICE_MAX_L_AUX, int1e, int1e_nuclear_dev, int2c2e, int2c2e_dev, int3c2e
 from .geometry import alkane, water_cluster  # noqa: F401  (re-exported)
-from .rijk import RIJK
-from .eigsolve import refine
+from .rijk import RIJK, RIJKGroup, group_tiles
+from .eigsolve import eigh_batched, refine
 from .scf import metric_inv_sqrt, metric_inv_sqrt_dev
 
 
@@ -90,7 +90,8 @@ class BatchedRHF:
                  precision: str = "fp64", integrals: str = "auto", rebuild_every: int = 16,
                  switch_etot: float = 1e-7, switch_rho: float = 1e-5, eig_workers: int = 8,
                  graphs: bool = False, split_min_basis: int = 512, refine_eigs: bool = True,
-                 setup_workers: int = 8, host_blas_threads: int | None = 1, contexts: list | None = None):
+                 setup_workers: int = 8, host_blas_threads: int | None = 1, contexts: list | None = None,
+                 grouped: bool = True, group_graphs: bool = True, native_eigh: bool = True):
         import torch
 
         if precision not in ("fp64", "mixed", "split"):
@@ -109,6 +110,8 @@ class BatchedRHF:
         # eigenbases of the previous iteration refined by matrix products
         # (eigsolve.refine); a fresh eigensolve only where that does not pass
         self.refine_eigs = refine_eigs
+        # fresh eigensolves on the library's batched solver (cuSOLVER as its fallback)
+        self.native_eigh = native_eigh
         self._vbasis, self._have_basis = None, []
         self._eig_counts = {"refined": 0, "eigh": 0}
         # CUDA graphs of the per-molecule FP64 J/K (orbital form), captured after
@@ -123,6 +126,20 @@ class BatchedRHF:
         self._borrowed = contexts is not None
         with host_blas_limit(host_blas_threads):
             self._setup(mols, basis, auxbas, device, metric, integrals, setup_workers, contexts)
+        # Grouped FP64 build: every molecule's J + K in one set of launches
+        # (rijk_group_*), tile shapes from the autotuner on the largest molecule,
+        # captured once in a CUDA graph and replayed every iteration.  It serves
+        # every build when no molecule takes split-precision steps.
+        self._group, self._ggraph = None, None
+        self.group_graphs = group_graphs
+        all_fp64 = precision == "fp64" or (precision == "mixed" and max(self.n) < split_min_basis)
+        if grouped and all_fp64:
+            t0 = time.perf_counter()
+            big = max(range(self.B), key=lambda i: self.n[i])
+            tiles = group_tiles(self.ctx[big], self.nocc[big], sample_rows=256)
+            self._group = RIJKGroup(self.ctx, self.nocc, *tiles)
+            self.setup_parts["group"] = time.perf_counter() - t0
+            self.setup_s += self.setup_parts["group"]
 
     def _setup(self, mols, basis, auxbas, device, metric, integrals, setup_workers, contexts):
         import torch
@@ -251,10 +268,26 @@ class BatchedRHF:
         self.setup_parts = parts
         self.setup_s = time.perf_counter() - t0
 
-    def _eigh(self, fp):
-        """Batched symmetric eigensolve, split over several streams from host
-        threads: each cuSOLVER call is a chain of small kernels, and chains on
-        different streams overlap on the GPU."""
+    def _eigh(self, fp, nvalid=None):
+        """Batched symmetric eigensolve: the library's solver (one CTA per
+        matrix, rijk_eigh_batched_dev), with cuSOLVER only for a matrix it
+        reports as not converged or one beyond its size limit."""
+        torch = self.torch
+        if nvalid is not None and fp.shape[1] <= 768 and self.native_eigh:
+            lam, V, ok = eigh_batched(fp, nvalid, pad_value=1.0e6)
+            bad = torch.nonzero(~ok).flatten().tolist()
+            if bad:
+                bi = torch.as_tensor(bad, device=self.dev)
+                lb, vb = self._eigh_cusolver(fp[bi])
+                lam[bi], V[bi] = lb, vb
+                self._eig_counts["cusolver"] = self._eig_counts.get("cusolver", 0) + len(bad)
+            return lam, V
+        return self._eigh_cusolver(fp)
+
+    def _eigh_cusolver(self, fp):
+        """Batched symmetric eigensolve through cuSOLVER, split over several
+        streams from host threads: each cuSOLVER call is a chain of small kernels,
+        and chains on different streams overlap on the GPU."""
         torch = self.torch
         nw = min(self.eig_workers, fp.shape[0])
         if nw <= 1:
@@ -318,7 +351,7 @@ class BatchedRHF:
         todo = [k for k in range(nr) if not done[k]]
         if todo:
             ti = torch.as_tensor(todo, device=self.dev)
-            e_t, v_t = self._eigh(A[ti])
+            e_t, v_t = self._eigh(A[ti], [self.n[rows[k]] for k in todo])
             e_r[ti], cp[ti] = e_t, v_t
         self._eig_counts["refined"] += nr - len(todo)
         self._eig_counts["eigh"] += len(todo)
@@ -439,8 +472,49 @@ class BatchedRHF:
             self._streak[i] += 1
         return self._gout.clone()
 
+    def _jk_group(self, C, active):
+        """J + K of the active molecules by the grouped build (graph replay)."""
+        torch = self.torch
+        B, nm = self.B, self.nmax
+        act = torch.tensor([1 if a else 0 for a in active], dtype=torch.int32, device=self.dev)
+        args = (nm * nm, nm, 1, -0.5)
+        if not self.group_graphs:
+            out = torch.zeros(B, nm, nm, dtype=torch.float64, device=self.dev)
+            self._group.jk_occ_dev(C.contiguous().data_ptr(), *args, act.data_ptr(), out.data_ptr(), nm * nm, nm,
+                                   torch.cuda.current_stream().cuda_stream)
+        else:
+            if self._ggraph is None:
+                self._gsC = torch.zeros(B, nm, nm, dtype=torch.float64, device=self.dev)
+                self._gsA = torch.zeros(B, dtype=torch.int32, device=self.dev)
+                self._gsO = torch.zeros(B, nm, nm, dtype=torch.float64, device=self.dev)
+                st = torch.cuda.Stream(device=self.dev)
+
+                def call():
+                    self._group.jk_occ_dev(self._gsC.data_ptr(), *args, self._gsA.data_ptr(), self._gsO.data_ptr(),
+                                           nm * nm, nm, st.cuda_stream)
+
+                st.wait_stream(torch.cuda.current_stream())
+                with torch.cuda.stream(st):
+                    call()  # warm-up outside the capture (function attributes, module load)
+                st.synchronize()
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, stream=st):
+                    call()
+                self._ggraph = g
+            self._gsC.copy_(C)
+            self._gsA.copy_(act)
+            self._ggraph.replay()
+            out = self._gsO.clone()
+        for i in range(B):
+            if active[i]:
+                self._nfp64[i] += 1
+                self._streak[i] += 1
+        return out
+
     def _jk(self, C, active):
         """J + K (full, padded batch) for the active molecules from their orbitals."""
+        if self._group is not None:
+            return self._jk_group(C, active)
         if self._graph is not None:
             return self._jk_replay(C, active)
         torch = self.torch
@@ -593,7 +667,9 @@ class BatchedRHF:
             if given[i]:
                 n = self.n[i]
                 D[i] = 0.0
-                D[i, :n, :n] = torch.as_tensor(np.asarray(initial_densities[i]), dtype=f64, device=self.dev)
+                d0 = initial_densities[i]
+                D[i, :n, :n] = d0 if torch.is_tensor(d0) else torch.as_tensor(np.asarray(d0), dtype=f64,
+                                                                               device=self.dev)
         F = self.H + self._jk(C, [not g for g in given])
         if any(given):
             F = F + self._jk_dm(D, given)
@@ -700,6 +776,11 @@ class BatchedRHF:
 
     def close(self):
         self._graph = None  # graphs go before the contexts whose memory they use
+        self._ggraph = None
+        if self._group is not None:
+            self.torch.cuda.synchronize(self.dev)
+            self._group.close()
+            self._group = None
         if self._pool is not None:
             self._pool.shutdown()
             self._pool = None
@@ -721,7 +802,8 @@ def device_bytes(n: int, naux: int, nocc: int, precision: str = "fp64") -> int:
     ldx = -(-n // 128) * 128
     scratch = min(4 << 30, naux * ldx * (-(-nocc // 128) * 128) * 8)
     split = naux_pad * ldx * ldx * 4 if precision in ("mixed", "split") else 0
-    return tensor + scratch + split + 8 * n * n * 8
+    group = naux * nocc * ldx * 8  # the grouped build's half-transform scratch
+    return tensor + scratch + split + group + 8 * n * n * 8
 
 
 def pool_reuse(held: list, needs: list, budget: float) -> int:

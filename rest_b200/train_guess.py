@@ -44,7 +44,7 @@ def evaluate(guess: LearnedGuess, mols, group_size: int = 32) -> dict:
     t0 = time.perf_counter()
     dens, fallback = [], 0
     for m in mols:
-        d = guess.density(m, ovlp=int1e(m, m.shells(BASIS), "ovlp"))
+        d = guess.density(m, ovlp=int1e(m, m.shells(BASIS), "ovlp"), on_device=True)
         fallback += d is None
         dens.append(d)
     t_pred = time.perf_counter() - t0

@@ -188,3 +188,78 @@ def test_same_size_molecules_from_given_densities_are_reproducible():
     assert all(runs[0].converged) and all(runs[1].converged)
     assert runs[0].iterations == runs[1].iterations
     assert np.array_equal(np.array(runs[0].energies), np.array(runs[1].energies))
+
+
+def test_grouped_build_equals_per_molecule_build():
+    """rijk_group_jk_occ_dev against each molecule's own J (a2) and occupied-orbital
+    K (a3) at 1e-10, for uneven clusters and every CTA shape of the grouped build;
+    an inactive molecule's output is left untouched."""
+    import numpy as np
+    import torch
+
+    from rest_b200 import RIJK, RIJKGroup
+
+    mols = [water_cluster(k, seed=70 + k) for k in (3, 1, 5, 2)]
+    ctxs = [RIJK(0) for _ in mols]
+    try:
+        for c, m in zip(ctxs, mols):
+            c.build_rimatr_from_shells(m.shells("def2-SVP"), m.shells("def2-SVP-JKFIT"))
+        ns = [m.shells("def2-SVP").nfun for m in mols]
+        nocc = [m.nelec // 2 for m in mols]
+        nm, B = max(ns), len(mols)
+        rng = np.random.default_rng(5)
+        C = torch.zeros(B, nm, nm, dtype=torch.float64, device="cuda")
+        for i, n in enumerate(ns):
+            q = np.linalg.qr(rng.standard_normal((n, n)))[0]
+            C[i, :n, :n] = torch.as_tensor(q, device="cuda")
+        ref = torch.zeros(B, nm, nm, dtype=torch.float64, device="cuda")
+        st = torch.cuda.current_stream().cuda_stream
+        for i, (c, n, o) in enumerate(zip(ctxs, ns, nocc)):
+            ci = C[i, :n, :o]
+            d = (2.0 * ci @ ci.T).contiguous()
+            ccm = ci.T.contiguous()
+            occ = torch.full((o,), 2.0, dtype=torch.float64, device="cuda")
+            npair = n * (n + 1) // 2
+            vj = torch.empty(npair, dtype=torch.float64, device="cuda")
+            vk = torch.empty(npair, dtype=torch.float64, device="cuda")
+            c.vj_upper_dev(d.data_ptr(), 1, 1.0, 1, vj.data_ptr(), st)
+            c.vk_upper_occ_dev(ccm.data_ptr(), o, [o - 1], occ.data_ptr(), 1, -0.5, vk.data_ptr(), st)
+            c.synchronize(st)
+            il = torch.tril_indices(n, n, device="cuda")
+            full = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+            full[il[1], il[0]] = vj + vk
+            full[il[0], il[1]] = vj + vk
+            ref[i, :n, :n] = full
+        for tiles in ((1, 1), (0, 4), (4, 0)):
+            g = RIJKGroup(ctxs, nocc, *tiles)
+            try:
+                out = torch.full((B, nm, nm), 7.0, dtype=torch.float64, device="cuda")
+                act = torch.tensor([1, 1, 0, 1], dtype=torch.int32, device="cuda")
+                g.jk_occ_dev(C.data_ptr(), nm * nm, nm, 1, -0.5, act.data_ptr(), out.data_ptr(), nm * nm, nm, st)
+                g.synchronize(st)
+                for i, n in enumerate(ns):
+                    if i == 2:
+                        assert bool((out[i] == 7.0).all())  # inactive: untouched
+                        continue
+                    assert float((out[i, :n, :n] - ref[i, :n, :n]).abs().max()) <= 1e-10
+            finally:
+                g.close()
+    finally:
+        for c in ctxs:
+            c.close()
+
+
+def test_grouped_batch_equals_per_molecule_batch():
+    """The batched SCF with the grouped build (under a CUDA graph) and with
+    per-molecule builds converge to the same energies and iteration counts."""
+    mols = [water_cluster(k, seed=80 + k) for k in (2, 4, 1, 3)]
+    res = {}
+    for grouped in (True, False):
+        b = BatchedRHF(mols, "def2-SVP", "def2-SVP-JKFIT", precision="fp64", metric="cholesky", grouped=grouped)
+        try:
+            res[grouped] = b.run(max_cycle=100, **TIGHT_BATCH)
+        finally:
+            b.close()
+    assert all(res[True].converged) and all(res[False].converged)
+    for a, b in zip(res[True].energies, res[False].energies):
+        assert abs(a - b) < 1e-9

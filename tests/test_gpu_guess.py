@@ -172,3 +172,20 @@ def test_learned_density_handed_to_rest_as_init_guess(tmp_path):
     perm = rest_ao_order(sh)
     assert np.array_equal(raw.T, d[np.ix_(perm, perm)])  # column-major, REST's AO order
     assert abs(float(np.sum(back * s)) - mol.nelec) < 1e-8
+
+
+@pytest.mark.parametrize("k", [1, 4, 13])
+def test_device_assembly_matches_host_assembly(k):
+    """rijk_guess_assemble (per unordered pair, both water frames, no atomics)
+    against the NumPy assembly of the same network output."""
+    from rest_b200.guess import assemble_density, pair_features
+
+    guess = LearnedGuess.load()
+    mol = water_cluster(k, seed=90 + k)
+    sh = mol.shells(guess.basis)
+    ps = pair_features(mol)
+    y = guess._forward(ps)
+    ref = assemble_density(mol, sh, ps, guess.norm.blocks(y.cpu().numpy().astype(np.float64), ps.kind))
+    got = guess.assemble_device(mol, sh, ps, y).cpu().numpy()
+    assert np.max(np.abs(got - ref)) <= 1e-6 * np.max(np.abs(ref))
+    assert np.array_equal(got, got.T)

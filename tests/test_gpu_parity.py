@@ -433,3 +433,29 @@ def test_benched_shape_n1200_aux_slab_against_oracle(monkeypatch, scratch):
         assert _maxdiff(ku[1], -_k_occ_from_rimatr(case.rimatr, n, c2, np.ones(150))) <= TOL
     finally:
         c.close()
+
+
+@pytest.mark.parametrize("n,naux,occs", [(150, 300, (72,)), (130, 260, (80,)), (100, 200, (65,)), (137, 200, (64, 10)),
+                                         (97, 150, (60, 7))])
+def test_vk_remainder_columns_of_the_last_full_block(ctx, n, naux, occs):
+    """Valid orbital columns ending 1..16 past a multiple of 64 are computed by
+    the last full column block's CTAs (one or two extra fragments staged in the
+    slot padding); RHF and UHF K against the oracle."""
+    case = host_case(n, naux, 2, seed=500 + n)
+    ctx.set_rimatr(case.rimatr, n)
+    ri3 = O.ri3fn_from_rimatr(case.rimatr, n)
+    rng = np.random.default_rng(n)
+    spin = len(occs)
+    num_state = max(occs) + 1
+    eig, homo, occ = [], [], []
+    for s, o in enumerate(occs):
+        c = np.asfortranarray(np.linalg.qr(rng.standard_normal((n, o)))[0])
+        e = np.zeros((n, num_state), order="F")
+        e[:, :o] = c
+        eig.append(e)
+        homo.append(o - 1)
+        occ.append(np.r_[np.linspace(0.5, 2.0 / spin, o), np.zeros(num_state - o)])
+    got = ctx.vk_upper_with_ri_v(eig, homo, occ, spin, -0.5 if spin == 1 else -1.0)
+    ref = O.vk_upper_with_ri_v(ri3, eig, homo, occ, spin, -0.5 if spin == 1 else -1.0)
+    for s in range(spin):
+        assert _maxdiff(got[s], ref[s]) <= TOL

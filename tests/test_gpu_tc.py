@@ -36,7 +36,7 @@ def _split_k_occ(ctx, c, occ):
         return out.cpu().numpy()
 
 
-@pytest.mark.parametrize("n,naux,nocc", [(64, 24, 8), (100, 40, 16), (200, 30, 40)])
+@pytest.mark.parametrize("n,naux,nocc", [(64, 24, 8), (100, 40, 16), (200, 30, 40), (300, 20, 24), (520, 6, 72)])
 def test_split_exchange_is_exact_on_bf16_representable_input(ctx, n, naux, nocc):
     rng = np.random.default_rng(n)
     npair = n * (n + 1) // 2
