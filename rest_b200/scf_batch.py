@@ -41,6 +41,7 @@ criteria, :1875-1951) and stop being updated once converged.
 """
 from __future__ import annotations
 
+import os
 import threading
 import time
 from dataclasses import dataclass, field
@@ -91,7 +92,7 @@ class BatchedRHF:
                  switch_etot: float = 1e-7, switch_rho: float = 1e-5, eig_workers: int = 8,
                  graphs: bool = False, split_min_basis: int = 512, refine_eigs: bool = True,
                  setup_workers: int = 8, host_blas_threads: int | None = 1, contexts: list | None = None,
-                 grouped: bool = True, group_graphs: bool = True, native_eigh: bool = True):
+                 grouped: bool = True, group_graphs: bool = True, native_eigh: bool | None = None):
         import torch
 
         if precision not in ("fp64", "mixed", "split"):
@@ -110,7 +111,10 @@ class BatchedRHF:
         # eigenbases of the previous iteration refined by matrix products
         # (eigsolve.refine); a fresh eigensolve only where that does not pass
         self.refine_eigs = refine_eigs
-        # fresh eigensolves on the library's batched solver (cuSOLVER as its fallback)
+        # fresh eigensolves on the library's batched solver (cuSOLVER as its
+        # fallback); RIJK_NATIVE_EIGH=0 selects cuSOLVER alone
+        if native_eigh is None:
+            native_eigh = os.environ.get("RIJK_NATIVE_EIGH", "1") != "0"
         self.native_eigh = native_eigh
         self._vbasis, self._have_basis = None, []
         self._eig_counts = {"refined": 0, "eigh": 0}
@@ -615,9 +619,20 @@ class BatchedRHF:
 
     def run(self, max_cycle: int = 100, acc_etot: float = 1e-8, acc_rho: float = 1e-5, acc_eev: float = 1e-5,
             num_max_diis: int = 8, initial_densities: list | None = None,
-            return_densities: bool = False) -> BatchResult:
+            return_densities: bool = False, guess=None) -> BatchResult:
         """Converge every molecule.  ``initial_densities``: per molecule an AO
-        density (n x n) to start from, or None for REST's hcore guess."""
+        density (n x n) to start from, or None for REST's hcore guess.
+        ``guess``: a model with ``density(mol, ovlp=S, on_device=True)`` (the
+        learned guess) that supplies the densities instead, checked against the
+        overlap matrices already on the device; a molecule whose prediction
+        fails the check starts from hcore."""
+        if guess is not None:
+            t0 = time.perf_counter()
+            initial_densities = [guess.density(m, ovlp=self.S[i, :self.n[i], :self.n[i]], on_device=True)
+                                 for i, m in enumerate(self.mols)]
+            self.setup_parts["guess"] = self.setup_parts.get("guess", 0.0) + time.perf_counter() - t0
+            self.setup_parts["guess_fallbacks"] = self.setup_parts.get("guess_fallbacks", 0) + sum(
+                d is None for d in initial_densities)
         with host_blas_limit(self.host_blas_threads):
             return self._run(max_cycle, acc_etot, acc_rho, acc_eev, num_max_diis, initial_densities,
                              return_densities)
@@ -832,6 +847,7 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
     run_kw = {k: kw.pop(k) for k in ("max_cycle", "acc_etot", "acc_rho", "acc_eev", "num_max_diis",
                                       "return_densities") if k in kw}
     guesses = kw.pop("initial_densities", None)
+    model = kw.pop("guess", None)
     sizes = [m.shells(basis).nfun for m in mols]
     order = sorted(range(len(mols)), key=lambda i: sizes[i])
     torch.cuda.empty_cache()
@@ -877,7 +893,8 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
                 held[j] = max(held[j], need[i])
             b = BatchedRHF([mols[i] for i in idx], basis, auxbas, device=device, contexts=pool[:len(idx)], **kw)
             try:
-                r = b.run(initial_densities=None if guesses is None else [guesses[i] for i in idx], **run_kw)
+                r = b.run(initial_densities=None if guesses is None else [guesses[i] for i in idx], guess=model,
+                          **run_kw)
             finally:
                 tt = time.perf_counter()
                 b.close()

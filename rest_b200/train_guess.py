@@ -36,27 +36,20 @@ def clusters(count: int, kmin: int, kmax: int, seed: int):
 
 
 def evaluate(guess: LearnedGuess, mols, group_size: int = 32) -> dict:
-    from .basis import int1e
-
     t0 = time.perf_counter()
     ref = run_molecule_set(mols, BASIS, AUXBAS, group_size=group_size, **CRIT)
     t_ref = time.perf_counter() - t0
     t0 = time.perf_counter()
-    dens, fallback = [], 0
-    for m in mols:
-        d = guess.density(m, ovlp=int1e(m, m.shells(BASIS), "ovlp"), on_device=True)
-        fallback += d is None
-        dens.append(d)
-    t_pred = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    lrn = run_molecule_set(mols, BASIS, AUXBAS, group_size=group_size, initial_densities=dens, **CRIT)
+    lrn = run_molecule_set(mols, BASIS, AUXBAS, group_size=group_size, guess=guess, **CRIT)
     t_lrn = time.perf_counter() - t0
+    t_pred = lrn.timings["setup_parts"].get("guess", 0.0)
+    fallback = int(lrn.timings["setup_parts"].get("guess_fallbacks", 0))
     de = np.abs(np.array(lrn.energies) - np.array(ref.energies))
     return {
         "molecules": len(mols),
         "hcore": {"iterations_mean": float(np.mean(ref.iterations)), "wall_s": t_ref, "scf_s": ref.scf_s,
                   "converged": int(sum(ref.converged))},
-        "learned": {"iterations_mean": float(np.mean(lrn.iterations)), "wall_s": t_lrn + t_pred, "scf_s": lrn.scf_s,
+        "learned": {"iterations_mean": float(np.mean(lrn.iterations)), "wall_s": t_lrn, "scf_s": lrn.scf_s,
                     "predict_s": t_pred, "converged": int(sum(lrn.converged)), "fallbacks": int(fallback)},
         "max_abs_energy_difference": float(de.max()),
         "iterations_saved_fraction": float(1.0 - np.mean(lrn.iterations) / np.mean(ref.iterations)),
