@@ -190,13 +190,19 @@ class Rotator:
             yield sel, rows, cols, self.rot[ta][w], self.rot[tb][w]
 
 
+_PINV = {}  # l -> pseudo-inverse of the harmonics at the sample points (a constant)
+
+
 def shell_rotations(l: int, Fs: np.ndarray) -> np.ndarray:
-    """shell_rotation for a stack of frames: (nw, 2l+1, 2l+1)."""
+    """shell_rotation for a stack of frames: (nw, 2l+1, 2l+1), all frames in one
+    evaluation of the harmonics."""
     if l == 0:
         return np.ones((len(Fs), 1, 1))
-    pinv = np.linalg.pinv(_harmonics(l, _SAMPLES))
-    y_rot = np.stack([_harmonics(l, _SAMPLES @ F) for F in Fs])
-    return np.transpose(pinv @ y_rot, (0, 2, 1))
+    if l not in _PINV:
+        _PINV[l] = np.linalg.pinv(_harmonics(l, _SAMPLES))
+    pts = np.einsum("sj,wjk->wsk", _SAMPLES, Fs).reshape(-1, 3)  # rows: F^T u_s for every frame
+    y_rot = _harmonics(l, pts).reshape(len(Fs), len(_SAMPLES), 2 * l + 1)
+    return np.transpose(_PINV[l] @ y_rot, (0, 2, 1))
 
 
 def local_blocks(mol, sh, D: np.ndarray, ps: PairSet):
