@@ -227,7 +227,8 @@ int rijk_vk_upper_lowrank_split_dev(rijk_ctx* ctx, const double* d_V, int64_t ld
  * tile).  nocc[m]: doubly occupied orbitals of molecule m.  The CTA shapes are
  * 0, 1 or 4 of rijk_ctx_set_tiles (the caller's autotuner picks them).  The
  * group owns the scratch of all molecules (one allocation at creation); its
- * contexts must stay loaded and unchanged while it exists. */
+ * contexts must stay loaded and unchanged while it exists (a call after one of
+ * them loaded another tensor returns RIJK_ERR_ARG). */
 typedef struct rijk_group rijk_group;
 int rijk_group_create(rijk_ctx* const* ctxs, int count, const int64_t* nocc, int half_transform_cfg, int update_cfg,
                       rijk_group** out);
@@ -363,7 +364,8 @@ int rijk_mlp_to_bf16(const float* src, uint16_t* dst, int64_t count, void* strea
  * type (0, 1), AO count (<= 14) and water index; rot: per water and element the
  * 14 x 14 rotation G of that element's AO block into the water's frame.  Writes
  * dm (num_basis^2, device): D_AB = 1/2 (G_A P_AB G_B^T |frame of A's water +
- * G_A P_BA^T G_B^T |frame of B's water), D_BA = D_AB^T, zero beyond the cutoff. */
+ * G_A P_BA^T G_B^T |frame of B's water), D_BA = D_AB^T, zero beyond the cutoff.
+ * A pair with an atom of more than 14 AOs or a type other than 0 / 1 is skipped. */
 int rijk_guess_assemble(const float* y, const float* t_mean, const float* t_std, const int32_t* upairs,
                         int64_t npairs, const int32_t* atom_first, const int32_t* atom_type, const int32_t* atom_nfun,
                         const int32_t* atom_water, const double* rot, int64_t num_basis, double* dm, void* stream);

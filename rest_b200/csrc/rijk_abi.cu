@@ -1195,6 +1195,8 @@ int rijk_ao2mo(rijk_ctx* ctx, const double* eigv, int64_t num_state, int64_t row
 struct rijk_group {
   int device = 0;
   int count = 0;
+  std::vector<rijk_ctx*> ctxs;
+  std::vector<int64_t> versions;  // each context's tensor version at creation
   rijk::GroupPlan plan{};
   void* mem = nullptr;  // descriptors, prefix sums, error words and every molecule's scratch
   int* d_err = nullptr;
@@ -1295,6 +1297,10 @@ int rijk_group_create(rijk_ctx* const* ctxs, int count, const int64_t* nocc, int
   rijk_group* gr = new rijk_group();
   gr->device = device;
   gr->count = count;
+  for (int m = 0; m < count; ++m) {
+    gr->ctxs.push_back(ctxs[m]);
+    gr->versions.push_back(ctxs[m]->tensor_version);
+  }
   gr->mem = mem;
   gr->d_err = reinterpret_cast<int*>(base + err_off);
   gr->plan.mols = reinterpret_cast<rijk::GroupMol*>(base);
@@ -1328,6 +1334,11 @@ int rijk_group_jk_occ_dev(rijk_group* g, const double* d_C, int64_t c_mol, int64
                           double k_scale, const int* d_active, double* d_out, int64_t out_mol, int64_t ldo,
                           void* stream) {
   if (!g || !d_C || !d_active || !d_out || ldo <= 0) return RIJK_ERR_ARG;
+  for (int m = 0; m < g->count; ++m)
+    if (!g->ctxs[m]->have || g->ctxs[m]->tensor_version != g->versions[m]) {
+      g->last = "a context of the group has loaded another tensor since the group was created";
+      return RIJK_ERR_ARG;
+    }
   if (cudaSetDevice(g->device) != cudaSuccess) return RIJK_ERR_CUDA;
   rijk::launch_group(g->plan, d_C, c_mol, c_row, c_col, k_scale, d_out, out_mol, ldo, d_active, g->d_err, g->sms,
                      static_cast<cudaStream_t>(stream));

@@ -236,6 +236,7 @@ __global__ void __launch_bounds__(128) k_guess_assemble(const float* __restrict_
     const int a = up[4 * u], b = up[4 * u + 1];
     const int64_t iab = up[4 * u + 2], iba = up[4 * u + 3];
     const int ta = type[a], tb = type[b], na = nfun[a], nb = nfun[b];
+    if (na > GB || nb > GB || na < 0 || nb < 0 || (ta | tb) & ~1) continue;  // outside the 14 x 14 blocks: skipped
     const int kab = 2 * ta + tb, kba = 2 * tb + ta;
     const double* GAa = rot + ((int64_t)water[a] * 2 + ta) * GB2;
     const double* GBa = rot + ((int64_t)water[a] * 2 + tb) * GB2;

@@ -244,6 +244,19 @@ def test_grouped_build_equals_per_molecule_build():
                     assert float((out[i, :n, :n] - ref[i, :n, :n]).abs().max()) <= 1e-10
             finally:
                 g.close()
+        # a context that loads another tensor invalidates the group
+        from rest_b200 import RijkError
+
+        g = RIJKGroup(ctxs, nocc)
+        try:
+            ctxs[1].build_rimatr_from_shells(mols[1].shells("def2-SVP"), mols[1].shells("def2-SVP-JKFIT"))
+            out = torch.zeros(B, nm, nm, dtype=torch.float64, device="cuda")
+            act = torch.ones(B, dtype=torch.int32, device="cuda")
+            with pytest.raises(RijkError) as ei:
+                g.jk_occ_dev(C.data_ptr(), nm * nm, nm, 1, -0.5, act.data_ptr(), out.data_ptr(), nm * nm, nm, st)
+            assert ei.value.status == 1
+        finally:
+            g.close()
     finally:
         for c in ctxs:
             c.close()
