@@ -55,7 +55,7 @@ def workload(n: int, nocc: int = 0) -> dict:
 def config_of(w: dict, ngpu: int) -> dict:
     return {
         "workload": f"synthetic RI-JK sweep, FP64 plain form: n={w['n']}, N={w['naux']}, nocc={w['nocc']}; "
-        "one Fock build (J + occupied-orbital K) per step",
+        "one Fock build (J of D = C C^T + occupied-orbital K) per step",
         "num_basis": w["n"],
         "num_auxbas": w["naux"],
         "nocc": w["nocc"],
@@ -230,9 +230,16 @@ def run_ours(args, w):
     vk = torch.empty(npair, dtype=torch.float64, device="cuda")
     st = ctx.stream
 
-    def step():
+    def step_separate():
         ctx.vj_upper_dev(dm.data_ptr(), 1, 1.0, 1, vj.data_ptr(), st)
         ctx.vk_upper_occ_dev(c_cm.data_ptr(), nocc, [nocc - 1], occ.data_ptr(), 1, -1.0, vk.data_ptr(), st)
+
+    def step_fused():
+        # J of D = C C^T and K in one build: J's aux-row scalars come out of the K half-transform
+        ctx.vjk_upper_occ_dev(c_cm.data_ptr(), nocc, [nocc - 1], occ.data_ptr(), 1, 1.0, -1.0, vj.data_ptr(),
+                              vk.data_ptr(), st)
+
+    step = step_fused if args.jk == "fused" else step_separate
 
     def barrier():
         torch.cuda.synchronize()
@@ -290,6 +297,25 @@ def run_ours(args, w):
     for k in ("j_pass1", "j_pass2"):
         if cls_time.get(k):
             j_rates[k] = w["j_pass_bytes"] / cls_time[k] / 1e9
+
+    # the other J/K form on the same workload, timed the same way (for the record)
+    other = None
+    if not args.no_split:
+        alt = step_separate if args.jk == "fused" else step_fused
+        for _ in range(2):
+            alt()
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(args.steps):
+            alt()
+        a1.record(stream)
+        torch.cuda.synchronize()
+        t_alt = a0.elapsed_time(a1) / 1e3 / args.steps
+        other = {"jk": "separate" if args.jk == "fused" else "fused", "ms_per_step": t_alt * 1e3,
+                 "value": world * flops / t_alt / 1e12,
+                 "what": "J by two passes over the tensor (rijk_vj_upper_dev) + K (rijk_vk_upper_occ_dev)"
+                 if args.jk == "fused" else "rijk_vjk_upper_occ_dev"}
 
     # split-precision exchange (3 x BF16 on tcgen05) on the same workload: the
     # first call builds the BF16 copies of the tensor (once per geometry)
@@ -354,10 +380,16 @@ def run_ours(args, w):
         homo = (C.c_int64 * 2)(nocc - 1, 0)
 
         def e2e_step():
-            r1 = L.rijk_vj_upper_with_rimatr_v(ctx.handle, C.c_void_p(h_dm.data_ptr()), 1, 1.0,
-                                               C.c_void_p(h_vj.data_ptr()))
-            r2 = L.rijk_vk_upper_with_ri_v(ctx.handle, C.c_void_p(h_c.data_ptr()), nocc, homo,
-                                           C.c_void_p(h_occ.data_ptr()), 1, -1.0, C.c_void_p(h_vk.data_ptr()))
+            if args.jk == "fused":
+                r1 = L.rijk_vjk_upper_with_ri_v(ctx.handle, C.c_void_p(h_c.data_ptr()), nocc, homo,
+                                                C.c_void_p(h_occ.data_ptr()), 1, 1.0, -1.0,
+                                                C.c_void_p(h_vj.data_ptr()), C.c_void_p(h_vk.data_ptr()))
+                r2 = 0
+            else:
+                r1 = L.rijk_vj_upper_with_rimatr_v(ctx.handle, C.c_void_p(h_dm.data_ptr()), 1, 1.0,
+                                                   C.c_void_p(h_vj.data_ptr()))
+                r2 = L.rijk_vk_upper_with_ri_v(ctx.handle, C.c_void_p(h_c.data_ptr()), nocc, homo,
+                                               C.c_void_p(h_occ.data_ptr()), 1, -1.0, C.c_void_p(h_vk.data_ptr()))
             if r1 or r2:
                 raise RuntimeError(f"e2e call failed: {r1} {r2}")
 
@@ -367,11 +399,13 @@ def run_ours(args, w):
         for _ in range(args.steps):
             e2e_step()
         te = replicas.max_over_ranks(rk, time.perf_counter() - t0)
-        h2d = (n * n + n * nocc + nocc) * 8
+        h2d = ((n * n if args.jk == "separate" else 0) + n * nocc + nocc) * 8
         d2h = 2 * npair * 8
         e2e = {"value": world * flops / (te / args.steps) / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": te / args.steps * 1e3,
-               "how": "rijk_vj_upper_with_rimatr_v + rijk_vk_upper_with_ri_v on pinned host buffers, wall clock"}
+               "how": ("rijk_vjk_upper_with_ri_v (orbitals and occupations in, J and K out)" if args.jk == "fused"
+                       else "rijk_vj_upper_with_rimatr_v + rijk_vk_upper_with_ri_v")
+               + " on pinned host buffers, wall clock"}
 
     # RI-HF SCF on the water molecule of the plain config (def2-SVP / def2-SVP-JKFIT):
     # FP64 GPU path and mixed-precision path, same converged energy
@@ -439,6 +473,8 @@ def run_ours(args, w):
             "gpu_launches": int(launches),
             "e2e": e2e,
             "cpu_baseline": cpu_base,
+            "jk_form": args.jk,
+            "other_jk_form": other,
             "split_precision": split,
             "scf_water": scf,
             **apps,
@@ -696,6 +732,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=1200, help="num_basis of the sweep workload")
     ap.add_argument("--nocc", type=int, default=0, help="occupied orbitals (default n // 6; for profiling cases)")
+    ap.add_argument("--jk", choices=["fused", "separate"], default="fused",
+                    help="fused: J and K from one build (rijk_vjk_upper_occ_dev); separate: J by its own two passes")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision (tcgen05) measurement")

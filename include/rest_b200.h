@@ -200,6 +200,24 @@ int rijk_vk_upper_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state
                           void* stream);
 int rijk_vk_upper_dm_dev(rijk_ctx* ctx, const double* d_dm, int spin_channel, double scaling_factor, double* d_vk,
                          void* stream);
+/* J and K together from the occupied orbitals, as REST's SCF asks for them
+ * (generate_hf_hamiltonian_ri_v, src/scf_io/mod.rs:1339-1381, which calls
+ * vj_upper_with_ri_v_sync on dm = C diag(occ) C^T and vk_upper_with_ri_v_sync on
+ * C).  dm_s = C_s[:, :homo+1] diag(occ_s) C_s[:, :homo+1]^T (REST's density
+ * matrix where the states above homo are empty); d_vj = j_scaling_factor
+ * upper(J[dm_s]) per spin, equal to rijk_vj_upper_dev(dm_mode 0) on that dm;
+ * d_vk as rijk_vk_upper_occ_dev (occupations >= 0).  J's
+ * per-aux-row scalars B_P : dm_s come out of the K half-transform, so the build
+ * reads the tensor once for K and once for J instead of once for K and twice
+ * for J. */
+int rijk_vjk_upper_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int64_t* homo,
+                           const double* d_occupation, int spin_channel, double j_scaling_factor,
+                           double k_scaling_factor, double* d_vj, double* d_vk, void* stream);
+/* Host-pointer form of rijk_vjk_upper_occ_dev (inputs as rijk_vk_upper_with_ri_v;
+ * vj and vk: spin_channel x npair each). */
+int rijk_vjk_upper_with_ri_v(rijk_ctx* ctx, const double* eigv, int64_t num_state, const int64_t* homo,
+                             const double* occupation, int spin_channel, double j_scaling_factor,
+                             double k_scaling_factor, double* vj, double* vk);
 
 /* ---- split-precision exchange on the 5th-generation tensor cores -------------- */
 /* Same contraction as rijk_vk_upper_occ_dev (REST vk_upper_with_ri_v_sync,
@@ -224,7 +242,8 @@ int rijk_vk_upper_lowrank_split_dev(rijk_ctx* ctx, const double* d_V, int64_t ld
  * 2490-2561, 2758-2834); a group runs that build for many molecules (one
  * context each, tensors loaded) in six launches for all of them, the two
  * tensor-core phases as persistent kernels over work items (molecule, aux row,
- * tile).  nocc[m]: doubly occupied orbitals of molecule m.  The CTA shapes are
+ * tile); J's aux-row scalars come out of the half-transform phase, so J reads
+ * each tensor once.  nocc[m]: doubly occupied orbitals of molecule m.  The CTA shapes are
  * 0, 1 or 4 of rijk_ctx_set_tiles (the caller's autotuner picks them).  The
  * group owns the scratch of all molecules (one allocation at creation); its
  * contexts must stay loaded and unchanged while it exists (a call after one of
@@ -259,6 +278,19 @@ int rijk_group_synchronize(rijk_group* group, void* stream);
  * matrix: Householder tridiagonalisation, explicit Q, implicit-shift QL. */
 int rijk_eigh_batched_dev(double* d_a, int64_t ld, const int32_t* d_nvalid, int64_t batch, double pad_value,
                           double* d_w, double* d_v, double* d_work, int32_t* d_info, void* stream);
+
+/* ---- batched DIIS coefficients (FP64) ------------------------------------------- */
+/* REST's diis_solver (src/scf_io/mod.rs:3138-3188) for a batch of molecules:
+ * d_gram: batch row-major m x m Gram matrices <e_i, e_j> of the error vectors
+ * (device); molecule b uses its leading k = min(d_count[b], m) rows and columns
+ * (d_count device int32; k = 0 writes zero coefficients).  d_coef (batch x m):
+ * c = x / sum(x) with B x = 1, i.e. REST's row sums of B^-1 over their total.
+ * Where B is exactly singular (a zero pivot of LU with partial pivoting, REST's
+ * _dinverse failure) or the result is not finite, d_status[b] = 1 and the
+ * coefficients are (1, 0, ..., 0): the caller restarts that history from its
+ * newest Fock matrix, stored in slot 0.  m <= 32, else RIJK_ERR_TOO_LARGE. */
+int rijk_diis_coefficients_dev(const double* d_gram, int64_t m, const int32_t* d_count, int64_t batch,
+                               double* d_coef, int32_t* d_status, void* stream);
 
 /* ---- J without any device allocation ----------------------------------------- */
 /* No counterpart in REST.  Same result as rijk_vj_upper_dev for callers that

@@ -76,6 +76,9 @@ SIGNATURES = {
     "rijk_group_jk_occ_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_double,
                                         C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p]),
     "rijk_group_synchronize": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "rijk_diis_coefficients_dev": (
+        C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p],
+    ),
     "rijk_eigh_batched_dev": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_double, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "rijk_ctx_selftest_timeout": (C.c_int, [_ctxp]),
@@ -107,6 +110,15 @@ SIGNATURES = {
         [_ctxp, C.c_void_p, C.c_int64, _i64p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p],
     ),
     "rijk_vk_upper_dm_dev": (C.c_int, [_ctxp, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
+    "rijk_vjk_upper_with_ri_v": (
+        C.c_int,
+        [_ctxp, C.c_void_p, C.c_int64, _i64p, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p],
+    ),
+    "rijk_vjk_upper_occ_dev": (
+        C.c_int,
+        [_ctxp, C.c_void_p, C.c_int64, _i64p, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+         C.c_void_p],
+    ),
     "rijk_vk_upper_occ_split_dev": (
         C.c_int,
         [_ctxp, C.c_void_p, C.c_int64, _i64p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p],

@@ -41,7 +41,7 @@ struct rijk_ctx {
   size_t dB_cap = 0;    // the allocation's size (it only grows: a smaller tensor reuses it)
   int* d_err = nullptr;   // device-side wait timeouts
   int* d_info = nullptr;  // Cholesky failing pivot
-  DevBuf stage, W, w, Jpart, Cw, X, Kpart, din, dout, docc, mV, mLinv, mT, mLinvd, mOut, Cr, Y, Yp;
+  DevBuf stage, W, w, Jpart, Jw, Cw, X, Kpart, din, dout, docc, mV, mLinv, mT, mLinvd, mOut, Cr, Y, Yp;
   // split-precision (tcgen05) state: BF16 hi/lo copies of the tensor, operands, partials
   DevBuf tcBhi, tcBlo, tcVhi, tcVlo, tcXhi, tcXlo, tcPart;
   int64_t tensor_version = 0, tc_version = -1;
@@ -344,9 +344,14 @@ int vj_dev(rijk_ctx* ctx, const double* d_dm, int spin, double scale, int mode, 
   return after_launch(ctx, "vj");
 }
 
-// ---- K, occupied-orbital form -------------------------------------------------
+// ---- K, occupied-orbital form (and J from the same half-transform) -------------
+// d_vj != nullptr: J of the densities D_s = C_s diag(occ_s) C_s^T as well.  The
+// half-transform's epilogue reduces w_P,s = <C_s diag(sqrt occ), X_P,s> =
+// B_P : D_s, which replaces J's first pass over the tensor; J's second pass
+// and finalisation follow the K chunks.
 int vk_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int64_t* homo, const double* d_occ,
-               int spin, double scale, double* d_out, cudaStream_t st) {
+               int spin, double scale, double* d_out, cudaStream_t st, double j_scale = 0.0,
+               double* d_vj = nullptr) {
   const Geom& g = ctx->g;
   int64_t nw[2] = {0, 0};
   for (int s = 0; s < spin; ++s) {
@@ -375,12 +380,23 @@ int vk_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int
   RIJK_TRY(ensure(ctx, ctx->Kpart, (size_t)splits_max * rijk::k_block_pairs(g, 0) * 128 * 128 * 8));
   double* X = static_cast<double*>(ctx->X.p);
   double* Kp = static_cast<double*>(ctx->Kpart.p);
+  double *jw = nullptr, *w = nullptr;
+  int jsplits = 0;
+  if (d_vj) {
+    jsplits = rijk::j_pass2_splits(g);
+    RIJK_TRY(ensure(ctx, ctx->Jw, (size_t)rijk::half_transform_warps(g, pchunk, ldx, ocols) * 2 * 8));
+    RIJK_TRY(ensure(ctx, ctx->w, (size_t)spin * g.naux * 8));
+    RIJK_TRY(ensure(ctx, ctx->Jpart, (size_t)jsplits * spin * g.ldB * 8));
+    jw = static_cast<double*>(ctx->Jw.p);
+    w = static_cast<double*>(ctx->w.p);
+  }
   for (int64_t p0 = 0; p0 < g.naux; p0 += pchunk) {
     const int64_t np = std::min(pchunk, g.naux - p0);
     const rijk::XMap xm{nw[0], (int)nw[0], (int)coff[1], spin == 2 ? (int)nw[1] : 0, np * nw[0], nw[1]};
     {
       ProfScope ps(ctx, RIJK_PROF_K_HALF, st);
-      rijk::launch_half_transform(g, ctx->dB, p0, np, Cw, ldx, ocols, ocols_valid, X, ldx, xm, ctx->d_err, st);
+      rijk::launch_half_transform(g, ctx->dB, p0, np, Cw, ldx, ocols, ocols_valid, X, ldx, xm, ctx->d_err, st, jw, w,
+                                  spin, spin == 2 ? (int)coff[1] : 1 << 30);
     }
     for (int s = 0; s < spin; ++s) {
       if (nw[s] == 0) continue;
@@ -394,7 +410,16 @@ int vk_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int
       rijk::launch_k_finalize(g, Kp, splits, 0, scale, p0 > 0 ? 1 : 0, 0, d_out + s * g.npair, st);
     }
   }
-  return after_launch(ctx, "vk occ");
+  if (d_vj) {
+    double* Jp = static_cast<double*>(ctx->Jpart.p);
+    {
+      ProfScope ps(ctx, RIJK_PROF_J_PASS2, st);
+      rijk::launch_j_pass2(g, ctx->dB, w, spin, jsplits, Jp, st);
+    }
+    ProfScope ps(ctx, RIJK_PROF_J_OTHER, st);
+    rijk::launch_j_finalize(g, Jp, spin, jsplits, j_scale, 0, d_vj, st);
+  }
+  return after_launch(ctx, d_vj ? "vjk occ" : "vk occ");
 }
 
 // ---- K, density form ----------------------------------------------------------
@@ -534,7 +559,7 @@ int rijk_ctx_destroy(rijk_ctx* ctx) {
   DevBuf* bufs[] = {&ctx->stage, &ctx->W,   &ctx->w,    &ctx->Jpart, &ctx->Cw,    &ctx->X,      &ctx->Kpart, &ctx->din,
                     &ctx->dout,  &ctx->docc, &ctx->mV, &ctx->mLinv, &ctx->mT, &ctx->mLinvd, &ctx->mOut,
                     &ctx->Cr,    &ctx->Y,    &ctx->Yp, &ctx->tcBhi, &ctx->tcBlo, &ctx->tcVhi, &ctx->tcVlo,
-                    &ctx->tcXhi, &ctx->tcXlo, &ctx->tcPart};
+                    &ctx->tcXhi, &ctx->tcXlo, &ctx->tcPart, &ctx->Jw};
   for (DevBuf* b : bufs) free_buf(ctx, *b);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto& r : ctx->prof_pending) {
@@ -949,6 +974,17 @@ int rijk_vk_upper_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state
                     pick(ctx, stream));
 }
 
+int rijk_vjk_upper_occ_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int64_t* homo,
+                           const double* d_occupation, int spin_channel, double j_scaling_factor,
+                           double k_scaling_factor, double* d_vj, double* d_vk, void* stream) {
+  RIJK_TRY(need_tensor(ctx));
+  RIJK_TRY(check_spin(ctx, spin_channel));
+  if (!d_eigv || !homo || !d_occupation || !d_vj || !d_vk || num_state <= 0 || d_vj == d_vk)
+    return set_err(ctx, RIJK_ERR_ARG, "bad argument");
+  return vk_occ_dev(ctx, d_eigv, num_state, homo, d_occupation, spin_channel, k_scaling_factor, d_vk,
+                    pick(ctx, stream), j_scaling_factor, d_vj);
+}
+
 int rijk_vk_upper_with_ri_v(rijk_ctx* ctx, const double* eigv, int64_t num_state, const int64_t* homo,
                             const double* occupation, int spin_channel, double scaling_factor, double* vk) {
   RIJK_TRY(need_tensor(ctx));
@@ -968,6 +1004,36 @@ int rijk_vk_upper_with_ri_v(rijk_ctx* ctx, const double* eigv, int64_t num_state
     return vk_occ_dev(ctx, din, num_state, homo, static_cast<double*>(ctx->docc.p), spin_channel, scaling_factor,
                       dout, ctx->stream);
   });
+}
+
+int rijk_vjk_upper_with_ri_v(rijk_ctx* ctx, const double* eigv, int64_t num_state, const int64_t* homo,
+                             const double* occupation, int spin_channel, double j_scaling_factor,
+                             double k_scaling_factor, double* vj, double* vk) {
+  RIJK_TRY(need_tensor(ctx));
+  RIJK_TRY(check_spin(ctx, spin_channel));
+  if (!eigv || !homo || !occupation || !vj || !vk || num_state <= 0) return set_err(ctx, RIJK_ERR_ARG, "bad argument");
+  for (int s = 0; s < spin_channel; ++s) {
+    if (homo[s] < 0 || homo[s] >= num_state) return set_err(ctx, RIJK_ERR_ARG, "homo out of range");
+    for (int64_t i = 0; i <= homo[s]; ++i)
+      if (!(occupation[s * num_state + i] >= 0.0)) return set_err(ctx, RIJK_ERR_ARG, "negative occupation");
+  }
+  const Geom& g = ctx->g;
+  const size_t ne = (size_t)spin_channel * g.n * num_state;
+  const size_t per = (size_t)spin_channel * g.npair;
+  RIJK_TRY(ensure(ctx, ctx->docc, (size_t)spin_channel * num_state * 8));
+  RIJK_CK(cudaMemcpyAsync(ctx->docc.p, occupation, (size_t)spin_channel * num_state * 8, cudaMemcpyHostToDevice,
+                          ctx->stream));
+  // J and K land side by side in the output staging buffer
+  RIJK_TRY(ensure(ctx, ctx->din, ne * 8));
+  RIJK_TRY(ensure(ctx, ctx->dout, 2 * per * 8));
+  double* din = static_cast<double*>(ctx->din.p);
+  double* dout = static_cast<double*>(ctx->dout.p);
+  RIJK_CK(cudaMemcpyAsync(din, eigv, ne * 8, cudaMemcpyHostToDevice, ctx->stream));
+  RIJK_TRY(vk_occ_dev(ctx, din, num_state, homo, static_cast<double*>(ctx->docc.p), spin_channel, k_scaling_factor,
+                      dout + per, ctx->stream, j_scaling_factor, dout));
+  RIJK_CK(cudaMemcpyAsync(vj, dout, per * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  RIJK_CK(cudaMemcpyAsync(vk, dout + per, per * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_and_check(ctx, ctx->stream);
 }
 
 int rijk_vk_upper_dm_dev(rijk_ctx* ctx, const double* d_dm, int spin_channel, double scaling_factor, double* d_vk,
@@ -1246,7 +1312,8 @@ int rijk_group_create(rijk_ctx* const* ctxs, int count, const int64_t* nocc, int
     d.nkb = cdiv(g.n, 128);
     d.pairs = d.nkb * (d.nkb + 1) / 2;
     d.npair = g.npair;
-    const int64_t counts[6] = {d.ldx * d.ocols + g.ldB, g.naux, g.naux * (d.ldx / BM) * (d.ocols / BN),
+    d.wper = (int)((d.ldx / BM) * (d.ocols / BN) * rijk::group_cta_warps(half_transform_cfg));
+    const int64_t counts[6] = {d.ldx * d.ocols, g.naux, g.naux * (d.ldx / BM) * (d.ocols / BN),
                                (int64_t)d.ksplits * d.pairs * subs, (int64_t)d.jsplits * cdiv(g.ldB / 2, 256),
                                g.npair};
     for (int ph = 0; ph < 6; ++ph) {
@@ -1254,7 +1321,7 @@ int rijk_group_create(rijk_ctx* const* ctxs, int count, const int64_t* nocc, int
       tot[ph] += counts[ph];
     }
     mol_off[m] = off;
-    off += round_up(d.ldx * d.ocols * 8, 256) + round_up(g.ldB * 8, 256) + round_up(g.naux * 8, 256) +
+    off += round_up(d.ldx * d.ocols * 8, 256) + round_up(g.naux * d.wper * 8, 256) + round_up(g.naux * 8, 256) +
            round_up((int64_t)d.jsplits * g.ldB * 8, 256) + round_up((g.naux * nocc[m] + rijk::TS) * d.ldx * 8, 256) +
            round_up((int64_t)d.ksplits * d.pairs * 128 * 128 * 8, 256);
   }
@@ -1274,7 +1341,7 @@ int rijk_group_create(rijk_ctx* const* ctxs, int count, const int64_t* nocc, int
       return reinterpret_cast<double*>(r);
     };
     d.Cw = take(d.ldx * d.ocols * 8);
-    d.W = take(g.ldB * 8);
+    d.wpart = take(g.naux * d.wper * 8);
     d.w = take(g.naux * 8);
     d.Jpart = take((int64_t)d.jsplits * g.ldB * 8);
     d.X = take((g.naux * d.nocc + rijk::TS) * d.ldx * 8);

@@ -82,9 +82,14 @@ struct XMap {
 // X_p = B_{p0+p} * W for p in [0, np): W is ldw x ncol (ncol a multiple of 64);
 // ldx = round_up(n, 128); the columns land where xm says.  Columns at or beyond
 // ncol_valid of W are zero and their fragments are skipped.
+// With wpart (scratch of 2 doubles per consumer warp, half_transform_warps of
+// them) the launch also writes J's scalars w[s][p0 + p] = B_p : D_s for the aux
+// rows of the chunk (D_s = W_s W_s^T; spin 1 = the columns from coff1 on).
+int64_t half_transform_warps(const Geom& g, int64_t np, int64_t ldx, int64_t ncol);
 void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
                            int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, const XMap& xm, int* err,
-                           cudaStream_t st);
+                           cudaStream_t st, double* wpart = nullptr, double* w = nullptr, int nspin = 1,
+                           int coff1 = 1 << 30);
 // Kpart[split][q] (128x128 blocks q over block pairs) = sum over the aux rows p
 // of the split of X_p X_p^T, where X holds X_p's nw columns at columns
 // [p nw, (p + 1) nw) (leading dimension ldx; the 32 columns after the last row
@@ -133,7 +138,8 @@ struct GroupMol {
   double* Cw;       // sqrt(2) C, ldx x ocols, column-major
   int64_t ldx;
   int ocols;        // a multiple of the half-transform CTA width
-  double* W;        // J weights (ldB)
+  double* wpart;    // J scalars per half-transform warp: naux x (ldx / BM) x (ocols / BN) x warps
+  int wper;         // wpart entries per aux row
   double* w;        // J scalars (naux)
   double* Jpart;    // jsplits x ldB
   int jsplits;
@@ -154,6 +160,7 @@ struct GroupPlan {
 int group_cta_rows(int cfg);
 int group_cta_cols(int cfg);
 int group_rank_subs(int cfg);
+int group_cta_warps(int cfg);
 // out[m] (ldo-strided, full and symmetric) = J(2 C_m C_m^T) + k_scale K(C_m) for
 // every molecule m with active[m] != 0; molecule m's orbitals C(mu, i) at
 // C0[m c_mol + mu c_row + i c_col] (occupation 2 for i < nocc).

@@ -439,12 +439,18 @@ struct LastTileK {
 // one row block run back to back and share its B tiles in L2.
 // XF > 0: the CTAs of the last column block (cb == ncb - 1) also compute the
 // XF * 8 remainder columns from xcol0 on (see ExtraCols).
+// wpart != nullptr: also J's scalars.  Consumer warp k of CTA bid writes its
+// share of w_P,s = <W_s, X_P,s> = sum over its outputs of X_P[m, c] W[m, c]
+// (W = C scaled by sqrt(occ), zero padded, so w_P,s = B_P : D_s with
+// D_s = W_s W_s^T) to wpart[2 (bid CWARPS + k) + s]; s = 0 for the columns
+// below coff1, else 1.
 template <class Cfg, int XF = 0>
 __global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_half_transform(const double* __restrict__ B, int64_t ldB, int64_t p0,
                                                                  int nrb, int ncb, const double* __restrict__ W,
                                                                  int64_t ldw, int n, int nt, int ncol_valid,
                                                                  double* __restrict__ X, int64_t ldx, XMap xm,
-                                                                 int* err, int xcol0) {
+                                                                 int* err, int xcol0, double* __restrict__ wpart,
+                                                                 int coff1) {
   extern __shared__ __align__(128) double smem[];
   const int64_t bid = blockIdx.x;
   const int cb = (int)(bid % ncb);
@@ -484,25 +490,105 @@ __global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_half_transfor
         }
     }
   }
+  if (wpart) {
+    // this warp's share of <W, X_P> per spin
+    double s0 = 0.0, s1 = 0.0;
+    const double* Wr = W + (int64_t)I0 * TS;
+    dmma_for_each<Cfg>(acc, [&](int m, int c, double v0, double v1) {
+      const int c0 = col0 + c;
+      const double t0 = v0 * Wr[m + (int64_t)c0 * ldw], t1 = v1 * Wr[m + (int64_t)(c0 + 1) * ldw];
+      if (c0 < coff1) s0 += t0; else s1 += t0;
+      if (c0 + 1 < coff1) s0 += t1; else s1 += t1;
+    });
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if constexpr (XF > 0) {
+      if (xc.on) {
+        const int wm = warp / Cfg::WN, wn = warp % Cfg::WN;
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+#pragma unroll
+          for (int j = 0; j < XF; ++j) {
+            const int m = wm * Cfg::WTM + (wn * 2 + e) * 8 + (lane >> 2);
+            const int c = xcol0 + 8 * j + 2 * (lane & 3);
+            const double t0 = xc.acc[e][j][0] * Wr[m + (int64_t)c * ldw];
+            const double t1 = xc.acc[e][j][1] * Wr[m + (int64_t)(c + 1) * ldw];
+            if (c < coff1) s0 += t0; else s1 += t0;
+            if (c + 1 < coff1) s0 += t1; else s1 += t1;
+          }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    }
+    if (lane == 0) {
+      wpart[2 * (bid * Cfg::CWARPS + warp)] = s0;
+      wpart[2 * (bid * Cfg::CWARPS + warp) + 1] = s1;
+    }
+  }
 }
+
+// w[s][p0 + p] = the sum, in a fixed order, of the per_row warp shares of aux
+// row p (one warp per row).
+__global__ void __launch_bounds__(256) k_j_wreduce(const double* __restrict__ wpart, int64_t np, int per_row,
+                                                   int nspin, int64_t naux, int64_t p0, double* __restrict__ w) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t pl = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; pl < np;
+       pl += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const double* src = wpart + pl * per_row * 2;
+    double a = 0.0, b = 0.0;
+    for (int t = lane; t < per_row; t += 32) {
+      a += src[2 * t];
+      b += src[2 * t + 1];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) {
+      w[p0 + pl] = a;
+      if (nspin == 2) w[naux + p0 + pl] = b;
+    }
+  }
+}
+
+void launch_j_wreduce(const double* wpart, int64_t np, int per_row, int nspin, int64_t naux, int64_t p0, double* w,
+                      cudaStream_t st) {
+  const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(np, 8), 148 * 8));
+  count_launch();
+  k_j_wreduce<<<blocks, 256, 0, st>>>(wpart, np, per_row, nspin, naux, p0, w);
+}
+
+// J scalars requested by the caller of launch_half_transform (see JFuse).
+struct JFuse {
+  double* wpart;  // scratch, 2 doubles per CTA
+  double* w;      // [spin][naux]
+  int nspin, coff1;
+  int64_t naux;
+};
 
 template <class Cfg, int XF = 0>
 static void half_transform_launch(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W,
                                   int64_t ldw, int ncb, int64_t ncol_valid, double* X, int64_t ldx, const XMap& xm,
-                                  int* err, int xcol0, cudaStream_t st) {
+                                  int* err, int xcol0, const JFuse* jf, cudaStream_t st) {
   cudaFuncSetAttribute(k_half_transform<Cfg, XF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)Cfg::SMEM_BYTES);
   const int nrb = (int)(ldx / Cfg::BM);
+  double* wpart = jf ? jf->wpart : nullptr;
   count_launch();
   k_half_transform<Cfg, XF><<<(unsigned)(np * nrb * ncb), Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(
-      B, g.ldB, p0, nrb, ncb, W, ldw, (int)g.n, (int)g.nt, (int)ncol_valid, X, ldx, xm, err, xcol0);
+      B, g.ldB, p0, nrb, ncb, W, ldw, (int)g.n, (int)g.nt, (int)ncol_valid, X, ldx, xm, err, xcol0, wpart,
+      jf ? jf->coff1 : 1 << 30);
+  if (wpart) launch_j_wreduce(wpart, np, nrb * ncb * Cfg::CWARPS, jf->nspin, jf->naux, p0, jf->w, st);
 }
 
 template <class Cfg>
 static void half_transform_cfg(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
                                int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, const XMap& xm, int* err,
-                               cudaStream_t st) {
-  half_transform_launch<Cfg>(g, B, p0, np, W, ldw, (int)(ncol / Cfg::BN), ncol_valid, X, ldx, xm, err, 0, st);
+                               const JFuse* jf, cudaStream_t st) {
+  half_transform_launch<Cfg>(g, B, p0, np, W, ldw, (int)(ncol / Cfg::BN), ncol_valid, X, ldx, xm, err, 0, jf, st);
 }
 
 // The default shape: when the valid columns end at most 16 past a multiple of
@@ -511,28 +597,42 @@ static void half_transform_cfg(const Geom& g, const double* B, int64_t p0, int64
 template <>
 void half_transform_cfg<HtCfg1>(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W,
                                 int64_t ldw, int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx,
-                                const XMap& xm, int* err, cudaStream_t st) {
+                                const XMap& xm, int* err, const JFuse* jf, cudaStream_t st) {
   const int64_t full = ncol_valid / HtCfg1::BN, rem = ncol_valid - full * HtCfg1::BN;
   const int xcol0 = (int)(full * HtCfg1::BN);
   if (full >= 1 && rem > 0 && rem <= 8)
     return half_transform_launch<HtCfg1, 1>(g, B, p0, np, W, ldw, (int)full, ncol_valid, X, ldx, xm, err, xcol0,
-                                            st);
+                                            jf, st);
   if (full >= 1 && rem > 8 && rem <= 16)
     return half_transform_launch<HtCfg1, 2>(g, B, p0, np, W, ldw, (int)full, ncol_valid, X, ldx, xm, err, xcol0,
-                                            st);
-  half_transform_launch<HtCfg1>(g, B, p0, np, W, ldw, (int)(ncol / HtCfg1::BN), ncol_valid, X, ldx, xm, err, 0, st);
+                                            jf, st);
+  half_transform_launch<HtCfg1>(g, B, p0, np, W, ldw, (int)(ncol / HtCfg1::BN), ncol_valid, X, ldx, xm, err, 0, jf,
+                                st);
+}
+
+int64_t half_transform_warps(const Geom& g, int64_t np, int64_t ldx, int64_t ncol) {
+  switch (g.ht_cfg) {
+    case 1: return np * (ldx / HtCfg1::BM) * (ncol / HtCfg1::BN) * HtCfg1::CWARPS;
+    case 2: return np * (ldx / HtCfg2::BM) * (ncol / HtCfg2::BN) * HtCfg2::CWARPS;
+    case 3: return np * (ldx / HtCfg3::BM) * (ncol / HtCfg3::BN) * HtCfg3::CWARPS;
+    case 4: return np * (ldx / HtCfg4::BM) * (ncol / HtCfg4::BN) * HtCfg4::CWARPS;
+    case 5: return np * (ldx / HtCfg5::BM) * (ncol / HtCfg5::BN) * HtCfg5::CWARPS;
+    default: return np * (ldx / HtCfg0::BM) * (ncol / HtCfg0::BN) * HtCfg0::CWARPS;
+  }
 }
 
 void launch_half_transform(const Geom& g, const double* B, int64_t p0, int64_t np, const double* W, int64_t ldw,
                            int64_t ncol, int64_t ncol_valid, double* X, int64_t ldx, const XMap& xm, int* err,
-                           cudaStream_t st) {
+                           cudaStream_t st, double* wpart, double* w, int nspin, int coff1) {
+  JFuse jfs{wpart, w, nspin, coff1, g.naux};
+  const JFuse* jf = wpart ? &jfs : nullptr;
   switch (g.ht_cfg) {
-    case 1: return half_transform_cfg<HtCfg1>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, st);
-    case 2: return half_transform_cfg<HtCfg2>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, st);
-    case 3: return half_transform_cfg<HtCfg3>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, st);
-    case 4: return half_transform_cfg<HtCfg4>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, st);
-    case 5: return half_transform_cfg<HtCfg5>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, st);
-    default: return half_transform_cfg<HtCfg0>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, st);
+    case 1: return half_transform_cfg<HtCfg1>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, jf, st);
+    case 2: return half_transform_cfg<HtCfg2>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, jf, st);
+    case 3: return half_transform_cfg<HtCfg3>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, jf, st);
+    case 4: return half_transform_cfg<HtCfg4>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, jf, st);
+    case 5: return half_transform_cfg<HtCfg5>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, jf, st);
+    default: return half_transform_cfg<HtCfg0>(g, B, p0, np, W, ldw, ncol, ncol_valid, X, ldx, xm, err, jf, st);
   }
 }
 
@@ -793,9 +893,7 @@ __device__ __forceinline__ int group_find(const int64_t* __restrict__ pre, int c
   return lo;
 }
 
-// Phase 1: Cw = sqrt(2) C (ldx x ocols, zero padded) and the J weights W from
-// D = 2 C C^T folded onto the tile layout (REST's a2 weights: off-diagonal
-// tiles 2 D, diagonal tiles D; D symmetric).
+// Phase 1: Cw = sqrt(2) C (ldx x ocols, zero padded).
 __global__ void __launch_bounds__(256) k_grp_prepare(const GroupMol* __restrict__ mols, const int64_t* __restrict__ pre,
                                                      int count, int64_t total, const double* __restrict__ C0,
                                                      int64_t c_mol, int64_t c_row, int64_t c_col,
@@ -806,46 +904,9 @@ __global__ void __launch_bounds__(256) k_grp_prepare(const GroupMol* __restrict_
     const GroupMol& g = mols[m];
     const double* C = C0 + m * c_mol;
     const int64_t t = e - pre[m];
-    const int64_t ncw = g.ldx * g.ocols;
-    if (t < ncw) {
-      const int64_t row = t % g.ldx, col = t / g.ldx;
-      g.Cw[t] = (row < g.n && col < g.nocc) ? 1.4142135623730951 * C[row * c_row + col * c_col] : 0.0;
-    } else {
-      const int64_t k = t - ncw;
-      const int64_t tile = k >> 10;
-      const int rc = (int)(k & 1023), r = rc & 31, c = rc >> 5;
-      const int64_t J = tri_root(tile), I = tile - J * (J + 1) / 2;
-      const int64_t mu = I * TS + r, nu = J * TS + c;
-      double v = 0.0;
-      if (mu < g.n && nu < g.n) {
-        const int64_t i = mu < nu ? mu : nu, j = mu < nu ? nu : mu;
-        for (int o = 0; o < g.nocc; ++o) v = fma(C[i * c_row + o * c_col], C[j * c_row + o * c_col], v);
-        v *= (I < J ? 4.0 : 2.0);
-      }
-      g.W[k] = v;
-    }
+    const int64_t row = t % g.ldx, col = t / g.ldx;
+    g.Cw[t] = (row < g.n && col < g.nocc) ? 1.4142135623730951 * C[row * c_row + col * c_col] : 0.0;
   }
-}
-
-// Phase 2: w_P = B_P . W, one CTA per (molecule, aux row).
-__global__ void __launch_bounds__(256) k_grp_pass1(const GroupMol* __restrict__ mols, const int64_t* __restrict__ pre,
-                                                   int count, const int* __restrict__ active) {
-  const int m = group_find(pre, count, blockIdx.x);
-  if (!active[m]) return;
-  const GroupMol& g = mols[m];
-  const int64_t P = blockIdx.x - pre[m];
-  const double2* b = reinterpret_cast<const double2*>(g.B + P * g.ldB);
-  const double2* w0 = reinterpret_cast<const double2*>(g.W);
-  const int64_t nq = g.ldB / 2;
-  double s[1] = {0.0}, s2 = 0.0;
-  for (int64_t q = threadIdx.x; q < nq; q += 256) {
-    const double2 x = ld_stream(b + q);
-    const double2 a = __ldg(w0 + q);
-    s[0] = fma(x.x, a.x, s[0]);
-    s2 = fma(x.y, a.y, s2);
-  }
-  s[0] += s2;
-  block_reduce_store<1>(s, g.w + P, g.naux);
 }
 
 // Phase 3 (persistent): X_P = B_P Cw for every (molecule, aux row, row block, column block).
@@ -873,14 +934,40 @@ __global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_grp_half(cons
     __syncthreads();  // the previous item's warps are done with the stages
     if (dmma_mainloop<Cfg>(sc, ktiles, smem, acc, err, g.n - I0 * TS, g.nocc - col0, kv)) {
       double* Xr = g.X + (int64_t)I0 * TS;
+      const double* Wr = g.Cw + (int64_t)I0 * TS;
       const int64_t nw = g.nocc;
+      double s = 0.0;  // this warp's share of w_P = <Cw, X_P> = B_P : 2 C C^T
       dmma_for_each<Cfg>(acc, [&](int mm, int c, double v0, double v1) {
         const int64_t c0 = col0 + c;
         if (c0 < nw) Xr[mm + (pl * nw + c0) * g.ldx] = v0;
         if (c0 + 1 < nw) Xr[mm + (pl * nw + c0 + 1) * g.ldx] = v1;
+        s = fma(v0, Wr[mm + c0 * g.ldx], s);
+        s = fma(v1, Wr[mm + (c0 + 1) * g.ldx], s);
       });
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if ((threadIdx.x & 31) == 0) g.wpart[bid * Cfg::CWARPS + (threadIdx.x >> 5)] = s;
     }
   }
+}
+
+// Phase 2 (after phase 3): w_P = the warp shares of aux row P summed in a fixed
+// order, one warp per (molecule, aux row).
+__global__ void __launch_bounds__(256) k_grp_wreduce(const GroupMol* __restrict__ mols,
+                                                     const int64_t* __restrict__ pre, int count, int64_t total,
+                                                     const int* __restrict__ active) {
+  const int64_t it = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (it >= total) return;
+  const int m = group_find(pre, count, it);
+  if (!active[m]) return;
+  const GroupMol& g = mols[m];
+  const int64_t P = it - pre[m];
+  const double* src = g.wpart + P * g.wper;
+  double a = 0.0;
+  for (int t = threadIdx.x & 31; t < g.wper; t += 32) a += src[t];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & 31) == 0) g.w[P] = a;
 }
 
 // Phase 4 (persistent): Kpart = sum_p X_p X_p^T per (molecule, upper K sub-block, split).
@@ -990,6 +1077,7 @@ static void grp_rank_cfg(const GroupMol* mols, const int64_t* pre, int count, in
 int group_cta_rows(int cfg) { return cfg == 4 ? 128 : 64; }
 int group_cta_cols(int cfg) { return 64; }
 int group_rank_subs(int cfg) { return cfg == 4 ? 2 : 4; }
+int group_cta_warps(int cfg) { return cfg == 4 ? HtCfg4::CWARPS : cfg == 0 ? HtCfg0::CWARPS : HtCfg1::CWARPS; }
 
 void launch_group(const GroupPlan& gp, const double* C0, int64_t c_mol, int64_t c_row, int64_t c_col, double k_scale,
                   double* out0, int64_t out_mol, int64_t ldo, const int* active, int* err, int sms, cudaStream_t st) {
@@ -999,13 +1087,13 @@ void launch_group(const GroupPlan& gp, const double* C0, int64_t c_mol, int64_t 
     count_launch();
     k_grp_prepare<<<blocks, 256, 0, st>>>(gp.mols, gp.pre[0], n, gp.total[0], C0, c_mol, c_row, c_col, active);
   }
-  count_launch();
-  k_grp_pass1<<<(unsigned)gp.total[1], 256, 0, st>>>(gp.mols, gp.pre[1], n, active);
   switch (gp.ht_cfg) {
     case 0: grp_half_cfg<HtCfg0>(gp.mols, gp.pre[2], n, gp.total[2], active, err, sms, st); break;
     case 4: grp_half_cfg<HtCfg4>(gp.mols, gp.pre[2], n, gp.total[2], active, err, sms, st); break;
     default: grp_half_cfg<HtCfg1>(gp.mols, gp.pre[2], n, gp.total[2], active, err, sms, st); break;
   }
+  count_launch();
+  k_grp_wreduce<<<(unsigned)cdiv(gp.total[1], 8), 256, 0, st>>>(gp.mols, gp.pre[1], n, gp.total[1], active);
   switch (gp.rk_cfg) {
     case 0: grp_rank_cfg<RkCfg0>(gp.mols, gp.pre[3], n, gp.total[3], active, err, sms, st); break;
     case 4: grp_rank_cfg<RkCfg4>(gp.mols, gp.pre[3], n, gp.total[3], active, err, sms, st); break;

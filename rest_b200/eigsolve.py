@@ -122,3 +122,29 @@ def eigh_batched(A, nvalid, pad_value: float = 1.0e6):
     if st != 0:
         raise RijkError(st, "batched eigensolver")
     return lam, V, info == 0
+
+
+def diis_coefficients(gram, count):
+    """REST's diis_solver for a batch (rijk_diis_coefficients_dev): gram is
+    B x m x m (FP64, device), count[b] the history length of molecule b (its
+    leading min(count, m) slots are used).  Returns (coef B x m, failed B bool):
+    a molecule whose Gram matrix is exactly singular gets (1, 0, ..., 0) and
+    failed = True, and its caller restarts the history from slot 0."""
+    import ctypes as C
+
+    import torch
+
+    from ._abi import RijkError, lib
+
+    B, m, _ = gram.shape
+    dev = gram.device
+    g = gram.contiguous()
+    cnt = torch.as_tensor(count, dtype=torch.int32, device=dev)
+    coef = torch.empty(B, m, dtype=torch.float64, device=dev)
+    status = torch.empty(B, dtype=torch.int32, device=dev)
+    st = lib().rijk_diis_coefficients_dev(C.c_void_p(g.data_ptr()), m, C.c_void_p(cnt.data_ptr()), B,
+                                          C.c_void_p(coef.data_ptr()), C.c_void_p(status.data_ptr()),
+                                          C.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    if st != 0:
+        raise RijkError(st, "batched DIIS coefficients")
+    return coef, status != 0

@@ -265,6 +265,25 @@ class RIJK:
         p = self.npair
         return _rest_list([out[s * p:(s + 1) * p].copy() for s in range(spin_channel)])
 
+    def vjk_upper_with_ri_v(self, eigv, homo, occupation, spin_channel: int, j_scaling_factor: float,
+                            k_scaling_factor: float):
+        """J and K of REST ``generate_hf_hamiltonian_ri_v`` (scf_io/mod.rs:1339-1381)
+        in one build: (vj, vk) with vj of dm_s = C_s diag(occ_s) C_s^T (the
+        states up to homo) and vk as ``vk_upper_with_ri_v``."""
+        n = self.num_basis
+        num_state = np.asarray(eigv[0]).shape[1]
+        c = _stack_spin(eigv, spin_channel, (n, num_state))
+        occ = np.ascontiguousarray(np.stack([_f64(occupation[s])[:num_state] for s in range(spin_channel)]))
+        hm = (C.c_int64 * 2)(*[int(homo[s]) if s < spin_channel else 0 for s in range(2)])
+        vj = np.empty(spin_channel * self.npair)
+        vk = np.empty(spin_channel * self.npair)
+        self._check(lib().rijk_vjk_upper_with_ri_v(self._h, _ptr(c), num_state, hm, _ptr(occ), spin_channel,
+                                                   float(j_scaling_factor), float(k_scaling_factor), _ptr(vj),
+                                                   _ptr(vk)))
+        p = self.npair
+        return (_rest_list([vj[s * p:(s + 1) * p].copy() for s in range(spin_channel)]),
+                _rest_list([vk[s * p:(s + 1) * p].copy() for s in range(spin_channel)]))
+
     def _vk_dm(self, fn, dm, spin_channel, scaling_factor, full=False):
         n = self.num_basis
         d = _stack_spin(dm, spin_channel, (n, n))
@@ -299,6 +318,16 @@ class RIJK:
         self._check(lib().rijk_vk_upper_occ_dev(self._h, C.c_void_p(d_eigv), num_state, hm, C.c_void_p(d_occ),
                                                 spin_channel, float(scaling_factor), C.c_void_p(d_vk),
                                                 C.c_void_p(stream or None)))
+
+    def vjk_upper_occ_dev(self, d_eigv: int, num_state: int, homo, d_occ: int, spin_channel: int,
+                          j_scaling_factor: float, k_scaling_factor: float, d_vj: int, d_vk: int, stream: int = 0):
+        """J of dm_s = C_s diag(occ_s) C_s^T and the occupied-orbital K in one
+        build (REST generate_hf_hamiltonian_ri_v, scf_io/mod.rs:1339-1381): J's
+        aux-row scalars come out of the K half-transform."""
+        hm = (C.c_int64 * 2)(*[int(homo[s]) if s < spin_channel else 0 for s in range(2)])
+        self._check(lib().rijk_vjk_upper_occ_dev(self._h, C.c_void_p(d_eigv), num_state, hm, C.c_void_p(d_occ),
+                                                 spin_channel, float(j_scaling_factor), float(k_scaling_factor),
+                                                 C.c_void_p(d_vj), C.c_void_p(d_vk), C.c_void_p(stream or None)))
 
     def vk_upper_dm_dev(self, d_dm: int, spin_channel: int, scaling_factor: float, d_vk: int, stream: int = 0):
         self._check(lib().rijk_vk_upper_dm_dev(self._h, C.c_void_p(d_dm), spin_channel, float(scaling_factor),

@@ -9,20 +9,28 @@ stream), and the SCF iterations of the whole set advance together:
                of host threads (``setup_workers``), each with its own stream, so
                that one molecule's host-side plan and one-electron integrals
                overlap the others' device work;
-  J / K        per molecule through the device entry points (rijk_vj_upper_dev,
-               rijk_vk_upper_occ_dev or the split-precision tcgen05 forms), the
-               molecules' launches overlapping on their streams;
+  J / K        FP64 builds of a group of molecules (``grouped``) by the
+               library's grouped build (rijk_group_jk_occ_dev: six launches for
+               all of them, captured once in a CUDA graph and replayed every
+               iteration with the converged molecules switched off); otherwise
+               per molecule through the device entry points
+               (rijk_vjk_upper_occ_dev, which takes J from the K half-transform,
+               or the split-precision tcgen05 forms), the molecules' launches
+               overlapping on their streams;
   Fock, DIIS   on the device for the padded batch: F = h + J + K, the error
                vectors F D S - S D F of REST's DIIS (src/scf_io/mod.rs:3094-3136)
                kept as a batched history, the B matrices of diis_solver
-               (:3138-3188) formed in one batched product and solved per molecule;
+               (:3138-3188) formed in one batched product and solved for all
+               molecules by one launch (rijk_diis_coefficients_dev);
   diagonalise  the generalised eigenproblem F C = S C e of diagonalize_hamiltonian
                (:1843-1873) in the standard form X^T F X with X = L^-T from the
                Cholesky factor S = L L^T (the reduction of REST's LAPACK dspgvx),
                padding rows pushed to the top of the spectrum; each molecule's
                eigenbasis from the previous iteration is refined by matrix
                products (eigsolve.refine), and molecules where that does not
-               pass take a batched cuSOLVER eigensolve;
+               pass take the library's batched eigensolver
+               (rijk_eigh_batched_dev; cuSOLVER for a matrix it does not
+               converge or one beyond its size limit);
   density      D = 2 C_occ C_occ^T on the device.
 
 Precision of the exchange build:
@@ -51,7 +59,7 @@ import numpy as np
 from .basis import DEVICE_MAX_L_AO, DEVICE_MAX_L_AUX, int1e, int1e_nuclear_dev, int2c2e, int2c2e_dev, int3c2e
 from .geometry import alkane, water_cluster  # noqa: F401  (re-exported)
 from .rijk import RIJK, RIJKGroup, group_tiles
-from .eigsolve import eigh_batched, refine
+from .eigsolve import diis_coefficients, eigh_batched, refine
 from .scf import metric_inv_sqrt, metric_inv_sqrt_dev
 
 
@@ -435,14 +443,12 @@ class BatchedRHF:
             npair = n * (n + 1) // 2
 
             def body():
-                c = self._gC[i, :n, :o]
-                d = 2.0 * (c @ c.T)
-                c_cm = c.T.contiguous()
+                c_cm = self._gC[i, :n, :o].T.contiguous()
                 vj = torch.empty(npair, dtype=torch.float64, device=self.dev)
                 vk = torch.empty(npair, dtype=torch.float64, device=self.dev)
-                ctx.vj_upper_dev(d.data_ptr(), 1, 1.0, 1, vj.data_ptr(), st.cuda_stream)
-                ctx.vk_upper_occ_dev(c_cm.data_ptr(), o, [o - 1], self._gocc.data_ptr(), 1, -0.5, vk.data_ptr(),
-                                     st.cuda_stream)
+                # J of D = 2 C C^T and K from one build (J's scalars from the K half-transform)
+                ctx.vjk_upper_occ_dev(c_cm.data_ptr(), o, [o - 1], self._gocc.data_ptr(), 1, 1.0, -0.5,
+                                      vj.data_ptr(), vk.data_ptr(), st.cuda_stream)
                 self._gout[i, :n, :n] = self._upper_to_full(vj + vk, n)
 
             st.wait_stream(torch.cuda.current_stream())
@@ -540,11 +546,14 @@ class BatchedRHF:
             st.wait_event(ev)
             with torch.cuda.stream(st):
                 c = C[i, :n, :o]
-                d = 2.0 * (c @ c.T)
                 npair = n * (n + 1) // 2
                 vj = torch.empty(npair, dtype=torch.float64, device=self.dev)
-                ctx.vj_upper_dev(d.contiguous().data_ptr(), 1, 1.0, 1, vj.data_ptr(), ctx.stream)
-                keep = [d, vj]
+                keep = [vj]
+                fused = not incr[i] and self.precision != "split"
+                if not fused:
+                    d = (2.0 * (c @ c.T)).contiguous()
+                    ctx.vj_upper_dev(d.data_ptr(), 1, 1.0, 1, vj.data_ptr(), ctx.stream)
+                    keep.append(d)
                 if incr[i]:
                     vk = self._kref[i].clone()
                     V, npos = factors[i]
@@ -567,8 +576,9 @@ class BatchedRHF:
                                                    vk.data_ptr(), ctx.stream)
                         self._nsplit[i] += 1
                     else:
-                        ctx.vk_upper_occ_dev(c_cm.data_ptr(), o, [o - 1], occ.data_ptr(), 1, -0.5, vk.data_ptr(),
-                                             ctx.stream)
+                        # J of D = 2 C C^T and K from one build
+                        ctx.vjk_upper_occ_dev(c_cm.data_ptr(), o, [o - 1], occ.data_ptr(), 1, 1.0, -0.5,
+                                              vj.data_ptr(), vk.data_ptr(), ctx.stream)
                         self._nfp64[i] += 1
                         self._streak[i] += 1
                     self._split_steps[i] = 0
@@ -713,28 +723,19 @@ class BatchedRHF:
             for i in range(B):
                 if active[i]:
                     count[i] += 1
-            bm = (err_hist @ err_hist.transpose(1, 2)).cpu().numpy()
-            coef = np.zeros((B, m))
-            for i in range(B):
-                k = min(count[i], m)
-                if not active[i] or k == 0:
-                    continue
-                try:
-                    binv = np.linalg.inv(bm[i, :k, :k])
-                    if not np.all(np.isfinite(binv)):
-                        raise np.linalg.LinAlgError
-                    coef[i, :k] = binv.sum(axis=1) / binv.sum()
-                except np.linalg.LinAlgError:
-                    # singular B: restart the history from the newest Fock matrix
-                    last = (count[i] - 1) % m
-                    err_hist[i, 0] = err_hist[i, last].clone()
-                    f_hist[i, 0] = f_hist[i, last].clone()
-                    err_hist[i, 1:] = 0.0
-                    f_hist[i, 1:] = 0.0
-                    count[i] = 1
-                    coef[i, 0] = 1.0
+            bm = err_hist @ err_hist.transpose(1, 2)
+            # REST's diis_solver per molecule, on the device (rijk_diis_coefficients_dev)
+            coef, failed = diis_coefficients(bm, [count[i] if active[i] else 0 for i in range(B)])
+            for i in torch.nonzero(failed).flatten().tolist():
+                # singular B: restart the history from the newest Fock matrix (coefficients (1, 0, ...))
+                last = (count[i] - 1) % m
+                err_hist[i, 0] = err_hist[i, last].clone()
+                f_hist[i, 0] = f_hist[i, last].clone()
+                err_hist[i, 1:] = 0.0
+                f_hist[i, 1:] = 0.0
+                count[i] = 1
             tb = time.perf_counter()
-            Fx = torch.einsum("bm,bmij->bij", torch.as_tensor(coef, device=self.dev), f_hist)
+            Fx = torch.einsum("bm,bmij->bij", coef, f_hist)
             Fx = torch.where(act[:, None, None], Fx, F)
             e, C = diag(Fx, [i for i in range(B) if active[i]])
             tc = time.perf_counter()
