@@ -670,15 +670,16 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
     return res
 
 
-# DRAM traffic of the half-transform per launch.  ncu at n=600 (N=2400, one
-# launch over all aux rows; profiles/k_half_transform_rank_update_n600.md)
-# measured dram read 3.7407 GB + write 1.2123 GB = 4.9529 GB, which is 0.9977
-# of the bytes the launch must move: the tile-packed tensor rows it reads plus
-# the X rows it writes (ldx x nocc per aux row).  The n=1200 tensor (29 GB) is
-# too large to capture under a multi-pass ncu run, so its traffic is that ratio
-# times the same byte count for the rows of one n=1200 launch.
-TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_half_transform at n=600 "
-                  "(0.9977 of tensor rows read + X rows written), scaled to this launch's rows and sizes")
+# DRAM traffic of the half-transform per launch.  ncu at n=600, nocc=72 (N=2400,
+# one launch over all aux rows, the fused form with remainder columns;
+# profiles/k_half_transform_rank_update_n600.md) measured dram read 3.8403 GB +
+# write 0.9461 GB = 4.7865 GB, which is 1.036 of the bytes the launch must move:
+# the tile-packed tensor rows it reads plus the X rows it writes (ldx x nocc per
+# aux row).  The n=1200 tensor (29 GB) is too large to capture under a
+# multi-pass ncu run, so its traffic is that ratio times the same byte count for
+# the rows of one n=1200 launch.
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_half_transform at n=600, nocc=72 "
+                  "(1.036 of tensor rows read + X rows written), scaled to this launch's rows and sizes")
 
 
 def half_transform_bytes(n: int, nocc: int, rows: float) -> float:
@@ -690,7 +691,7 @@ def half_transform_bytes(n: int, nocc: int, rows: float) -> float:
     return rows * 8.0 * (ldb + ldx * nocc)
 
 
-TRAFFIC_RATIO_K_HALF = 4.9529e9 / half_transform_bytes(600, 100, 2400)
+TRAFFIC_RATIO_K_HALF = 4.7865e9 / half_transform_bytes(600, 72, 2400)
 
 
 def traffic_per_launch(kernel: str, w: dict, launches: int):
