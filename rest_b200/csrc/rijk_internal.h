@@ -112,6 +112,8 @@ struct TcGeom {
   int npad = 0;  // column count padded to 64 / 128 / 256
   int nib = 0;   // npad / 64
   int64_t block_elems = 0;
+  int pair = 0;       // half-transform on SM pairs (cta_group::2); V stored in column halves
+  int pair_rank = 0;  // rank update on SM pairs (cta_group::2)
 };
 TcGeom make_tc_geom(const Geom& g, int ncols);
 // BF16 elements of one plane (hi or lo) of the split tensor

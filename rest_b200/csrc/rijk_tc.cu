@@ -32,6 +32,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -187,18 +188,23 @@ __global__ void __launch_bounds__(256) k_split_tensor(const double* __restrict__
 }
 
 // Vs[kb] (hi, lo): columns of V (n x ncols, column-major, ld) as the B operand
-// of the half-transform, N = npad rows (columns of V), K = kappa.
+// of the half-transform, N = npad rows (columns of V), K = kappa.  With
+// halves = 2 each K block is two (npad/2 x 64) K-major blocks, columns
+// [0, npad/2) then [npad/2, npad): the two CTAs of a paired launch copy one each.
 __global__ void __launch_bounds__(256) k_split_cols(const double* __restrict__ V, int64_t ldv, int64_t n,
-                                                    int ncols, int npad, int nkb, __nv_bfloat16* __restrict__ hi,
-                                                    __nv_bfloat16* __restrict__ lo) {
+                                                    int ncols, int npad, int nkb, int halves,
+                                                    __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
   const int64_t per_kb = (int64_t)npad * TC_KB;
   const int64_t total = per_kb * nkb;
+  const int rows = npad / halves;  // rows of one K-major block
+  const int64_t per_half = (int64_t)rows * TC_KB;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int kb = (int)(e / per_kb);
-    const int o = (int)(e - kb * per_kb);
+    const int oo = (int)(e - kb * per_kb);
+    const int half = (int)(oo / per_half), o = (int)(oo - half * per_half);
     const int within = o & 63, core = o >> 6;
-    const int i = ((core % (npad / 8)) << 3) | (within >> 3);
-    const int k = ((core / (npad / 8)) << 3) | (within & 7);
+    const int i = half * rows + (((core % (rows / 8)) << 3) | (within >> 3));
+    const int k = ((core / (rows / 8)) << 3) | (within & 7);
     const int64_t ka = (int64_t)kb * TC_KB + k;
     const double x = (i < ncols && ka < n) ? V[ka + ldv * i] : 0.0;
     __nv_bfloat16 h, l;
@@ -393,6 +399,288 @@ __global__ void __launch_bounds__(192, 1)
   if (warp == 0) tc_dealloc(tmem, 2 * NPAD);
 }
 
+// ---- paired half-transform: one M = 256 MMA over two SMs (cta_group::2) -----------
+// The persistent kernel above streams all of V (n_pad x npad, hi and lo) from
+// L2 again for every 128-row tile: two thirds of each stage.  Here a cluster of
+// two CTAs runs one tcgen05.mma.cta_group::2 with M = 256: CTA r supplies the A
+// rows of aux row P0 + r (same row block mb, so both take the same mirrored or
+// direct reading of the same square position) and half r of V's columns, and
+// each CTA's tensor memory receives its own 128 rows x npad columns.  Per SM a
+// stage is then A (32 KB) + half of V, and V crosses from L2 once per pair.
+//
+// Synchronisation (one MMA issuer, thread 32 of CTA 0):
+//  * each CTA's producer fills its own stage and arms its own full[s];
+//  * CTA 1's thread 32 waits its full[s] and arrives on CTA 0's pfull[s], so
+//    CTA 0 issues only when both halves of the stage have landed;
+//  * the issuer's commits arrive on empty[s] and acc_full[b] of both CTAs
+//    (commit multicast over the pair);
+//  * the four epilogue warps of each CTA arrive on CTA 0's acc_empty[b]
+//    (count 8) when they have read their rows of accumulator b.
+// All waits are bounded by the context's budget; every thread reaches the final
+// cluster barrier, after which the pair releases its tensor memory together.
+template <int NPAD>
+struct HalfTcPair {
+  static constexpr int STAGES = NPAD == 256 ? 3 : NPAD == 128 ? 4 : 5;
+  static constexpr uint32_t VH_BYTES = (NPAD / 2) * TC_KB * 2;  // one plane's half of V per stage
+  static constexpr uint32_t STAGE_BYTES = 2 * BLOCK_BYTES + 2 * VH_BYTES;
+  static constexpr size_t SMEM = 232448;
+  static_assert((size_t)STAGES * STAGE_BYTES + 1024 + 512 <= SMEM, "stage budget");
+};
+
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+
+// shared::cluster address of the same object in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(addr) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_cluster_bounded(uint64_t* bar, uint32_t parity, int* err) {
+  if (mbar_try_wait_cluster(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  const uint64_t limit = wait_budget_ns(err);
+  while (true) {
+    if (mbar_try_wait_cluster(bar, parity)) return true;
+    if (globaltimer_ns() - t0 > limit) {
+      if (err) atomicCAS(err, DEV_OK, DEV_WAIT_TIMEOUT);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void tc2_alloc(uint32_t* dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc2_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void tc2_mma(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// arrive (once the issuer's earlier MMAs complete) on `bar` in both CTAs of the pair
+__device__ __forceinline__ void tc2_commit_pair(uint64_t* bar) {
+  const uint16_t mask = 3;
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::
+                   "r"(smem_u32(bar)),
+               "h"(mask)
+               : "memory");
+}
+
+template <int NPAD>
+__global__ void __launch_bounds__(192, 1)
+    k_half_tc_pair(const __nv_bfloat16* __restrict__ Bhi, const __nv_bfloat16* __restrict__ Blo, int nmb, int nkb,
+                   const __nv_bfloat16* __restrict__ Vhi, const __nv_bfloat16* __restrict__ Vlo, int nib, int64_t np,
+                   int64_t ntp, __nv_bfloat16* __restrict__ Xhi, __nv_bfloat16* __restrict__ Xlo, int* err,
+                   const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo, int use_tm,
+                   int64_t p0) {
+  const int64_t nsq = (int64_t)nmb * (nmb + 1) / 2;
+  using C = HalfTcPair<NPAD>;
+  constexpr int S = C::STAGES;
+  constexpr int NH = NPAD / 2;  // V columns (B rows) per CTA
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_BYTES);
+  uint64_t* empty = full + S;
+  uint64_t* pfull = empty + S;
+  uint64_t* acc_full = pfull + S;      // [2]
+  uint64_t* acc_empty = acc_full + 2;  // [2], used in CTA 0
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const int64_t NPR = gridDim.x / 2, pair = blockIdx.x / 2;
+  const int64_t my_tiles = ntp > pair ? (ntp - pair + NPR - 1) / NPR : 0;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+      mbar_init(&pfull[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 8);
+    }
+    mbar_fence_init();
+  }
+  if (warp == 0) tc2_alloc(tmem_slot, 2 * NPAD);
+  tc_fence_before();
+  cluster_sync_all();  // barriers initialised and tensor memory allocated in both CTAs
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool ok = true;
+
+  if (warp == 0) {
+    for (int64_t lt = 0; lt < my_tiles && ok; ++lt) {
+      const int64_t tile = pair + lt * NPR;
+      const int64_t P0 = 2 * (tile / nmb);
+      const int mb = (int)(tile % nmb);
+      const int64_t pl = P0 + (int64_t)rank < np ? P0 + (int64_t)rank : P0;  // a missing partner reads P0
+      for (int kb = 0; kb < nkb && ok; ++kb) {
+        const int64_t g = lt * nkb + kb;
+        const int s = (int)(g % S);
+        if (lane == 0 && g >= S) ok = mbar_wait_cluster_bounded(&empty[s], (uint32_t)(((g / S) - 1) & 1), err);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) break;
+        uint8_t* st = smem + s * C::STAGE_BYTES;
+        if (lane == 0) mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
+        __syncwarp();
+        const int Kb = kb >> 1, j = kb & 1;
+        if (mb <= Kb) {
+          const int64_t boff = ((pl * nsq + sq_index(mb, Kb)) * 2 + j) * BLOCK_ELEMS;
+          if (lane == 0) bulk_g2s(st, Bhi + boff, BLOCK_BYTES, &full[s]);
+          if (lane == 1) bulk_g2s(st + BLOCK_BYTES, Blo + boff, BLOCK_BYTES, &full[s]);
+        } else if (use_tm) {
+          const int z = (int)(((p0 + pl) * nsq + sq_index(Kb, mb)) * 16);
+          if (lane == 0) tma_load_3d(st, &tm_hi, 0, 2 * j, z, &full[s]);
+          if (lane == 1) tma_load_3d(st + BLOCK_BYTES, &tm_lo, 0, 2 * j, z, &full[s]);
+        } else {
+          const int64_t sbase = (pl * nsq + sq_index(Kb, mb)) * 2 * BLOCK_ELEMS + (int64_t)(8 * j) * 64;
+          const int run = lane & 15;
+          const int64_t src = sbase + (int64_t)(run >> 3) * BLOCK_ELEMS + (int64_t)((run & 7) * (TC_M / 8)) * 64;
+          if (lane < 16)
+            bulk_g2s(st + run * 1024, Bhi + src, 1024, &full[s]);
+          else
+            bulk_g2s(st + BLOCK_BYTES + run * 1024, Blo + src, 1024, &full[s]);
+        }
+        // V in halves: stage kb holds half 0 then half 1, each (NH x 64) K-major
+        const int64_t voff = ((int64_t)kb * 2 + rank) * NH * TC_KB;
+        if (lane == 2) bulk_g2s(st + 2 * BLOCK_BYTES, Vhi + voff, C::VH_BYTES, &full[s]);
+        if (lane == 3) bulk_g2s(st + 2 * BLOCK_BYTES + C::VH_BYTES, Vlo + voff, C::VH_BYTES, &full[s]);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && rank == 0) {
+      constexpr uint32_t idesc_k = idesc_bf16(2 * TC_M, NPAD, false);
+      constexpr uint32_t idesc_mn = idesc_bf16(2 * TC_M, NPAD, false, true);
+      for (int64_t lt = 0; lt < my_tiles && ok; ++lt) {
+        const int b = (int)(lt & 1);
+        const int mb = (int)((pair + lt * NPR) % nmb);
+        if (lt >= 2) ok = mbar_wait_cluster_bounded(&acc_empty[b], (uint32_t)(((lt / 2) - 1) & 1), err);
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(b * NPAD);
+        for (int kb = 0; kb < nkb && ok; ++kb) {
+          const int64_t g = lt * nkb + kb;
+          const int s = (int)(g % S);
+          ok = mbar_wait_cluster_bounded(&full[s], (uint32_t)((g / S) & 1), err) &&
+               mbar_wait_cluster_bounded(&pfull[s], (uint32_t)((g / S) & 1), err);
+          if (!ok) break;
+          tc_fence_after();
+          const uint8_t* st = smem + s * C::STAGE_BYTES;
+          const bool mirror = mb > (kb >> 1);
+          const uint32_t idesc = mirror ? idesc_mn : idesc_k;
+          const uint32_t a_lbo = mirror ? 128u : (TC_M / 8) * 128u, a_sbo = mirror ? 1024u : 128u;
+#pragma unroll
+          for (int ks = 0; ks < TC_KB / 16; ++ks) {
+            const uint32_t ak = mirror ? 2 * ks * 128 : 2 * ks * (TC_M / 8) * 128, vk = 2 * ks * (NH / 8) * 128;
+            const uint64_t dah = smem_desc(st + ak, a_lbo, a_sbo);
+            const uint64_t dal = smem_desc(st + BLOCK_BYTES + ak, a_lbo, a_sbo);
+            const uint64_t dvh = smem_desc(st + 2 * BLOCK_BYTES + vk, (NH / 8) * 128, 128);
+            const uint64_t dvl = smem_desc(st + 2 * BLOCK_BYTES + C::VH_BYTES + vk, (NH / 8) * 128, 128);
+            const uint32_t acc0 = (kb > 0 || ks > 0) ? 1u : 0u;
+            tc2_mma(d, dah, dvh, idesc, acc0);
+            tc2_mma(d, dah, dvl, idesc, 1u);
+            tc2_mma(d, dal, dvh, idesc, 1u);
+          }
+          tc2_commit_pair(&empty[s]);
+        }
+        tc2_commit_pair(&acc_full[b]);
+      }
+    } else if (lane == 0) {
+      // CTA 1: tell CTA 0's issuer when this CTA's half of each stage has landed
+      const uint32_t remote = 0;
+      for (int64_t lt = 0; lt < my_tiles && ok; ++lt)
+        for (int kb = 0; kb < nkb && ok; ++kb) {
+          const int64_t g = lt * nkb + kb;
+          const int s = (int)(g % S);
+          ok = mbar_wait_cluster_bounded(&full[s], (uint32_t)((g / S) & 1), err);
+          if (ok) mbar_arrive_cluster(cluster_addr(&pfull[s], remote));
+        }
+    }
+  } else {
+    // epilogue warps 2..5: this CTA's 128 rows of accumulator b
+    const int quad = warp & 3;
+    const int m = quad * 32 + lane;
+    const uint32_t acc_empty0 = cluster_addr(&acc_empty[0], 0);
+    const uint32_t acc_empty1 = cluster_addr(&acc_empty[1], 0);
+    for (int64_t lt = 0; lt < my_tiles; ++lt) {
+      const int b = (int)(lt & 1);
+      const bool got = mbar_wait_cluster_bounded(&acc_full[b], (uint32_t)((lt / 2) & 1), err);
+      if (!__all_sync(0xffffffffu, got)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int64_t tile = pair + lt * NPR;
+      const int64_t pl = 2 * (tile / nmb) + (int64_t)rank;
+      const int mb = (int)(tile % nmb);
+      if (pl < np) {
+        const int64_t xbase = ((pl * nmb + mb) * (int64_t)nib) * BLOCK_ELEMS;
+#pragma unroll 1
+        for (int c0 = 0; c0 < NPAD; c0 += 32) {
+          float v[32];
+          tc_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * NPAD + c0), v);
+          const int ib = c0 / TC_KB;
+#pragma unroll
+          for (int gq = 0; gq < 4; ++gq) {
+            __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj) split_bf16((double)v[gq * 8 + jj], h[jj], l[jj]);
+            const int k = (c0 % TC_KB) + gq * 8;
+            const int64_t off = xbase + (int64_t)ib * BLOCK_ELEMS + core_off(m, k, TC_M);
+            *reinterpret_cast<uint4*>(Xhi + off) = *reinterpret_cast<const uint4*>(h);
+            *reinterpret_cast<uint4*>(Xlo + off) = *reinterpret_cast<const uint4*>(l);
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(b ? acc_empty1 : acc_empty0);
+    }
+  }
+  tc_fence_before();
+  cluster_sync_all();  // the pair's MMAs, copies and remote arrivals are over
+  tc_fence_after();
+  if (warp == 0) tc2_dealloc(tmem, 2 * NPAD);
+}
+
 // ---- rank update on tcgen05 --------------------------------------------------------
 // CTA per (upper block pair q, P split): K[Ib][Jb] (128 x 128) = sum_p sum_ib
 // X_p[Ib, ib] S X_p[Jb, ib]^T, FP32 in TMEM, written as an FP32 partial.
@@ -402,7 +690,7 @@ struct RankTc {
   // The whole per-CTA shared memory is reserved (one CTA per SM either way),
   // so descriptor strides never point outside the allocation.
   static constexpr size_t SMEM = 232448;
-  static_assert((size_t)STAGES * STAGE_BYTES + 1024 + 128 <= SMEM, "rank stage budget");
+  static_assert((size_t)STAGES * STAGE_BYTES + 1024 + 256 <= SMEM, "rank stage budget");
 };
 
 __device__ __forceinline__ int64_t tri_root_tc(int64_t t) {
@@ -509,6 +797,136 @@ __global__ void __launch_bounds__(128, 1)
   if (warp == 0) tc_dealloc(tmem, 128);
 }
 
+// Paired rank update: a cluster of two CTAs computes the 2 x 2 group of K blocks
+// {2a, 2a+1} x {2c, 2c+1} (a <= c) with M = 256, N = 256 MMAs over the pair:
+// CTA r holds the A rows of block 2a + r and the B rows of block 2c + r, and
+// its tensor memory receives rows 2a + r against both column blocks.  Per SM a
+// stage is one A and one B block (64 KB) for twice the MMA work of the one-SM
+// kernel, and each SM reads half the shared-memory operand bytes per flop.
+// Blocks below the diagonal (the (2c+1, 2c) block of a diagonal group) and
+// blocks beyond n are computed but not written.  Same partial layout as
+// k_rank_tc: part[(sp pairs + q) 128 x 128], q = Jb (Jb + 1) / 2 + Ib.
+// Synchronisation as in k_half_tc_pair (relay of CTA 1's stage arrivals, commit
+// multicast over the pair, bounded waits, a cluster barrier before release).
+__global__ void __launch_bounds__(128, 1)
+    k_rank_tc_pair(const __nv_bfloat16* __restrict__ Xhi, const __nv_bfloat16* __restrict__ Xlo, int nmb, int nib,
+                   int npos_blocks, int64_t np, int splits, int64_t ngroups, float* __restrict__ part, int* err) {
+  using C = RankTc;
+  constexpr int S = C::STAGES;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_BYTES);
+  uint64_t* empty = full + S;
+  uint64_t* pfull = empty + S;
+  uint64_t* accf = pfull + S;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const int64_t cl = blockIdx.x / 2;
+  const int64_t gq = cl % ngroups;
+  const int sp = (int)(cl / ngroups);
+  const int64_t gc = tri_root_tc(gq), ga = gq - gc * (gc + 1) / 2;
+  const int64_t Ib = 2 * ga + rank, Jb = 2 * gc + rank;  // this CTA's A rows and B rows
+  const int64_t Ia = Ib < nmb ? Ib : 2 * ga, Ja = Jb < nmb ? Jb : 2 * gc;  // blocks actually read
+  const int64_t pa = np * sp / splits, pb = np * (sp + 1) / splits;
+  const int64_t nsteps = (pb - pa) * nib;
+  const int64_t pairs = (int64_t)nmb * (nmb + 1) / 2;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+      mbar_init(&pfull[s], 1);
+    }
+    mbar_init(accf, 1);
+    mbar_fence_init();
+  }
+  if (warp == 0) tc2_alloc(tmem_slot, 256);
+  tc_fence_before();
+  cluster_sync_all();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool ok = true;
+
+  if (warp == 0 && lane == 0) {
+    for (int64_t t = 0; t < nsteps && ok; ++t) {
+      const int s = (int)(t % S);
+      if (t >= S) ok = mbar_wait_cluster_bounded(&empty[s], (uint32_t)(((t / S) - 1) & 1), err);
+      if (!ok) break;
+      const int64_t p = pa + t / nib;
+      const int ib = (int)(t % nib);
+      uint8_t* st = smem + s * C::STAGE_BYTES;
+      mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
+      const int64_t ao = ((p * nmb + Ia) * (int64_t)nib + ib) * BLOCK_ELEMS;
+      const int64_t bo = ((p * nmb + Ja) * (int64_t)nib + ib) * BLOCK_ELEMS;
+      bulk_g2s(st, Xhi + ao, BLOCK_BYTES, &full[s]);
+      bulk_g2s(st + BLOCK_BYTES, Xlo + ao, BLOCK_BYTES, &full[s]);
+      bulk_g2s(st + 2 * BLOCK_BYTES, Xhi + bo, BLOCK_BYTES, &full[s]);
+      bulk_g2s(st + 3 * BLOCK_BYTES, Xlo + bo, BLOCK_BYTES, &full[s]);
+    }
+  } else if (warp == 1 && lane == 0 && rank == 0) {
+    constexpr uint32_t id_pos = idesc_bf16(2 * TC_M, 2 * TC_M, false);
+    constexpr uint32_t id_neg = idesc_bf16(2 * TC_M, 2 * TC_M, true);
+    for (int64_t t = 0; t < nsteps && ok; ++t) {
+      const int s = (int)(t % S);
+      ok = mbar_wait_cluster_bounded(&full[s], (uint32_t)((t / S) & 1), err) &&
+           mbar_wait_cluster_bounded(&pfull[s], (uint32_t)((t / S) & 1), err);
+      if (!ok) break;
+      tc_fence_after();
+      const int ib = (int)(t % nib);
+      const uint32_t idesc = ib < npos_blocks ? id_pos : id_neg;
+      const uint8_t* st = smem + s * C::STAGE_BYTES;
+#pragma unroll
+      for (int ks = 0; ks < TC_KB / 16; ++ks) {
+        const uint32_t kof = 2 * ks * (TC_M / 8) * 128;
+        const uint64_t dah = smem_desc(st + kof, (TC_M / 8) * 128, 128);
+        const uint64_t dal = smem_desc(st + BLOCK_BYTES + kof, (TC_M / 8) * 128, 128);
+        const uint64_t dbh = smem_desc(st + 2 * BLOCK_BYTES + kof, (TC_M / 8) * 128, 128);
+        const uint64_t dbl = smem_desc(st + 3 * BLOCK_BYTES + kof, (TC_M / 8) * 128, 128);
+        const uint32_t acc0 = (t > 0 || ks > 0) ? 1u : 0u;
+        tc2_mma(tmem, dah, dbh, idesc, acc0);
+        tc2_mma(tmem, dah, dbl, idesc, 1u);
+        tc2_mma(tmem, dal, dbh, idesc, 1u);
+      }
+      tc2_commit_pair(&empty[s]);
+    }
+    tc2_commit_pair(accf);
+  } else if (warp == 1 && lane == 0) {
+    for (int64_t t = 0; t < nsteps && ok; ++t) {
+      const int s = (int)(t % S);
+      ok = mbar_wait_cluster_bounded(&full[s], (uint32_t)((t / S) & 1), err);
+      if (ok) mbar_arrive_cluster(cluster_addr(&pfull[s], 0));
+    }
+  }
+  __syncwarp();
+  const bool acc_ok = __syncthreads_and(ok) && nsteps > 0 && mbar_wait_cluster_bounded(accf, 0, err);
+  tc_fence_after();
+  const int m = warp * 32 + lane;
+#pragma unroll 1
+  for (int h = 0; h < 2; ++h) {
+    const int64_t jb = 2 * gc + h;
+    if (Ib >= nmb || jb >= nmb || Ib > jb) continue;  // uniform over the CTA
+    const int64_t q = jb * (jb + 1) / 2 + Ib;
+    float* out = part + ((int64_t)sp * pairs + q) * (TC_M * TC_M);
+#pragma unroll 1
+    for (int c0 = 0; c0 < TC_M; c0 += 32) {
+      float v[32];
+      if (acc_ok) {
+        tc_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * TC_M + c0), v);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = 0.0f;
+      }
+#pragma unroll
+      for (int i = 0; i < 32; ++i) out[m + TC_M * (c0 + i)] = v[i];
+    }
+  }
+  tc_fence_before();
+  cluster_sync_all();
+  tc_fence_after();
+  if (warp == 0) tc2_dealloc(tmem, 256);
+}
+
 // FP32 partials -> packed upper K (FP64), out (+)= scale * sum_splits.
 __global__ void __launch_bounds__(256) k_rank_tc_finalize(int64_t n, int64_t npair, const float* __restrict__ part,
                                                           int splits, int64_t pairs, double scale, int accumulate,
@@ -537,6 +955,20 @@ TcGeom make_tc_geom(const Geom& g, int ncols) {
   t.npad = ncols <= 64 ? 64 : ncols <= 128 ? 128 : 256;
   t.nib = t.npad / TC_KB;
   t.block_elems = BLOCK_ELEMS;
+  // SM-pair (cta_group::2) kernels: measured on B200 at n = 600 / 1200, the
+  // paired rank update is faster from about eight 128-row blocks on (5.46 vs
+  // 6.25 ms at n = 1200, slower at n = 600 where each CTA has few k steps),
+  // and the paired half-transform is not (10.0 vs 9.3 ms at n = 1200).
+  // RIJK_TC_PAIR=0 / 1 turns both off / on.
+  const char* e = getenv("RIJK_TC_PAIR");
+  if (e && e[0] == '0') {
+    t.pair = t.pair_rank = 0;
+  } else if (e && e[0] == '1') {
+    t.pair = t.pair_rank = 1;
+  } else {
+    t.pair = 0;
+    t.pair_rank = t.nmb >= 8 ? 1 : 0;
+  }
   return t;
 }
 
@@ -564,8 +996,8 @@ void launch_split_cols(const Geom& g, const TcGeom& t, const double* V, int64_t 
   const int64_t total = (int64_t)t.npad * TC_KB * t.nkb;
   const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv_t(total, 256), 148 * 8));
   count_launch();
-  k_split_cols<<<blocks, 256, 0, st>>>(V, ldv, g.n, ncols, t.npad, t.nkb, static_cast<__nv_bfloat16*>(hi),
-                                       static_cast<__nv_bfloat16*>(lo));
+  k_split_cols<<<blocks, 256, 0, st>>>(V, ldv, g.n, ncols, t.npad, t.nkb, t.pair ? 2 : 1,
+                                       static_cast<__nv_bfloat16*>(hi), static_cast<__nv_bfloat16*>(lo));
 }
 
 static int sm_count() {
@@ -630,8 +1062,66 @@ static void half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void*
       static_cast<__nv_bfloat16*>(Xhi), static_cast<__nv_bfloat16*>(Xlo), err, mhi, mlo, tm ? 1 : 0, p0);
 }
 
+template <int NPAD>
+static void half_tc_pair(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
+                         const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st) {
+  using C = HalfTcPair<NPAD>;
+  auto kern = k_half_tc_pair<NPAD>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+  const int64_t per_p = tc_row_elems(g);
+  const int64_t ntp = cdiv_t(np, 2) * t.nmb;  // (aux-row pair, row block) tiles
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.blockDim = dim3(192, 1, 1);
+  cfg.dynamicSmemBytes = C::SMEM;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  // as many pairs as can be resident at once (an SM without a partner in its
+  // cluster group takes none), at most one per tile
+  static int resident = 0;
+  if (resident == 0) {
+    cfg.gridDim = dim3((unsigned)(2 * (sm_count() / 2)), 1, 1);
+    int nc = 0;
+    if (cudaOccupancyMaxActiveClusters(&nc, kern, &cfg) != cudaSuccess || nc <= 0) {
+      cudaGetLastError();
+      nc = sm_count() / 2;
+    }
+    resident = nc;
+  }
+  const int64_t pairs = std::max<int64_t>(1, std::min<int64_t>(ntp, resident));
+  cfg.gridDim = dim3((unsigned)(2 * pairs), 1, 1);
+  const int64_t rows = g.naux * (int64_t)t.nmb * (t.nmb + 1) / 2 * 16;
+  CUtensorMap mhi, mlo;
+  const bool tm = mirror_map(&mhi, Bhi, rows) && mirror_map(&mlo, Blo, rows);
+  if (!tm) {
+    memset(&mhi, 0, sizeof(mhi));
+    memset(&mlo, 0, sizeof(mlo));
+  }
+  count_launch();
+  // a failed launch stays the thread's last CUDA error, which the caller checks
+  (void)cudaLaunchKernelEx(&cfg, kern, static_cast<const __nv_bfloat16*>(Bhi) + p0 * per_p,
+                     static_cast<const __nv_bfloat16*>(Blo) + p0 * per_p, t.nmb, t.nkb,
+                     static_cast<const __nv_bfloat16*>(Vhi), static_cast<const __nv_bfloat16*>(Vlo), t.nib, np, ntp,
+                     static_cast<__nv_bfloat16*>(Xhi), static_cast<__nv_bfloat16*>(Xlo), err, mhi, mlo, tm ? 1 : 0,
+                     p0);
+}
+
 void launch_half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
                     const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st) {
+  if (t.pair) {
+    if (t.npad == 64)
+      half_tc_pair<64>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
+    else if (t.npad == 128)
+      half_tc_pair<128>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
+    else
+      half_tc_pair<256>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
+    return;
+  }
   if (t.npad == 64)
     half_tc<64>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
   else if (t.npad == 128)
@@ -643,14 +1133,38 @@ void launch_half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void*
 // Each split accumulates at most ~64 aux rows in FP32 in tensor memory (the
 // splits are then summed in FP64), and there are enough CTAs to fill the GPU.
 int tc_rank_splits(const TcGeom& t, int64_t np) {
-  const int64_t pairs = (int64_t)t.nmb * (t.nmb + 1) / 2;
-  const int64_t s = std::max<int64_t>(cdiv_t(2 * 148, pairs), cdiv_t(np, 64));
+  const int64_t nmg = cdiv_t(t.nmb, 2);
+  const int64_t ctas = t.pair_rank ? 2 * (nmg * (nmg + 1) / 2) : (int64_t)t.nmb * (t.nmb + 1) / 2;
+  const int64_t s = std::max<int64_t>(cdiv_t(2 * 148, ctas), cdiv_t(np, 64));
   return (int)std::max<int64_t>(1, std::min<int64_t>(np, s));
 }
 
 void launch_rank_tc(const Geom& g, const TcGeom& t, const void* Xhi, const void* Xlo, int64_t np, int npos_blocks,
                     int splits, float* part, int* err, cudaStream_t st) {
   const int64_t pairs = (int64_t)t.nmb * (t.nmb + 1) / 2;
+  if (t.pair_rank) {
+    const int64_t nmg = cdiv_t(t.nmb, 2), ngroups = nmg * (nmg + 1) / 2;
+    cudaFuncSetAttribute(k_rank_tc_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RankTc::SMEM);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(2 * ngroups * splits), 1, 1);
+    cfg.blockDim = dim3(128, 1, 1);
+    cfg.dynamicSmemBytes = RankTc::SMEM;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    count_launch();
+    // a failed launch stays the thread's last CUDA error, which the caller checks
+    (void)cudaLaunchKernelEx(&cfg, k_rank_tc_pair, static_cast<const __nv_bfloat16*>(Xhi),
+                             static_cast<const __nv_bfloat16*>(Xlo), t.nmb, t.nib, npos_blocks, np, splits, ngroups,
+                             part, err);
+    (void)g;
+    return;
+  }
   cudaFuncSetAttribute(k_rank_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RankTc::SMEM);
   dim3 grid((unsigned)pairs, (unsigned)splits);
   count_launch();

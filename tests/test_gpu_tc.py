@@ -36,8 +36,15 @@ def _split_k_occ(ctx, c, occ):
         return out.cpu().numpy()
 
 
-@pytest.mark.parametrize("n,naux,nocc", [(64, 24, 8), (100, 40, 16), (200, 30, 40), (300, 20, 24), (520, 6, 72)])
-def test_split_exchange_is_exact_on_bf16_representable_input(ctx, n, naux, nocc):
+@pytest.mark.parametrize("pair", ["1", "0"])
+@pytest.mark.parametrize("n,naux,nocc", [(64, 24, 8), (100, 40, 16), (200, 30, 40), (300, 20, 24), (520, 6, 72),
+                                         (100, 41, 16), (520, 7, 72), (200, 31, 160), (390, 9, 130)])
+def test_split_exchange_is_exact_on_bf16_representable_input(ctx, monkeypatch, pair, n, naux, nocc):
+    """Both half-transform / rank-update forms (SM pairs with cta_group::2, and
+    one SM per tile), odd aux counts (a pair whose second aux row is missing),
+    odd 128-row block counts (K block groups with rows beyond n) and every
+    column padding (64, 128, 256)."""
+    monkeypatch.setenv("RIJK_TC_PAIR", pair)
     rng = np.random.default_rng(n)
     npair = n * (n + 1) // 2
     rimatr = np.asfortranarray(rng.integers(-1, 2, size=(npair, naux)).astype(np.float64))
