@@ -62,7 +62,7 @@ __device__ double block_sum(double v, double* red) {
   return red[0];
 }
 
-__global__ void __launch_bounds__(ET) k_eigh(double* __restrict__ Aall, int64_t ld, const int32_t* __restrict__ nvalid,
+__global__ void __launch_bounds__(ET, 1) k_eigh(double* __restrict__ Aall, int64_t ld, const int32_t* __restrict__ nvalid,
                                              double pad_value, double* __restrict__ Wall, double* __restrict__ Vall,
                                              double* __restrict__ Zall, int32_t* __restrict__ info) {
   __shared__ double d[MAX_N], e[MAX_N], v[MAX_N], w[MAX_N], rc[MAX_N], rs[MAX_N];
@@ -196,7 +196,10 @@ __global__ void __launch_bounds__(ET) k_eigh(double* __restrict__ Aall, int64_t 
           for (; i >= l; --i) {
             const double f = s * e[i];
             const double bb = c * e[i];
-            r = hypot(f, g);
+            // |f|, |g| are bounded by the matrix norm, far from FP64 overflow:
+            // sqrt of the sum of squares and one reciprocal keep the serial
+            // chain short
+            r = sqrt(fma(f, f, g * g));
             e[i + 1] = r;
             if (r == 0.0) {  // the sweep splits here: deflate and sweep again
               d[i + 1] -= p;
@@ -204,8 +207,9 @@ __global__ void __launch_bounds__(ET) k_eigh(double* __restrict__ Aall, int64_t 
               early = true;
               break;
             }
-            s = f / r;
-            c = g / r;
+            const double ri = 1.0 / r;
+            s = f * ri;
+            c = g * ri;
             g = d[i + 1] - p;
             r = (d[i] - g) * s + 2.0 * c * bb;
             p = s * r;
@@ -230,10 +234,24 @@ __global__ void __launch_bounds__(ET) k_eigh(double* __restrict__ Aall, int64_t 
       if (m == l) break;
       const int lo = sweep_info[1];
       // the chain i = m-1 .. lo on rows i, i+1 of Z; each thread owns column t
-      // and carries the partly rotated row i+1 in a register
+      // and carries the partly rotated row i+1 in a register.  Rows are read
+      // eight at a time ahead of their rotations (each row is read before the
+      // rotation that overwrites it), so eight L2 round trips overlap.
       for (int t = tid; t < n; t += ET) {
         double zi1 = Z[(int64_t)m * ld + t];
-        for (int i = m - 1; i >= lo; --i) {
+        int i = m - 1;
+        for (; i - 7 >= lo; i -= 8) {
+          double zr[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) zr[u] = Z[(int64_t)(i - u) * ld + t];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const double c = rc[i - u], s = rs[i - u];
+            Z[(int64_t)(i - u + 1) * ld + t] = s * zr[u] + c * zi1;
+            zi1 = c * zr[u] - s * zi1;
+          }
+        }
+        for (; i >= lo; --i) {
           const double c = rc[i], s = rs[i];
           const double zi = Z[(int64_t)i * ld + t];
           Z[(int64_t)(i + 1) * ld + t] = s * zi + c * zi1;
