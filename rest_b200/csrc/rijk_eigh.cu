@@ -173,6 +173,14 @@ __global__ void __launch_bounds__(ET, 1) k_eigh(double* __restrict__ Aall, int64
   // rotations below, which mix indices i and i+1, mix whole rows of Z.
 
   // ---- 3. implicit QL on (d, e) ------------------------------------------------
+  // Each sweep: thread 0 finds the unreduced block [l, m], then computes the
+  // chain of plane rotations i = m-1 .. lo one after another (a serial
+  // recurrence) and publishes its progress in `prog`; warps 1.. apply each
+  // rotation to their columns of Z as soon as it is published, so the rows of
+  // Z stream through L2 while the chain is still being computed.  Waits are
+  // bounded: a sweep whose chain is not published in time marks the matrix as
+  // failed (info = 2) and the caller re-solves it with another solver.
+  __shared__ volatile int prog, chain_done;
   for (int l = 0; l < n; ++l) {
     for (int iter = 0;; ++iter) {
       if (tid == 0) {
@@ -181,83 +189,111 @@ __global__ void __launch_bounds__(ET, 1) k_eigh(double* __restrict__ Aall, int64
           const double dd = fabs(d[m]) + fabs(d[m + 1]);
           if (fabs(e[m]) + dd == dd) break;
         }
-        int lo = l;
         if (m != l && iter >= 30) {
           info[b] = 1;  // no convergence: leave this eigenvalue as it stands
           m = l;
-        } else if (m != l) {
-          // Wilkinson's shift from the leading 2 x 2 of the block
-          double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-          double r = hypot(g, 1.0);
-          g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? fabs(r) : -fabs(r)));
-          double s = 1.0, c = 1.0, p = 0.0;
-          bool early = false;
-          int i = m - 1;
-          for (; i >= l; --i) {
-            const double f = s * e[i];
-            const double bb = c * e[i];
-            // |f|, |g| are bounded by the matrix norm, far from FP64 overflow:
-            // sqrt of the sum of squares and one reciprocal keep the serial
-            // chain short
-            r = sqrt(fma(f, f, g * g));
-            e[i + 1] = r;
-            if (r == 0.0) {  // the sweep splits here: deflate and sweep again
-              d[i + 1] -= p;
-              e[m] = 0.0;
-              early = true;
-              break;
-            }
-            const double ri = 1.0 / r;
-            s = f * ri;
-            c = g * ri;
-            g = d[i + 1] - p;
-            r = (d[i] - g) * s + 2.0 * c * bb;
-            p = s * r;
-            d[i + 1] = g + p;
-            g = c * r - bb;
-            rc[i] = c;
-            rs[i] = s;
-          }
-          if (early) {
-            lo = i + 1;
-          } else {
-            d[l] -= p;
-            e[l] = g;
-            e[m] = 0.0;
-          }
         }
         sweep_info[0] = m;
-        sweep_info[1] = lo;
+        sweep_info[1] = m;
+        prog = m;
+        chain_done = 0;
       }
       __syncthreads();
       const int m = sweep_info[0];
       if (m == l) break;
-      const int lo = sweep_info[1];
-      // the chain i = m-1 .. lo on rows i, i+1 of Z; each thread owns column t
-      // and carries the partly rotated row i+1 in a register.  Rows are read
-      // eight at a time ahead of their rotations (each row is read before the
-      // rotation that overwrites it), so eight L2 round trips overlap.
-      for (int t = tid; t < n; t += ET) {
-        double zi1 = Z[(int64_t)m * ld + t];
+      if (tid == 0) {
+        // Wilkinson's shift from the leading 2 x 2 of the block
+        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+        double r = hypot(g, 1.0);
+        g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? fabs(r) : -fabs(r)));
+        double s = 1.0, c = 1.0, p = 0.0;
+        bool early = false;
         int i = m - 1;
-        for (; i - 7 >= lo; i -= 8) {
-          double zr[8];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) zr[u] = Z[(int64_t)(i - u) * ld + t];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const double c = rc[i - u], s = rs[i - u];
-            Z[(int64_t)(i - u + 1) * ld + t] = s * zr[u] + c * zi1;
-            zi1 = c * zr[u] - s * zi1;
+        for (; i >= l; --i) {
+          const double f = s * e[i];
+          const double bb = c * e[i];
+          // |f|, |g| are bounded by the matrix norm, far from FP64 overflow:
+          // one reciprocal square root keeps the serial chain short
+          const double r2 = fma(f, f, g * g);
+          if (r2 == 0.0) {  // the sweep splits here: deflate and sweep again
+            e[i + 1] = 0.0;
+            d[i + 1] -= p;
+            e[m] = 0.0;
+            early = true;
+            break;
           }
+          const double ri = rsqrt(r2);
+          r = r2 * ri;
+          e[i + 1] = r;
+          s = f * ri;
+          c = g * ri;
+          g = d[i + 1] - p;
+          r = (d[i] - g) * s + 2.0 * c * bb;
+          p = s * r;
+          d[i + 1] = g + p;
+          g = c * r - bb;
+          rc[i] = c;
+          rs[i] = s;
+          __threadfence_block();
+          prog = i;  // rotations i .. m-1 are ready
         }
-        for (; i >= lo; --i) {
-          const double c = rc[i], s = rs[i];
-          const double zi = Z[(int64_t)i * ld + t];
-          Z[(int64_t)(i + 1) * ld + t] = s * zi + c * zi1;
-          zi1 = c * zi - s * zi1;
+        if (!early) {
+          d[l] -= p;
+          e[l] = g;
+          e[m] = 0.0;
         }
-        Z[(int64_t)lo * ld + t] = zi1;
+        sweep_info[1] = early ? i + 1 : l;
+        __threadfence_block();
+        chain_done = 1;
+      } else if (warp > 0) {
+        // the chain on rows i, i+1 of Z; each thread owns column t and carries
+        // the partly rotated row i+1 in a register; rows are read up to eight
+        // ahead of their rotations (each row before the rotation that
+        // overwrites it)
+        for (int t = tid - 32; t < n; t += ET - 32) {
+          double zi1 = Z[(int64_t)m * ld + t];
+          int i = m - 1;
+          int lo = m;
+          bool stalled = false;
+          while (true) {
+            int pr = prog, done = chain_done;
+            for (int spin = 0; pr > i && !done; ++spin) {
+              if (spin > (1 << 24)) {
+                stalled = true;
+                break;
+              }
+              pr = prog;
+              done = chain_done;
+            }
+            if (stalled) break;
+            __threadfence_block();
+            if (done) lo = sweep_info[1];
+            const int stop = done ? lo : pr;
+            for (; i - 7 >= stop; i -= 8) {
+              double zr[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u) zr[u] = Z[(int64_t)(i - u) * ld + t];
+#pragma unroll
+              for (int u = 0; u < 8; ++u) {
+                const double c = rc[i - u], s = rs[i - u];
+                Z[(int64_t)(i - u + 1) * ld + t] = s * zr[u] + c * zi1;
+                zi1 = c * zr[u] - s * zi1;
+              }
+            }
+            for (; i >= stop; --i) {
+              const double c = rc[i], s = rs[i];
+              const double zi = Z[(int64_t)i * ld + t];
+              Z[(int64_t)(i + 1) * ld + t] = s * zi + c * zi1;
+              zi1 = c * zi - s * zi1;
+            }
+            if (done) break;
+          }
+          if (stalled) {
+            info[b] = 2;
+            break;
+          }
+          Z[(int64_t)lo * ld + t] = zi1;
+        }
       }
       __syncthreads();
     }
