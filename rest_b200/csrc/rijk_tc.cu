@@ -144,6 +144,22 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfl
   lo = __double2bfloat16(x - (double)__bfloat162float(hi));
 }
 
+// The same split of eight FP32 accumulator values, in FP32: bf16(v) rounds
+// exactly as bf16((double)v) does, and v - hi is exact in FP32 (hi agrees with v
+// in its leading bits), so hi and lo equal split_bf16((double)v) bit for bit
+// while the conversions run as packed FP32 -> BF16 pairs instead of FP64.
+__device__ __forceinline__ void split_bf16x8(const float* v, uint4& hi, uint4& lo) {
+  __nv_bfloat162 h[4], l[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+    const float2 hf = __bfloat1622float2(h[q]);
+    l[q] = __floats2bfloat162_rn(v[2 * q] - hf.x, v[2 * q + 1] - hf.y);
+  }
+  hi = *reinterpret_cast<const uint4*>(h);
+  lo = *reinterpret_cast<const uint4*>(l);
+}
+
 // ---- layout producers --------------------------------------------------------
 // Square (I <= J) of B_P is number J (J + 1) / 2 + I, two (128 x 64) K-major
 // blocks (K halves j = 0, 1): rows mu = 128 I + r, K kappa = 128 J + 64 j + k.
@@ -220,13 +236,18 @@ __global__ void __launch_bounds__(256) k_split_cols(const double* __restrict__ V
 // the epilogue of tile i (4 warps, TMEM -> BF16 split -> HBM) overlaps the MMAs
 // of tile i+1.  Warp 0: producer, warp 1: MMA issuer, warps 2..5: epilogue
 // (warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31).
-template <int NPAD>
+// KS: K per pipeline stage (64, or 32 for twice as many stages in the same
+// shared memory, i.e. a deeper look-ahead for the same bytes in flight).
+template <int NPAD, int KS = TC_KB>
 struct HalfTcP {
-  static constexpr int STAGES = NPAD == 256 ? 2 : NPAD == 128 ? 3 : 4;
-  static constexpr uint32_t V_BYTES = NPAD * TC_KB * 2;
-  static constexpr uint32_t STAGE_BYTES = 2 * BLOCK_BYTES + 2 * V_BYTES;
+  static_assert(KS == 64 || KS == 32, "stage K");
+  static constexpr uint32_t A_BYTES = TC_M * KS * 2;  // one plane's A tile per stage
+  static constexpr uint32_t V_BYTES = NPAD * KS * 2;
+  static constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * V_BYTES;
   static constexpr size_t SMEM = 232448;  // whole per-CTA budget (one CTA per SM)
-  static_assert((size_t)STAGES * STAGE_BYTES + 1024 + 256 <= SMEM, "stage budget");
+  static constexpr int STAGES = (int)((SMEM - 1024 - 256) / STAGE_BYTES) > 8 ? 8
+                                                                            : (int)((SMEM - 1024 - 256) / STAGE_BYTES);
+  static_assert(STAGES >= 2 && (size_t)STAGES * STAGE_BYTES + 1024 + 256 <= SMEM, "stage budget");
 };
 
 // K step kb of row block mb reads square (mb, kb / 2) when mb <= kb / 2, else
@@ -238,7 +259,7 @@ struct HalfTcP {
 // seen as rows of 1024 BF16 (one group of 8 rows of a square, all 16 of its K
 // groups), as dims {256, 4, rows}; the box {256, 2, 16} at (0, 2 j, 16 square)
 // is K half j of the square's 16 row groups, landing at 1 KB per group.
-template <int NPAD>
+template <int NPAD, int KS>
 __global__ void __launch_bounds__(192, 1)
     k_half_tc_persistent(const __nv_bfloat16* __restrict__ Bhi, const __nv_bfloat16* __restrict__ Blo, int nmb,
                          int nkb, const __nv_bfloat16* __restrict__ Vhi, const __nv_bfloat16* __restrict__ Vlo,
@@ -246,8 +267,9 @@ __global__ void __launch_bounds__(192, 1)
                          int* err, const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
                          int use_tm, int64_t p0) {
   const int64_t nsq = (int64_t)nmb * (nmb + 1) / 2;
-  using C = HalfTcP<NPAD>;
+  using C = HalfTcP<NPAD, KS>;
   constexpr int S = C::STAGES;
+  constexpr int QK = TC_KB / KS;  // stages per 64-wide K block
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_BYTES);
@@ -281,12 +303,13 @@ __global__ void __launch_bounds__(192, 1)
     // The whole warp stages: lane 0 waits for the slot and arms the barrier,
     // then the copies are issued one per lane (a mirrored square is 32 runs
     // of 1 KB, hi and lo).
+    const int nks = nkb * QK;  // stages per tile
     for (int64_t lt = 0; lt < my_tiles && ok; ++lt) {
       const int64_t tile = blockIdx.x + lt * G;
       const int64_t pl = tile / nmb;
       const int mb = (int)(tile % nmb);
-      for (int kb = 0; kb < nkb && ok; ++kb) {
-        const int64_t g = lt * nkb + kb;
+      for (int ksg = 0; ksg < nks && ok; ++ksg) {
+        const int64_t g = lt * nks + ksg;
         const int s = (int)(g % S);
         if (lane == 0 && g >= S) ok = mbar_wait_bounded(&empty[s], (uint32_t)(((g / S) - 1) & 1), err);
         ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -294,16 +317,21 @@ __global__ void __launch_bounds__(192, 1)
         uint8_t* st = smem + s * C::STAGE_BYTES;
         if (lane == 0) mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
         __syncwarp();
+        const int kb = ksg / QK, q = ksg % QK;  // 64-wide K block, and this stage's part of it
         const int Kb = kb >> 1, j = kb & 1;
         if (mb <= Kb) {
-          const int64_t boff = ((pl * nsq + sq_index(mb, Kb)) * 2 + j) * BLOCK_ELEMS;
-          if (lane == 0) bulk_g2s(st, Bhi + boff, BLOCK_BYTES, &full[s]);
-          if (lane == 1) bulk_g2s(st + BLOCK_BYTES, Blo + boff, BLOCK_BYTES, &full[s]);
+          // stage q of a K-major block: K groups [8 q KS/64 ..) are its first / second half
+          const int64_t boff = ((pl * nsq + sq_index(mb, Kb)) * 2 + j) * BLOCK_ELEMS + (int64_t)q * (TC_M * KS);
+          if (lane == 0) bulk_g2s(st, Bhi + boff, C::A_BYTES, &full[s]);
+          if (lane == 1) bulk_g2s(st + C::A_BYTES, Blo + boff, C::A_BYTES, &full[s]);
         } else if (use_tm) {
+          // mirrored square: K rows [64 j + KS q, +KS) of it are the 512-element
+          // pieces y = (64 j + KS q) / 32 .. of each of its 16 K-group rows
           const int z = (int)(((p0 + pl) * nsq + sq_index(Kb, mb)) * 16);
-          if (lane == 0) tma_load_3d(st, &tm_hi, 0, 2 * j, z, &full[s]);
-          if (lane == 1) tma_load_3d(st + BLOCK_BYTES, &tm_lo, 0, 2 * j, z, &full[s]);
-        } else {
+          const int y = (64 * j + KS * q) / 32;
+          if (lane == 0) tma_load_3d(st, &tm_hi, 0, y, z, &full[s]);
+          if (lane == 1) tma_load_3d(st + C::A_BYTES, &tm_lo, 0, y, z, &full[s]);
+        } else if (KS == TC_KB) {
           const int64_t sbase = (pl * nsq + sq_index(Kb, mb)) * 2 * BLOCK_ELEMS + (int64_t)(8 * j) * 64;
           const int run = lane & 15;  // M group of 8 rows: run `run` of 1 KB
           const int64_t src = sbase + (int64_t)(run >> 3) * BLOCK_ELEMS + (int64_t)((run & 7) * (TC_M / 8)) * 64;
@@ -312,15 +340,17 @@ __global__ void __launch_bounds__(192, 1)
           else
             bulk_g2s(st + BLOCK_BYTES + run * 1024, Blo + src, 1024, &full[s]);
         }
-        const int64_t voff = (int64_t)kb * NPAD * TC_KB;
-        if (lane == 2) bulk_g2s(st + 2 * BLOCK_BYTES, Vhi + voff, C::V_BYTES, &full[s]);
-        if (lane == 3) bulk_g2s(st + 2 * BLOCK_BYTES + C::V_BYTES, Vlo + voff, C::V_BYTES, &full[s]);
+        // V stage: K groups [KS q / 8, +KS / 8) of block kb, contiguous
+        const int64_t voff = (int64_t)kb * NPAD * TC_KB + (int64_t)q * NPAD * KS;
+        if (lane == 2) bulk_g2s(st + 2 * C::A_BYTES, Vhi + voff, C::V_BYTES, &full[s]);
+        if (lane == 3) bulk_g2s(st + 2 * C::A_BYTES + C::V_BYTES, Vlo + voff, C::V_BYTES, &full[s]);
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t idesc_k = idesc_bf16(TC_M, NPAD, false);
       constexpr uint32_t idesc_mn = idesc_bf16(TC_M, NPAD, false, true);
+      const int nks = nkb * QK;
       for (int64_t lt = 0; lt < my_tiles && ok; ++lt) {
         const int b = (int)(lt & 1);
         const int mb = (int)((blockIdx.x + lt * G) % nmb);
@@ -328,26 +358,27 @@ __global__ void __launch_bounds__(192, 1)
         if (!ok) break;
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(b * NPAD);
-        for (int kb = 0; kb < nkb && ok; ++kb) {
-          const int64_t g = lt * nkb + kb;
+        for (int ksg = 0; ksg < nks && ok; ++ksg) {
+          const int64_t g = lt * nks + ksg;
           const int s = (int)(g % S);
           ok = mbar_wait_bounded(&full[s], (uint32_t)((g / S) & 1), err);
           if (!ok) break;
           tc_fence_after();
           const uint8_t* st = smem + s * C::STAGE_BYTES;
-          const bool mirror = mb > (kb >> 1);
+          const bool mirror = mb > ((ksg / QK) >> 1);
           const uint32_t idesc = mirror ? idesc_mn : idesc_k;
           // K-major: K groups 2 KB apart, row groups 128 B; MN-major mirror:
-          // K groups 128 B apart (LBO), row groups 1 KB (SBO)
-          const uint32_t a_lbo = mirror ? 128u : (TC_M / 8) * 128u, a_sbo = mirror ? 1024u : 128u;
+          // K groups 128 B apart (LBO), row groups KS * 16 B (SBO: one
+          // 2 KB-strided K-group row of the square holds KS / 8 cores per stage)
+          const uint32_t a_lbo = mirror ? 128u : (TC_M / 8) * 128u, a_sbo = mirror ? (uint32_t)(KS * 16) : 128u;
 #pragma unroll
-          for (int ks = 0; ks < TC_KB / 16; ++ks) {
+          for (int ks = 0; ks < KS / 16; ++ks) {
             const uint32_t ak = mirror ? 2 * ks * 128 : 2 * ks * (TC_M / 8) * 128, vk = 2 * ks * (NPAD / 8) * 128;
             const uint64_t dah = smem_desc(st + ak, a_lbo, a_sbo);
-            const uint64_t dal = smem_desc(st + BLOCK_BYTES + ak, a_lbo, a_sbo);
-            const uint64_t dvh = smem_desc(st + 2 * BLOCK_BYTES + vk, (NPAD / 8) * 128, 128);
-            const uint64_t dvl = smem_desc(st + 2 * BLOCK_BYTES + C::V_BYTES + vk, (NPAD / 8) * 128, 128);
-            const uint32_t acc0 = (kb > 0 || ks > 0) ? 1u : 0u;
+            const uint64_t dal = smem_desc(st + C::A_BYTES + ak, a_lbo, a_sbo);
+            const uint64_t dvh = smem_desc(st + 2 * C::A_BYTES + vk, (NPAD / 8) * 128, 128);
+            const uint64_t dvl = smem_desc(st + 2 * C::A_BYTES + C::V_BYTES + vk, (NPAD / 8) * 128, 128);
+            const uint32_t acc0 = (ksg > 0 || ks > 0) ? 1u : 0u;
             tc_mma(d, dah, dvh, idesc, acc0);
             tc_mma(d, dah, dvl, idesc, 1u);
             tc_mma(d, dal, dvh, idesc, 1u);
@@ -380,13 +411,12 @@ __global__ void __launch_bounds__(192, 1)
         const int ib = c0 / TC_KB;
 #pragma unroll
         for (int gq = 0; gq < 4; ++gq) {
-          __align__(16) __nv_bfloat16 h[8], l[8];
-#pragma unroll
-          for (int j = 0; j < 8; ++j) split_bf16((double)v[gq * 8 + j], h[j], l[j]);
+          uint4 h, l;
+          split_bf16x8(v + gq * 8, h, l);
           const int k = (c0 % TC_KB) + gq * 8;
           const int64_t off = xbase + (int64_t)ib * BLOCK_ELEMS + core_off(m, k, TC_M);
-          *reinterpret_cast<uint4*>(Xhi + off) = *reinterpret_cast<const uint4*>(h);
-          *reinterpret_cast<uint4*>(Xlo + off) = *reinterpret_cast<const uint4*>(l);
+          *reinterpret_cast<uint4*>(Xhi + off) = h;
+          *reinterpret_cast<uint4*>(Xlo + off) = l;
         }
       }
       tc_fence_before();
@@ -660,13 +690,12 @@ __global__ void __launch_bounds__(192, 1)
           const int ib = c0 / TC_KB;
 #pragma unroll
           for (int gq = 0; gq < 4; ++gq) {
-            __align__(16) __nv_bfloat16 h[8], l[8];
-#pragma unroll
-            for (int jj = 0; jj < 8; ++jj) split_bf16((double)v[gq * 8 + jj], h[jj], l[jj]);
+            uint4 h, l;
+            split_bf16x8(v + gq * 8, h, l);
             const int k = (c0 % TC_KB) + gq * 8;
             const int64_t off = xbase + (int64_t)ib * BLOCK_ELEMS + core_off(m, k, TC_M);
-            *reinterpret_cast<uint4*>(Xhi + off) = *reinterpret_cast<const uint4*>(h);
-            *reinterpret_cast<uint4*>(Xlo + off) = *reinterpret_cast<const uint4*>(l);
+            *reinterpret_cast<uint4*>(Xhi + off) = h;
+            *reinterpret_cast<uint4*>(Xlo + off) = l;
           }
         }
       }
@@ -1027,39 +1056,62 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // Map of one split plane for the mirrored reads (see k_half_tc_persistent).
-static bool mirror_map(CUtensorMap* m, const void* plane, int64_t rows) {
+// ks: K rows of the mirrored square per copy (64 or 32), i.e. ks / 32 of the
+// four 256-element pieces of each of its K-group rows.
+static bool mirror_map(CUtensorMap* m, const void* plane, int64_t rows, int ks = TC_KB) {
   auto enc = tensor_map_encoder();
   if (!enc || rows <= 0 || rows > (int64_t)INT32_MAX) return false;
   const cuuint64_t dims[3] = {256, 4, (cuuint64_t)rows};
   const cuuint64_t strides[2] = {512, 2048};  // bytes, dims 1 and 2
-  const cuuint32_t box[3] = {256, 2, 16};
+  const cuuint32_t box[3] = {256, (cuuint32_t)(ks / 32), 16};
   const cuuint32_t estr[3] = {1, 1, 1};
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(plane), dims, strides, box, estr,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int NPAD>
-static void half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
-                    const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st) {
-  using C = HalfTcP<NPAD>;
-  cudaFuncSetAttribute(k_half_tc_persistent<NPAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+template <int NPAD, int KS>
+static void half_tc_ks(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
+                       const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st,
+                       const CUtensorMap& mhi, const CUtensorMap& mlo, bool tm) {
+  using C = HalfTcP<NPAD, KS>;
+  cudaFuncSetAttribute(k_half_tc_persistent<NPAD, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
   const int64_t per_p = tc_row_elems(g);
   const int64_t ntiles = np * t.nmb;
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, sm_count()));
+  count_launch();
+  k_half_tc_persistent<NPAD, KS><<<grid, 192, C::SMEM, st>>>(
+      static_cast<const __nv_bfloat16*>(Bhi) + p0 * per_p, static_cast<const __nv_bfloat16*>(Blo) + p0 * per_p,
+      t.nmb, t.nkb, static_cast<const __nv_bfloat16*>(Vhi), static_cast<const __nv_bfloat16*>(Vlo), t.nib, ntiles,
+      static_cast<__nv_bfloat16*>(Xhi), static_cast<__nv_bfloat16*>(Xlo), err, mhi, mlo, tm ? 1 : 0, p0);
+}
+
+// K 64 per stage; RIJK_TC_KS=32 halves the stage (twice the stages in the same
+// shared memory, where the mirrored squares can be fetched by tensor copies).
+// Measured on B200, K 32 is slower at every width (n = 1200: 9.8 against 9.7 ms
+// at 256 columns, 9.3 against 5.5 ms at 128, 8.2 against 4.1 ms at 64), so the
+// look-ahead of two 96 KB stages is not what bounds the kernel.
+template <int NPAD>
+static void half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
+                    const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st) {
+  const char* e = getenv("RIJK_TC_KS");
+  int ks = (e && atoi(e) == 32) ? 32 : 64;
   // the maps cover the whole split tensor (g.naux rows of squares), from p = 0
   const int64_t rows = g.naux * (int64_t)t.nmb * (t.nmb + 1) / 2 * 16;
   CUtensorMap mhi, mlo;
-  const bool tm = mirror_map(&mhi, Bhi, rows) && mirror_map(&mlo, Blo, rows);
+  bool tm = mirror_map(&mhi, Bhi, rows, ks) && mirror_map(&mlo, Blo, rows, ks);
+  if (!tm && ks != 64) {
+    ks = 64;
+    tm = mirror_map(&mhi, Bhi, rows, ks) && mirror_map(&mlo, Blo, rows, ks);
+  }
   if (!tm) {
     memset(&mhi, 0, sizeof(mhi));
     memset(&mlo, 0, sizeof(mlo));
   }
-  count_launch();
-  k_half_tc_persistent<NPAD><<<grid, 192, C::SMEM, st>>>(
-      static_cast<const __nv_bfloat16*>(Bhi) + p0 * per_p, static_cast<const __nv_bfloat16*>(Blo) + p0 * per_p,
-      t.nmb, t.nkb, static_cast<const __nv_bfloat16*>(Vhi), static_cast<const __nv_bfloat16*>(Vlo), t.nib, ntiles,
-      static_cast<__nv_bfloat16*>(Xhi), static_cast<__nv_bfloat16*>(Xlo), err, mhi, mlo, tm ? 1 : 0, p0);
+  if (ks == 32)
+    half_tc_ks<NPAD, 32>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, mhi, mlo, tm);
+  else
+    half_tc_ks<NPAD, 64>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, mhi, mlo, tm);
 }
 
 template <int NPAD>

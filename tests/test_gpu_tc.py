@@ -36,15 +36,20 @@ def _split_k_occ(ctx, c, occ):
         return out.cpu().numpy()
 
 
-@pytest.mark.parametrize("pair", ["1", "0"])
+@pytest.mark.parametrize("env", [{}, {"RIJK_TC_PAIR": "1"}, {"RIJK_TC_PAIR": "0", "RIJK_TC_KS": "32"}])
 @pytest.mark.parametrize("n,naux,nocc", [(64, 24, 8), (100, 40, 16), (200, 30, 40), (300, 20, 24), (520, 6, 72),
                                          (100, 41, 16), (520, 7, 72), (200, 31, 160), (390, 9, 130)])
-def test_split_exchange_is_exact_on_bf16_representable_input(ctx, monkeypatch, pair, n, naux, nocc):
-    """Both half-transform / rank-update forms (SM pairs with cta_group::2, and
-    one SM per tile), odd aux counts (a pair whose second aux row is missing),
-    odd 128-row block counts (K block groups with rows beyond n) and every
-    column padding (64, 128, 256)."""
-    monkeypatch.setenv("RIJK_TC_PAIR", pair)
+def test_split_exchange_is_exact_on_bf16_representable_input(ctx, monkeypatch, env, n, naux, nocc):
+    """Every kernel form: the defaults (one SM per half-transform tile with K 64
+    per stage, the rank update on SM pairs from eight 128-row blocks on), both
+    kernels on SM pairs (cta_group::2), and one SM each with K 32 per stage; odd
+    aux counts (a pair whose second aux row is missing), odd 128-row block
+    counts (K block groups with rows beyond n) and every column padding (64,
+    128, 256)."""
+    monkeypatch.delenv("RIJK_TC_PAIR", raising=False)
+    monkeypatch.delenv("RIJK_TC_KS", raising=False)
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
     rng = np.random.default_rng(n)
     npair = n * (n + 1) // 2
     rimatr = np.asfortranarray(rng.integers(-1, 2, size=(npair, naux)).astype(np.float64))
