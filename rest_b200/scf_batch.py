@@ -282,10 +282,13 @@ class BatchedRHF:
 
     def _eigh(self, fp, nvalid=None):
         """Batched symmetric eigensolve: the library's solver (one CTA per
-        matrix, rijk_eigh_batched_dev), with cuSOLVER only for a matrix it
-        reports as not converged or one beyond its size limit."""
+        matrix, rijk_eigh_batched_dev) for batches of at least 16 matrices, with
+        cuSOLVER for a matrix it reports as not converged, one beyond its size
+        limit, and batches of fewer matrices (one CTA per matrix would leave most
+        of the GPU idle; in the alkane runs, one molecule per batch, a 490 x 490
+        eigensolve on one SM made each SCF iteration several times slower)."""
         torch = self.torch
-        if nvalid is not None and fp.shape[1] <= 768 and self.native_eigh:
+        if nvalid is not None and fp.shape[1] <= 768 and self.native_eigh and fp.shape[0] >= 16:
             lam, V, ok = eigh_batched(fp, nvalid, pad_value=1.0e6)
             bad = torch.nonzero(~ok).flatten().tolist()
             if bad:
