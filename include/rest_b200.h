@@ -224,7 +224,8 @@ int rijk_vjk_upper_with_ri_v(rijk_ctx* ctx, const double* eigv, int64_t num_stat
  * src/scf_io/mod.rs:2758-2834) with every FP64 operand split into two BF16
  * parts and three tcgen05 products per pair accumulated in FP32 (relative
  * error about 1e-5 of |K|).  The first call after a tensor change builds BF16
- * copies of the tensor (4 bytes per element of the full n x n B_P). */
+ * hi / lo copies of the tensor (4 bytes per element of the upper 128 x 128
+ * squares of each B_P). */
 int rijk_vk_upper_occ_split_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int64_t* homo,
                                 const double* d_occupation, int spin_channel, double scaling_factor, double* d_vk,
                                 void* stream);
@@ -235,6 +236,15 @@ int rijk_vk_upper_occ_split_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num
  * exchange matrix of dD, whose split-precision error shrinks with |dD|. */
 int rijk_vk_upper_lowrank_split_dev(rijk_ctx* ctx, const double* d_V, int64_t ld_v, int64_t ncols, int64_t npos,
                                     double scaling_factor, int accumulate, double* d_vk, void* stream);
+/* J and K of the same difference: as rijk_vk_upper_lowrank_split_dev for d_vk,
+ * and d_vj = j_scaling_factor * upper(J[dD]) (always overwritten), whose per-aux-
+ * row scalars B_P : dD = sum_c S_c <V_c, (B_P V)_c> come out of the split
+ * half-transform's epilogue (FP32 accumulators against V in FP64), followed by
+ * one FP64 pass over the tensor.  For incremental builds J_k = J_ref + J[dD]
+ * in which, as for K, the split error shrinks with |dD|. */
+int rijk_vjk_upper_lowrank_split_dev(rijk_ctx* ctx, const double* d_V, int64_t ld_v, int64_t ncols, int64_t npos,
+                                     double j_scaling_factor, double k_scaling_factor, int accumulate, double* d_vj,
+                                     double* d_vk, void* stream);
 
 /* ---- grouped build over a molecule set ----------------------------------------- */
 /* No single counterpart in REST: REST builds J and K one SCF at a time

@@ -123,6 +123,11 @@ SIGNATURES = {
         C.c_int,
         [_ctxp, C.c_void_p, C.c_int64, _i64p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p],
     ),
+    "rijk_vjk_upper_lowrank_split_dev": (
+        C.c_int,
+        [_ctxp, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int, C.c_void_p,
+         C.c_void_p, C.c_void_p],
+    ),
     "rijk_vk_upper_lowrank_split_dev": (
         C.c_int,
         [_ctxp, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_int, C.c_void_p, C.c_void_p],

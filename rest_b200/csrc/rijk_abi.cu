@@ -1122,8 +1122,9 @@ static int tc_prepare(rijk_ctx* ctx, cudaStream_t st) {
 }
 
 // out (+)= scale sum_P (B_P V)(S)(B_P V)^T for the columns [c0, c0 + nc) of V, all of sign `sgn`
+// With w: also w[p] += sgn <V, B_p V> (J's scalars of the same difference).
 static int tc_lowrank_group(rijk_ctx* ctx, const double* d_V, int64_t ldv, int c0, int nc, int sgn, double scale,
-                            int accumulate, double* d_out, cudaStream_t st) {
+                            int accumulate, double* d_out, cudaStream_t st, double* w = nullptr) {
   const Geom& g = ctx->g;
   const rijk::TcGeom t = rijk::make_tc_geom(g, nc);
   const size_t vbytes = (size_t)t.npad * 64 * t.nkb * 2;
@@ -1137,12 +1138,17 @@ static int tc_lowrank_group(rijk_ctx* ctx, const double* d_V, int64_t ldv, int c
   const int64_t pairs = (int64_t)t.nmb * (t.nmb + 1) / 2;
   const int splits_max = rijk::tc_rank_splits(t, pchunk);
   RIJK_TRY(ensure(ctx, ctx->tcPart, (size_t)splits_max * pairs * 128 * 128 * 4));
+  rijk::TcJ jw{d_V + (int64_t)c0 * ldv, ldv, nc, (double)sgn, nullptr, w};
+  if (w) {
+    RIJK_TRY(ensure(ctx, ctx->Jw, (size_t)pchunk * 4 * t.nmb * 8));
+    jw.wpart = static_cast<double*>(ctx->Jw.p);
+  }
   for (int64_t p0 = 0; p0 < g.naux; p0 += pchunk) {
     const int64_t np = std::min(pchunk, g.naux - p0);
     {
       ProfScope ps(ctx, RIJK_PROF_K_HALF, st);
       rijk::launch_half_tc(g, t, ctx->tcBhi.p, ctx->tcBlo.p, p0, np, ctx->tcVhi.p, ctx->tcVlo.p, ctx->tcXhi.p,
-                           ctx->tcXlo.p, ctx->d_err, st);
+                           ctx->tcXlo.p, ctx->d_err, st, w ? &jw : nullptr);
     }
     const int splits = rijk::tc_rank_splits(t, np);
     {
@@ -1176,6 +1182,41 @@ int rijk_vk_upper_lowrank_split_dev(rijk_ctx* ctx, const double* d_V, int64_t ld
     c0 += nc;
   }
   return RIJK_OK;
+}
+
+int rijk_vjk_upper_lowrank_split_dev(rijk_ctx* ctx, const double* d_V, int64_t ld_v, int64_t ncols, int64_t npos,
+                                     double j_scaling_factor, double k_scaling_factor, int accumulate, double* d_vj,
+                                     double* d_vk, void* stream) {
+  RIJK_TRY(need_tensor(ctx));
+  if (!d_V || !d_vj || !d_vk || d_vj == d_vk || ncols < 0 || npos < 0 || npos > ncols || ld_v < ctx->g.n ||
+      (ld_v & 1) || (reinterpret_cast<uintptr_t>(d_V) & 15))
+    return set_err(ctx, RIJK_ERR_ARG, "bad argument");
+  const Geom& g = ctx->g;
+  cudaStream_t st = pick(ctx, stream);
+  RIJK_TRY(tc_prepare(ctx, st));
+  RIJK_TRY(ensure(ctx, ctx->w, (size_t)g.naux * 8));
+  double* w = static_cast<double*>(ctx->w.p);
+  RIJK_CK(cudaMemsetAsync(w, 0, (size_t)g.naux * 8, st));
+  bool first = !accumulate;
+  if (ncols == 0 && first) RIJK_CK(cudaMemsetAsync(d_vk, 0, (size_t)g.npair * 8, st));
+  for (int64_t c0 = 0; c0 < ncols;) {
+    const int64_t end = c0 < npos ? npos : ncols;
+    const int nc = (int)std::min<int64_t>(256, end - c0);
+    RIJK_TRY(tc_lowrank_group(ctx, d_V, ld_v, (int)c0, nc, c0 < npos ? 1 : -1, k_scaling_factor, first ? 0 : 1,
+                              d_vk, st, w));
+    first = false;
+    c0 += nc;
+  }
+  const int jsplits = rijk::j_pass2_splits(g);
+  RIJK_TRY(ensure(ctx, ctx->Jpart, (size_t)jsplits * g.ldB * 8));
+  double* Jp = static_cast<double*>(ctx->Jpart.p);
+  {
+    ProfScope ps(ctx, RIJK_PROF_J_PASS2, st);
+    rijk::launch_j_pass2(g, ctx->dB, w, 1, jsplits, Jp, st);
+  }
+  ProfScope ps(ctx, RIJK_PROF_J_OTHER, st);
+  rijk::launch_j_finalize(g, Jp, 1, jsplits, j_scaling_factor, 0, d_vj, st);
+  return after_launch(ctx, "split J and exchange");
 }
 
 int rijk_vk_upper_occ_split_dev(rijk_ctx* ctx, const double* d_eigv, int64_t num_state, const int64_t* homo,

@@ -122,8 +122,19 @@ void launch_split_tensor(const Geom& g, const double* B, int64_t p0, int64_t np,
 void launch_split_cols(const Geom& g, const TcGeom& t, const double* V, int64_t ldv, int ncols, void* hi, void* lo,
                        cudaStream_t st);
 // X (np x nmb x nib blocks, hi/lo) = B_{p0..p0+np} V
+// J's scalars from the split half-transform: w[p0 + p] += sgn <V, X_p> with V the
+// FP64 columns (ldv x ncols, column c at Vd + c ldv) the launch multiplies by.
+struct TcJ {
+  const double* Vd;
+  int64_t ldv;
+  int ncols;
+  double sgn;
+  double* wpart;  // 4 nmb doubles per aux row of the chunk
+  double* w;      // [naux]
+};
 void launch_half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
-                    const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st);
+                    const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st,
+                    const TcJ* jw = nullptr);
 int tc_rank_splits(const TcGeom& t, int64_t np);
 // part[split][pair][128x128] = sum_p X_p S X_p^T (S = -1 on blocks >= npos_blocks)
 void launch_rank_tc(const Geom& g, const TcGeom& t, const void* Xhi, const void* Xlo, int64_t np, int npos_blocks,

@@ -265,7 +265,8 @@ __global__ void __launch_bounds__(192, 1)
                          int nkb, const __nv_bfloat16* __restrict__ Vhi, const __nv_bfloat16* __restrict__ Vlo,
                          int nib, int64_t ntiles, __nv_bfloat16* __restrict__ Xhi, __nv_bfloat16* __restrict__ Xlo,
                          int* err, const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
-                         int use_tm, int64_t p0) {
+                         int use_tm, int64_t p0, const double* __restrict__ Vd, int64_t ldv, int ncols, int nrows,
+                         double* __restrict__ wpart) {
   const int64_t nsq = (int64_t)nmb * (nmb + 1) / 2;
   using C = HalfTcP<NPAD, KS>;
   constexpr int S = C::STAGES;
@@ -404,10 +405,19 @@ __global__ void __launch_bounds__(192, 1)
       const int64_t pl = tile / nmb;
       const int mb = (int)(tile % nmb);
       const int64_t xbase = ((pl * nmb + mb) * (int64_t)nib) * BLOCK_ELEMS;
+      // with wpart: this row's share of J's scalar <V, X_P> (V in FP64, X the
+      // FP32 accumulator) for the aux row of the tile
+      const int row = mb * TC_M + m;
+      double jacc = 0.0;
 #pragma unroll 1
       for (int c0 = 0; c0 < NPAD; c0 += 32) {
         float v[32];
         tc_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * NPAD + c0), v);
+        if (wpart && row < nrows) {
+#pragma unroll 8
+          for (int jj = 0; jj < 32 && c0 + jj < ncols; ++jj)
+            jacc = fma((double)v[jj], Vd[(int64_t)(c0 + jj) * ldv + row], jacc);
+        }
         const int ib = c0 / TC_KB;
 #pragma unroll
         for (int gq = 0; gq < 4; ++gq) {
@@ -422,11 +432,31 @@ __global__ void __launch_bounds__(192, 1)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[b]);
+      if (wpart) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) jacc += __shfl_xor_sync(0xffffffffu, jacc, o);
+        if (lane == 0) wpart[tile * 4 + quad] = jacc;
+      }
     }
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tc_dealloc(tmem, 2 * NPAD);
+}
+
+// w[p0 + p] += sgn * (the 4 nmb warp shares of aux row p, in a fixed order);
+// one warp per aux row.
+__global__ void __launch_bounds__(256) k_tc_wreduce(const double* __restrict__ wpart, int64_t np, int per_row,
+                                                    double sgn, int64_t p0, double* __restrict__ w) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t pl = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; pl < np;
+       pl += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    double a = 0.0;
+    for (int t = lane; t < per_row; t += 32) a += wpart[pl * per_row + t];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) w[p0 + pl] += sgn * a;
+  }
 }
 
 // ---- paired half-transform: one M = 256 MMA over two SMs (cta_group::2) -----------
@@ -1073,7 +1103,7 @@ static bool mirror_map(CUtensorMap* m, const void* plane, int64_t rows, int ks =
 template <int NPAD, int KS>
 static void half_tc_ks(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
                        const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st,
-                       const CUtensorMap& mhi, const CUtensorMap& mlo, bool tm) {
+                       const CUtensorMap& mhi, const CUtensorMap& mlo, bool tm, const TcJ* jw) {
   using C = HalfTcP<NPAD, KS>;
   cudaFuncSetAttribute(k_half_tc_persistent<NPAD, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
   const int64_t per_p = tc_row_elems(g);
@@ -1083,7 +1113,13 @@ static void half_tc_ks(const Geom& g, const TcGeom& t, const void* Bhi, const vo
   k_half_tc_persistent<NPAD, KS><<<grid, 192, C::SMEM, st>>>(
       static_cast<const __nv_bfloat16*>(Bhi) + p0 * per_p, static_cast<const __nv_bfloat16*>(Blo) + p0 * per_p,
       t.nmb, t.nkb, static_cast<const __nv_bfloat16*>(Vhi), static_cast<const __nv_bfloat16*>(Vlo), t.nib, ntiles,
-      static_cast<__nv_bfloat16*>(Xhi), static_cast<__nv_bfloat16*>(Xlo), err, mhi, mlo, tm ? 1 : 0, p0);
+      static_cast<__nv_bfloat16*>(Xhi), static_cast<__nv_bfloat16*>(Xlo), err, mhi, mlo, tm ? 1 : 0, p0,
+      jw ? jw->Vd : nullptr, jw ? jw->ldv : 0, jw ? jw->ncols : 0, (int)g.n, jw ? jw->wpart : nullptr);
+  if (jw) {
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv_t(np, 8), 148 * 8));
+    count_launch();
+    k_tc_wreduce<<<blocks, 256, 0, st>>>(jw->wpart, np, 4 * t.nmb, jw->sgn, p0, jw->w);
+  }
 }
 
 // K 64 per stage; RIJK_TC_KS=32 halves the stage (twice the stages in the same
@@ -1093,7 +1129,8 @@ static void half_tc_ks(const Geom& g, const TcGeom& t, const void* Bhi, const vo
 // look-ahead of two 96 KB stages is not what bounds the kernel.
 template <int NPAD>
 static void half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
-                    const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st) {
+                    const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st,
+                    const TcJ* jw) {
   const char* e = getenv("RIJK_TC_KS");
   int ks = (e && atoi(e) == 32) ? 32 : 64;
   // the maps cover the whole split tensor (g.naux rows of squares), from p = 0
@@ -1109,9 +1146,9 @@ static void half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void*
     memset(&mlo, 0, sizeof(mlo));
   }
   if (ks == 32)
-    half_tc_ks<NPAD, 32>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, mhi, mlo, tm);
+    half_tc_ks<NPAD, 32>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, mhi, mlo, tm, jw);
   else
-    half_tc_ks<NPAD, 64>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, mhi, mlo, tm);
+    half_tc_ks<NPAD, 64>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, mhi, mlo, tm, jw);
 }
 
 template <int NPAD>
@@ -1164,8 +1201,9 @@ static void half_tc_pair(const Geom& g, const TcGeom& t, const void* Bhi, const 
 }
 
 void launch_half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
-                    const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st) {
-  if (t.pair) {
+                    const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st,
+                    const TcJ* jw) {
+  if (t.pair && !jw) {
     if (t.npad == 64)
       half_tc_pair<64>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
     else if (t.npad == 128)
@@ -1175,11 +1213,11 @@ void launch_half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void*
     return;
   }
   if (t.npad == 64)
-    half_tc<64>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
+    half_tc<64>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, jw);
   else if (t.npad == 128)
-    half_tc<128>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
+    half_tc<128>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, jw);
   else
-    half_tc<256>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
+    half_tc<256>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, jw);
 }
 
 // Each split accumulates at most ~64 aux rows in FP32 in tensor memory (the

@@ -356,6 +356,16 @@ class RIJK:
                                                       spin_channel, float(scaling_factor), C.c_void_p(d_vk),
                                                       C.c_void_p(stream or None)))
 
+    def vjk_upper_lowrank_split_dev(self, d_v: int, ld_v: int, ncols: int, npos: int, j_scaling_factor: float,
+                                    k_scaling_factor: float, accumulate: bool, d_vj: int, d_vk: int,
+                                    stream: int = 0):
+        """J (overwritten) and K ((+)=) of dD = V S V^T in split precision, J's
+        scalars from the split half-transform."""
+        self._check(lib().rijk_vjk_upper_lowrank_split_dev(self._h, C.c_void_p(d_v), ld_v, ncols, npos,
+                                                           float(j_scaling_factor), float(k_scaling_factor),
+                                                           1 if accumulate else 0, C.c_void_p(d_vj),
+                                                           C.c_void_p(d_vk), C.c_void_p(stream or None)))
+
     def vk_upper_lowrank_split_dev(self, d_v: int, ld_v: int, ncols: int, npos: int, scaling_factor: float,
                                    accumulate: bool, d_vk: int, stream: int = 0):
         self._check(lib().rijk_vk_upper_lowrank_split_dev(self._h, C.c_void_p(d_v), ld_v, ncols, npos,

@@ -36,7 +36,10 @@ stream), and the SCF iterations of the whole set advance together:
 Precision of the exchange build:
   fp64   every K in FP64 (DMMA);
   mixed  for molecules with at least ``split_min_basis`` (512) basis functions,
-         incremental split-precision K: K_k = K_{k-1} + K_split(D_k - D_{k-1}) with
+         incremental split-precision J and K: K_k = K_{k-1} + K_split(D_k - D_{k-1})
+         and J_k = J_{k-1} + J(D_k - D_{k-1}), J's aux-row scalars taken from the
+         split half-transform of the difference (one FP64 pass over the tensor
+         instead of two), with
          the density difference in its exact low-rank form V S V^T (batched thin
          QR of [Y_k, Y_{k-1}] and an eigendecomposition of the small core, so the
          split error scales with |dD|), a full FP64 rebuild every
@@ -552,21 +555,25 @@ class BatchedRHF:
                 npair = n * (n + 1) // 2
                 vj = torch.empty(npair, dtype=torch.float64, device=self.dev)
                 keep = [vj]
-                fused = not incr[i] and self.precision != "split"
-                if not fused:
+                if self.precision == "split":
                     d = (2.0 * (c @ c.T)).contiguous()
                     ctx.vj_upper_dev(d.data_ptr(), 1, 1.0, 1, vj.data_ptr(), ctx.stream)
                     keep.append(d)
                 if incr[i]:
+                    # J and K of the density difference in split precision, added to the
+                    # previous build's: J_k = J_ref + J(dD), K_k = K_ref + K(dD)
                     vk = self._kref[i].clone()
+                    vj.copy_(self._jref[i])
                     V, npos = factors[i]
                     if V is not None:
                         ld = n + (n & 1)
                         buf = torch.zeros(V.shape[1], ld, dtype=torch.float64, device=self.dev)
                         buf[:, :n] = V.T
-                        ctx.vk_upper_lowrank_split_dev(buf.data_ptr(), ld, V.shape[1], npos, -0.5, True,
-                                                       vk.data_ptr(), ctx.stream)
-                        keep.append(buf)
+                        vjd = torch.empty(npair, dtype=torch.float64, device=self.dev)
+                        ctx.vjk_upper_lowrank_split_dev(buf.data_ptr(), ld, V.shape[1], npos, 1.0, -0.5, True,
+                                                        vjd.data_ptr(), vk.data_ptr(), ctx.stream)
+                        vj.add_(vjd)
+                        keep += [buf, vjd]
                     self._split_steps[i] += 1
                     self._nsplit[i] += 1
                     self._streak[i] = 0
@@ -588,6 +595,7 @@ class BatchedRHF:
                     keep += [c_cm, occ]
                 if self.precision == "mixed":
                     self._kref[i] = vk
+                    self._jref[i] = vj
                     self._yref[i] = Y[i].clone()
                 out[i, :n, :n] = self._upper_to_full(vj + vk, n)
                 done = torch.cuda.Event()
@@ -660,7 +668,7 @@ class BatchedRHF:
         self._occ_mask = torch.zeros(B, nm, dtype=f64, device=self.dev)
         for i in range(B):
             self._occ_mask[i, :self.nocc[i]] = 1.0
-        self._kref, self._yref = [None] * B, [None] * B
+        self._kref, self._jref, self._yref = [None] * B, [None] * B, [None] * B
         self._split_steps, self._nsplit, self._nfp64, self._streak = [0] * B, [0] * B, [0] * B, [0] * B
         self._fp64_now = [self.precision != "mixed" or self.n[i] < self.split_min_basis for i in range(B)]
         nmask = torch.arange(nm, device=self.dev)[None, :] < ns[:, None]

@@ -93,3 +93,45 @@ def test_split_lowrank_signed(ctx, n, naux, npos, nneg):
         ctx.synchronize(st)
         got = out.cpu().numpy()
     assert np.max(np.abs(got - ref)) <= 1e-4 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("n,naux,npos,nneg,exact", [(120, 41, 20, 12, True), (200, 30, 150, 0, True),
+                                                    (260, 1000, 300, 40, False), (390, 500, 64, 70, False)])
+def test_split_lowrank_j_and_k(ctx, n, naux, npos, nneg, exact):
+    """rijk_vjk_upper_lowrank_split_dev: J of dD = V S V^T from the split
+    half-transform's epilogue and K of the same difference, against the FP64
+    density-form builds; bit for bit on integer-valued input (every product and
+    sum exact), else within 1e-4 of max |J| and |K|."""
+    import torch
+
+    rng = np.random.default_rng(n + naux)
+    if exact:
+        npair = n * (n + 1) // 2
+        rimatr = np.asfortranarray(rng.integers(-1, 2, size=(npair, naux)).astype(np.float64))
+        v = rng.integers(-1, 2, size=(n, npos + nneg)).astype(np.float64)
+    else:
+        rimatr = host_case(n, naux, 4, seed=9 + n).rimatr
+        v = rng.standard_normal((n, npos + nneg)) / np.sqrt(n)
+    ctx.set_rimatr(rimatr, n)
+    s = np.concatenate([np.ones(npos), -np.ones(nneg)])
+    dd = (v * s) @ v.T
+    jref = ctx.vj_upper_with_rimatr_v([dd], 1, 1.0)[0]
+    kref = ctx.vk_upper_with_rimatr_use_dm_only([dd], 1, 1.0)[0]
+    st = ctx.stream
+    ld = n + (n & 1)
+    vp = np.zeros((ld, npos + nneg))
+    vp[:n] = v
+    with torch.cuda.stream(torch.cuda.ExternalStream(st)):
+        dv = _dev(np.asfortranarray(vp).T.copy())
+        vj = torch.full((n * (n + 1) // 2,), np.nan, dtype=torch.float64, device="cuda")
+        vk = torch.empty(n * (n + 1) // 2, dtype=torch.float64, device="cuda")
+        ctx.vjk_upper_lowrank_split_dev(dv.data_ptr(), ld, npos + nneg, npos, 1.0, 1.0, False, vj.data_ptr(),
+                                        vk.data_ptr(), st)
+        ctx.synchronize(st)
+        gj, gk = vj.cpu().numpy(), vk.cpu().numpy()
+    if exact:
+        assert np.array_equal(gj, jref)
+        assert np.array_equal(gk, kref)
+    else:
+        assert np.max(np.abs(gj - jref)) <= 1e-4 * np.max(np.abs(jref))
+        assert np.max(np.abs(gk - kref)) <= 1e-4 * np.max(np.abs(kref))
