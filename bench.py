@@ -671,8 +671,8 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
 
 
 # DRAM traffic of the half-transform per launch.  ncu at n=600, nocc=72 (N=2400,
-# one launch over all aux rows, the fused form with remainder columns;
-# profiles/k_half_transform_rank_update_n600.md) measured dram read 3.8403 GB +
+# one launch over all aux rows, the fused form with remainder columns) measured
+# dram read 3.8403 GB +
 # write 0.9461 GB = 4.7865 GB, which is 1.036 of the bytes the launch must move:
 # the tile-packed tensor rows it reads plus the X rows it writes (ldx x nocc per
 # aux row).  The n=1200 tensor (29 GB) is too large to capture under a
