@@ -1353,8 +1353,16 @@ int rijk_group_create(rijk_ctx* const* ctxs, int count, const int64_t* nocc, int
     d.nkb = cdiv(g.n, 128);
     d.pairs = d.nkb * (d.nkb + 1) / 2;
     d.npair = g.npair;
-    d.wper = (int)((d.ldx / BM) * (d.ocols / BN) * rijk::group_cta_warps(half_transform_cfg));
-    const int64_t counts[6] = {d.ldx * d.ocols, g.naux, g.naux * (d.ldx / BM) * (d.ocols / BN),
+    {
+      // orbitals ending 1..16 columns past a full block: the last full block's
+      // CTAs compute them (shape 1 only), so no mostly empty block is launched
+      const int full = (int)(nocc[m] / BN), rem = (int)(nocc[m] - (int64_t)full * BN);
+      const int xr = rijk::group_remainder_cols(half_transform_cfg);
+      d.xcol0 = (full >= 1 && rem > 0 && rem <= xr) ? full * BN : 0;
+      d.ncb = d.xcol0 > 0 ? full : d.ocols / BN;
+    }
+    d.wper = (int)((d.ldx / BM) * d.ncb * rijk::group_cta_warps(half_transform_cfg));
+    const int64_t counts[6] = {d.ldx * d.ocols, g.naux, g.naux * (d.ldx / BM) * d.ncb,
                                (int64_t)d.ksplits * d.pairs * subs, (int64_t)d.jsplits * cdiv(g.ldB / 2, 256),
                                g.npair};
     for (int ph = 0; ph < 6; ++ph) {
@@ -1419,6 +1427,8 @@ int rijk_group_create(rijk_ctx* const* ctxs, int count, const int64_t* nocc, int
   }
   gr->plan.ht_cfg = half_transform_cfg;
   gr->plan.rk_cfg = update_cfg;
+  gr->plan.remainder = 0;
+  for (int m = 0; m < count; ++m) gr->plan.remainder |= mols[m].xcol0 > 0 ? 1 : 0;
   int sms = 148;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
     cudaGetLastError();

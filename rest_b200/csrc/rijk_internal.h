@@ -151,6 +151,8 @@ struct GroupMol {
   double* Cw;       // sqrt(2) C, ldx x ocols, column-major
   int64_t ldx;
   int ocols;        // a multiple of the half-transform CTA width
+  int ncb;          // column blocks launched (ocols / width, or the full blocks with remainder columns)
+  int xcol0;        // > 0: columns [xcol0, nocc) are remainder columns of the last full block
   double* wpart;    // J scalars per half-transform warp: naux x (ldx / BM) x (ocols / BN) x warps
   int wper;         // wpart entries per aux row
   double* w;        // J scalars (naux)
@@ -169,11 +171,13 @@ struct GroupPlan {
   int64_t* pre[6];
   int64_t total[6];
   int ht_cfg, rk_cfg;
+  int remainder;  // some molecule has remainder columns (the half-transform variant that computes them)
 };
 int group_cta_rows(int cfg);
 int group_cta_cols(int cfg);
 int group_rank_subs(int cfg);
 int group_cta_warps(int cfg);
+int group_remainder_cols(int cfg);  // remainder columns the half-transform shape computes in its last full block
 // out[m] (ldo-strided, full and symmetric) = J(2 C_m C_m^T) + k_scale K(C_m) for
 // every molecule m with active[m] != 0; molecule m's orbitals C(mu, i) at
 // C0[m c_mol + mu c_row + i c_col] (occupation 2 for i < nocc).

@@ -910,7 +910,10 @@ __global__ void __launch_bounds__(256) k_grp_prepare(const GroupMol* __restrict_
 }
 
 // Phase 3 (persistent): X_P = B_P Cw for every (molecule, aux row, row block, column block).
-template <class Cfg>
+// XF > 0: a molecule with g.xcol0 > 0 launches only its full column blocks, and
+// the CTAs of the last one also compute the XF * 8 remainder columns from xcol0
+// on (ExtraCols), as the single-molecule half-transform does.
+template <class Cfg, int XF = 0>
 __global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_grp_half(const GroupMol* __restrict__ mols,
                                                                             const int64_t* __restrict__ pre, int count,
                                                                             int64_t total, const int* __restrict__ active,
@@ -920,19 +923,22 @@ __global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_grp_half(cons
     const int m = group_find(pre, count, it);
     if (!active[m]) continue;  // uniform over the CTA
     const GroupMol& g = mols[m];
-    const int nrb = (int)(g.ldx / Cfg::BM), ncb = g.ocols / Cfg::BN;
+    const int nrb = (int)(g.ldx / Cfg::BM), ncb = g.ncb;
     const int64_t bid = it - pre[m];
     const int cb = (int)(bid % ncb);
     const int64_t rest = bid / ncb;
     const int64_t pl = rest / nrb;
     const int I0 = (int)(rest % nrb) * Cfg::MT;
     const int col0 = cb * Cfg::BN;
-    HalfTransformSched sc{g.B + pl * g.ldB, g.Cw, g.ldx, g.nt, I0, col0, 0};
+    HalfTransformSched sc{g.B + pl * g.ldB, g.Cw, g.ldx, g.nt, I0, col0, g.xcol0};
     double acc[Cfg::FM][Cfg::FN][2];
+    ExtraCols<XF> xc;
+    xc.on = XF > 0 && g.xcol0 > 0 && cb == ncb - 1;
     const int ktiles = I0 < g.nt ? g.nt : 0;
     const LastTileK kv{g.nt - 1, g.n - (g.nt - 1) * TS};
     __syncthreads();  // the previous item's warps are done with the stages
-    if (dmma_mainloop<Cfg>(sc, ktiles, smem, acc, err, g.n - I0 * TS, g.nocc - col0, kv)) {
+    if (dmma_mainloop<Cfg, HalfTransformSched, LastTileK, XF>(sc, ktiles, smem, acc, err, g.n - I0 * TS,
+                                                               g.nocc - col0, kv, &xc)) {
       double* Xr = g.X + (int64_t)I0 * TS;
       const double* Wr = g.Cw + (int64_t)I0 * TS;
       const int64_t nw = g.nocc;
@@ -944,6 +950,24 @@ __global__ void __launch_bounds__(Cfg::THREADS, min_ctas<Cfg>()) k_grp_half(cons
         s = fma(v0, Wr[mm + c0 * g.ldx], s);
         s = fma(v1, Wr[mm + (c0 + 1) * g.ldx], s);
       });
+      if constexpr (XF > 0) {
+        if (xc.on) {
+          const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+          const int wm = warp / Cfg::WN, wn = warp % Cfg::WN;
+#pragma unroll
+          for (int e = 0; e < 2; ++e)
+#pragma unroll
+            for (int j = 0; j < XF; ++j) {
+              const int mm = wm * Cfg::WTM + (wn * 2 + e) * 8 + (lane >> 2);
+              const int64_t c = g.xcol0 + 8 * j + 2 * (lane & 3);
+              const double v0 = xc.acc[e][j][0], v1 = xc.acc[e][j][1];
+              if (c < nw) Xr[mm + (pl * nw + c) * g.ldx] = v0;
+              if (c + 1 < nw) Xr[mm + (pl * nw + c + 1) * g.ldx] = v1;
+              s = fma(v0, Wr[mm + c * g.ldx], s);
+              s = fma(v1, Wr[mm + (c + 1) * g.ldx], s);
+            }
+        }
+      }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
       if ((threadIdx.x & 31) == 0) g.wpart[bid * Cfg::CWARPS + (threadIdx.x >> 5)] = s;
@@ -1056,13 +1080,13 @@ __global__ void __launch_bounds__(256) k_grp_finalize(const GroupMol* __restrict
 
 int group_ctas_per_sm(int cfg) { return cfg == 1 ? 3 : 2; }
 
-template <class Cfg>
+template <class Cfg, int XF = 0>
 static void grp_half_cfg(const GroupMol* mols, const int64_t* pre, int count, int64_t total, const int* active,
                          int* err, int sms, cudaStream_t st) {
-  cudaFuncSetAttribute(k_grp_half<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+  cudaFuncSetAttribute(k_grp_half<Cfg, XF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
   const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)sms * min_ctas<Cfg>()));
   count_launch();
-  k_grp_half<Cfg><<<(unsigned)grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(mols, pre, count, total, active, err);
+  k_grp_half<Cfg, XF><<<(unsigned)grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(mols, pre, count, total, active, err);
 }
 
 template <class Cfg>
@@ -1078,6 +1102,7 @@ int group_cta_rows(int cfg) { return cfg == 4 ? 128 : 64; }
 int group_cta_cols(int cfg) { return 64; }
 int group_rank_subs(int cfg) { return cfg == 4 ? 2 : 4; }
 int group_cta_warps(int cfg) { return cfg == 4 ? HtCfg4::CWARPS : cfg == 0 ? HtCfg0::CWARPS : HtCfg1::CWARPS; }
+int group_remainder_cols(int cfg) { return cfg == 1 ? 16 : 0; }
 
 void launch_group(const GroupPlan& gp, const double* C0, int64_t c_mol, int64_t c_row, int64_t c_col, double k_scale,
                   double* out0, int64_t out_mol, int64_t ldo, const int* active, int* err, int sms, cudaStream_t st) {
@@ -1090,7 +1115,12 @@ void launch_group(const GroupPlan& gp, const double* C0, int64_t c_mol, int64_t 
   switch (gp.ht_cfg) {
     case 0: grp_half_cfg<HtCfg0>(gp.mols, gp.pre[2], n, gp.total[2], active, err, sms, st); break;
     case 4: grp_half_cfg<HtCfg4>(gp.mols, gp.pre[2], n, gp.total[2], active, err, sms, st); break;
-    default: grp_half_cfg<HtCfg1>(gp.mols, gp.pre[2], n, gp.total[2], active, err, sms, st); break;
+    default:
+      if (gp.remainder)
+        grp_half_cfg<HtCfg1, 2>(gp.mols, gp.pre[2], n, gp.total[2], active, err, sms, st);
+      else
+        grp_half_cfg<HtCfg1>(gp.mols, gp.pre[2], n, gp.total[2], active, err, sms, st);
+      break;
   }
   count_launch();
   k_grp_wreduce<<<(unsigned)cdiv(gp.total[1], 8), 256, 0, st>>>(gp.mols, gp.pre[1], n, gp.total[1], active);

@@ -190,16 +190,19 @@ def test_same_size_molecules_from_given_densities_are_reproducible():
     assert np.array_equal(np.array(runs[0].energies), np.array(runs[1].energies))
 
 
-def test_grouped_build_equals_per_molecule_build():
+@pytest.mark.parametrize("ks", [(3, 1, 5, 2), (13, 2, 16, 15)])
+def test_grouped_build_equals_per_molecule_build(ks):
     """rijk_group_jk_occ_dev against each molecule's own J (a2) and occupied-orbital
     K (a3) at 1e-10, for uneven clusters and every CTA shape of the grouped build;
-    an inactive molecule's output is left untouched."""
+    an inactive molecule's output is left untouched.  (H2O)13..16 have 65..80
+    occupied orbitals: 1..16 past a full column block, which shape 1 computes as
+    remainder columns of that block."""
     import numpy as np
     import torch
 
     from rest_b200 import RIJK, RIJKGroup
 
-    mols = [water_cluster(k, seed=70 + k) for k in (3, 1, 5, 2)]
+    mols = [water_cluster(k, seed=70 + k) for k in ks]
     ctxs = [RIJK(0) for _ in mols]
     try:
         for c, m in zip(ctxs, mols):
