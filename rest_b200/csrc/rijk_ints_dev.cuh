@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(128) k_int3c2e_cls(DShells A, DShells Cs, cons
   constexpr int NA = ncart_c(LA), NB = ncart_c(LB), NC = ncart_c(LC);
   constexpr int SA = 2 * LA + 1, SB = 2 * LB + 1, SC = 2 * LC + 1;
   constexpr int L = LA + LB + LC, NT = (L + 1) * (L + 2) * (L + 3) / 6;
-  constexpr bool UNR = L <= 5 && NA * NB * NC <= 60;
+  constexpr bool UNR = L <= 6 && NA * NB * NC <= 108;
   const int64_t task = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (task >= (int64_t)npc * nkc) return;
   const int q = (int)(task % npc), k = kc[task / npc];
