@@ -41,8 +41,27 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found: the CUDA toolkit is required to build librest_b200.so")
 
 
+# rijk_ints_cls.cu holds one three-centre integral class, chosen by macros: it is
+# compiled once per class (AO l <= 2 twice, auxiliary l <= 4)
+INT3C_CLASSES = [(a, b, c) for a in range(3) for b in range(3) for c in range(5)]
+
+
 def sources() -> list[Path]:
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
+
+
+def _jobs() -> list[tuple[Path, list[str], str]]:
+    """(source, defines, object stem) per object; the per-class integral objects
+    first, since their unrolled kernels are the longest compiles."""
+    cls, rest = [], []
+    for src in sources():
+        if src.name == "rijk_ints_cls.cu":
+            cls += [(src, [f"-DRIJK_LA={a}", f"-DRIJK_LB={b}", f"-DRIJK_LC={c}"], f"rijk_ints_cls_{a}{b}{c}")
+                    for a, b, c in INT3C_CLASSES]
+        else:
+            rest.append((src, [], src.stem))
+    rest.sort(key=lambda j: j[0].stat().st_size, reverse=True)
+    return cls + rest
 
 
 def _stale(lib: Path) -> bool:
@@ -62,14 +81,15 @@ def _obj_stale(src: Path, obj: Path) -> bool:
     return any(p.stat().st_mtime > t for p in [src] + headers)
 
 
-def _compile(src: Path, extra: list[str], force: bool = False) -> Path:
-    obj = BUILD / (src.stem + ".o")
+def _compile(src: Path, extra: list[str], force: bool = False, defines: list[str] | None = None,
+             stem: str | None = None) -> Path:
+    obj = BUILD / ((stem or src.stem) + ".o")
     if not force and not extra and not _obj_stale(src, obj):
         return obj
     if src.suffix == ".cpp":  # host-only code: g++ with OpenMP
         cmd = ["g++", "-c", str(src), "-o", str(obj), "-O3", "-fPIC", "-fopenmp", "-std=c++17", "-I" + str(INCLUDE)]
     else:
-        cmd = [nvcc(), "-c", str(src), "-o", str(obj)] + NVCC_FLAGS + extra
+        cmd = [nvcc(), "-c", str(src), "-o", str(obj)] + NVCC_FLAGS + (defines or []) + extra
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed on {src.name}:\n{r.stdout}\n{r.stderr}")
@@ -85,10 +105,8 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     extra = ["-Xptxas", "-v"] if verbose_ptxas else []
     if verbose_ptxas:
         os.environ["RIJK_PTXAS_VERBOSE"] = "1"
-    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        # longest compiles first so that they overlap the short ones
-        srcs = sorted(sources(), key=lambda p: p.stat().st_size, reverse=True)
-        objs = list(ex.map(lambda s: _compile(s, extra, force), srcs))
+    with cf.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(lambda j: _compile(j[0], extra, force, j[1], j[2]), _jobs()))
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", str(tmp)] + [str(o) for o in objs] + ["-lgomp"]
     r = subprocess.run(cmd, capture_output=True, text=True)

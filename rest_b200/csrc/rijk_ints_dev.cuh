@@ -1,6 +1,9 @@
 // Device code of the Coulomb integral engine shared by rijk_ints_gpu.cu (plan,
-// two-centre kernel, launches) and rijk_ints_l{0,1,2}.cu (the three-centre
-// kernels of one AO angular momentum each, compiled in parallel).
+// two-centre kernel, launches) and rijk_ints_cls.cu (one three-centre class per
+// translation unit, compiled in parallel).
+// Classes up to 90 Cartesian component triples (and total l <= 6) are fully
+// unrolled, so their Hermite tables live in registers; the larger ones keep
+// their component loops rolled, which bounds code size and compile time.
 // McMurchie-Davidson: Hermite expansion coefficients of the bra pair and of the
 // single-centre ket, Hermite Coulomb integrals R_tuv from the Boys function, the
 // Cartesian block, then real solid harmonics through the c2s matrices held in
@@ -40,13 +43,25 @@ struct DShells {
 
 using Int3cKernel = void (*)(DShells, DShells, const int*, const int*, int, const int*, int, int64_t, int64_t,
                              double*);
-// three-centre class kernels and table loaders, one pair per AO angular momentum
-Int3cKernel int3c_kernel_la0(int lb, int lc);
-Int3cKernel int3c_kernel_la1(int lb, int lc);
-Int3cKernel int3c_kernel_la2(int lb, int lc);
-int int3c_tables_la0(const double* flat, const int* off, const double* boys);
-int int3c_tables_la1(const double* flat, const int* off, const double* boys);
-int int3c_tables_la2(const double* flat, const int* off, const double* boys);
+// three-centre class kernels and table loaders, one pair per class
+// (rijk_ints_cls.cu compiled with RIJK_LA, RIJK_LB, RIJK_LC)
+#define RIJK_INT3C_CLASS(a, b, c)               \
+  Int3cKernel int3c_kernel_##a##b##c();         \
+  int int3c_tables_##a##b##c(const double* flat, const int* off, const double* boys);
+#define RIJK_INT3C_LC(a, b) \
+  RIJK_INT3C_CLASS(a, b, 0) RIJK_INT3C_CLASS(a, b, 1) RIJK_INT3C_CLASS(a, b, 2) RIJK_INT3C_CLASS(a, b, 3) \
+  RIJK_INT3C_CLASS(a, b, 4)
+RIJK_INT3C_LC(0, 0)
+RIJK_INT3C_LC(0, 1)
+RIJK_INT3C_LC(0, 2)
+RIJK_INT3C_LC(1, 0)
+RIJK_INT3C_LC(1, 1)
+RIJK_INT3C_LC(1, 2)
+RIJK_INT3C_LC(2, 0)
+RIJK_INT3C_LC(2, 1)
+RIJK_INT3C_LC(2, 2)
+#undef RIJK_INT3C_LC
+#undef RIJK_INT3C_CLASS
 
 namespace {
 
@@ -276,7 +291,7 @@ __global__ void __launch_bounds__(128) k_int3c2e_cls(DShells A, DShells Cs, cons
   constexpr int NA = ncart_c(LA), NB = ncart_c(LB), NC = ncart_c(LC);
   constexpr int SA = 2 * LA + 1, SB = 2 * LB + 1, SC = 2 * LC + 1;
   constexpr int L = LA + LB + LC, NT = (L + 1) * (L + 2) * (L + 3) / 6;
-  constexpr bool UNR = L <= 6 && NA * NB * NC <= 108;
+  constexpr bool UNR = L <= 6 && NA * NB * NC <= 90;
   const int64_t task = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (task >= (int64_t)npc * nkc) return;
   const int q = (int)(task % npc), k = kc[task / npc];
@@ -356,18 +371,6 @@ __global__ void __launch_bounds__(128) k_int3c2e_cls(DShells A, DShells Cs, cons
   }
 }
 
-template <int LA, int LB>
-Int3cKernel class_kernel_lc(int lc) {
-  return lc == 0   ? k_int3c2e_cls<LA, LB, 0>
-         : lc == 1 ? k_int3c2e_cls<LA, LB, 1>
-         : lc == 2 ? k_int3c2e_cls<LA, LB, 2>
-         : lc == 3 ? k_int3c2e_cls<LA, LB, 3>
-                   : k_int3c2e_cls<LA, LB, 4>;
-}
-template <int LA>
-Int3cKernel class_kernel(int lb, int lc) {
-  return lb == 0 ? class_kernel_lc<LA, 0>(lc) : lb == 1 ? class_kernel_lc<LA, 1>(lc) : class_kernel_lc<LA, 2>(lc);
-}
 
 }  // namespace
 }  // namespace intsdev

@@ -29,6 +29,24 @@ using namespace intsdev;
 
 namespace {
 
+// The 45 three-centre classes (rijk_ints_cls.cu), indexed (3 la + lb) 5 + lc.
+using Int3cTables = int (*)(const double*, const int*, const double*);
+using Int3cGetter = Int3cKernel (*)();
+#define RIJK_CLS5(f, a, b) f##a##b##0, f##a##b##1, f##a##b##2, f##a##b##3, f##a##b##4
+#define RIJK_CLS45(f)                                                                                   \
+  RIJK_CLS5(f, 0, 0), RIJK_CLS5(f, 0, 1), RIJK_CLS5(f, 0, 2), RIJK_CLS5(f, 1, 0), RIJK_CLS5(f, 1, 1), \
+      RIJK_CLS5(f, 1, 2), RIJK_CLS5(f, 2, 0), RIJK_CLS5(f, 2, 1), RIJK_CLS5(f, 2, 2)
+const Int3cTables* int3c_class_tables() {
+  static const Int3cTables t[45] = {RIJK_CLS45(int3c_tables_)};
+  return t;
+}
+const Int3cGetter* int3c_class_kernels() {
+  static const Int3cGetter k[45] = {RIJK_CLS45(int3c_kernel_)};
+  return k;
+}
+#undef RIJK_CLS45
+#undef RIJK_CLS5
+
 // 1D Hermite coefficients e[i][j][t] (t <= i + j) of a Gaussian product with
 // exponents a, b and AB = A - B.  i <= GLC covers a lone auxiliary bra shell (j = 0).
 using HermE = double[GLC + 1][GLA + 1][GLC + 1];
@@ -331,8 +349,9 @@ int upload_c2s(const double* const* c2s, cudaStream_t st) {
   if (cudaStreamSynchronize(st) != cudaSuccess) return RIJK_ERR_CUDA;
   // every translation unit with integral kernels holds its own copy of the table
   const double* boys = boys_table().data();
-  if (upload_tables(flat.data(), off, boys) || int3c_tables_la0(flat.data(), off, boys) ||
-      int3c_tables_la1(flat.data(), off, boys) || int3c_tables_la2(flat.data(), off, boys))
+  bool bad = upload_tables(flat.data(), off, boys) != 0;
+  for (int c = 0; c < 45 && !bad; ++c) bad = int3c_class_tables()[c](flat.data(), off, boys) != 0;
+  if (bad)
     return RIJK_ERR_CUDA;
   uploaded[dev] = flat;
   return RIJK_OK;
@@ -434,9 +453,7 @@ void launch_int3c2e(const RiIntPlan* p, int k0, int k1, double* out, cudaStream_
       if (npc == 0) continue;
       const int64_t tasks = (int64_t)npc * nkc;
       count_launch();
-      const Int3cKernel kern = c < 3 ? int3c_kernel_la0(c % 3, lc)
-                               : c < 6 ? int3c_kernel_la1(c % 3, lc)
-                                       : int3c_kernel_la2(c % 3, lc);
+      const Int3cKernel kern = int3c_class_kernels()[c * 5 + lc]();
       kern<<<(unsigned)((tasks + 127) / 128), 128, 0, st>>>(
           p->A, p->C, p->dpi + p->pair_cls[c], p->dpj + p->pair_cls[c], npc, dkc, nkc, npair_fun, P0, out);
     }
