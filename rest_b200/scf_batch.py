@@ -908,9 +908,10 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
                 r = b.run(initial_densities=None if guesses is None else [guesses[i] for i in idx], guess=model,
                           **run_kw)
             finally:
+                # the next group reuses torch's cached blocks: releasing them here
+                # would only make it allocate them again
                 tt = time.perf_counter()
                 b.close()
-                torch.cuda.empty_cache()
                 teardown += time.perf_counter() - tt
             setup += r.setup_s
             scf += r.scf_s
