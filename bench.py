@@ -737,7 +737,8 @@ def main():
                     help="fused: J and K from one build (rijk_vjk_upper_occ_dev); separate: J by its own two passes")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-split", action="store_true", help="skip the split-precision (tcgen05) measurement")
+    ap.add_argument("--no-split", action="store_true",
+                    help="skip the split-precision (tcgen05) measurement and the timing of the other J/K form")
     ap.add_argument("--no-scf", action="store_true", help="skip the water SCF timing")
     ap.add_argument("--no-apps", action="store_true",
                     help="skip the application configs (device tensor build, alkanes, molecule set)")

@@ -36,6 +36,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 
 #include "rijk_common.cuh"
@@ -1171,8 +1172,17 @@ static void half_tc_pair(const Geom& g, const TcGeom& t, const void* Bhi, const 
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   // as many pairs as can be resident at once (an SM without a partner in its
-  // cluster group takes none), at most one per tile
-  static int resident = 0;
+  // cluster group takes none), at most one per tile; cached per device
+  static std::mutex mu;
+  static std::map<int, int> resident_of;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int resident = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = resident_of.find(dev);
+    if (it != resident_of.end()) resident = it->second;
+  }
   if (resident == 0) {
     cfg.gridDim = dim3((unsigned)(2 * (sm_count() / 2)), 1, 1);
     int nc = 0;
@@ -1181,6 +1191,8 @@ static void half_tc_pair(const Geom& g, const TcGeom& t, const void* Bhi, const 
       nc = sm_count() / 2;
     }
     resident = nc;
+    std::lock_guard<std::mutex> lock(mu);
+    resident_of[dev] = nc;
   }
   const int64_t pairs = std::max<int64_t>(1, std::min<int64_t>(ntp, resident));
   cfg.gridDim = dim3((unsigned)(2 * pairs), 1, 1);
