@@ -11,7 +11,7 @@ import json
 import sys
 from pathlib import Path
 
-SETS = ["STO-3G", "def2-SVP", "def2-SVP-JKFIT", "def2-SV(P)-JKFIT"]
+SETS = ["STO-3G", "def2-SVP", "def2-SVP-JKFIT", "def2-SV(P)-JKFIT", "aug-cc-pV5Z"]
 ELEMENTS = ["H", "C", "N", "O", "Cu"]
 
 

@@ -79,3 +79,18 @@ def test_uhf_radical_matches_oracle(ctx):
     got = SCF(mol, "def2-SVP", "def2-SVP-JKFIT", opts, ctx=ctx).run()
     assert ref.converged and got.converged
     assert abs(got.energy - ref.energy) < 1e-9
+
+
+def test_nh3_dimer_cation_uhf_matches_rest(ctx):
+    """(NH3)2+ RI-UHF (aug-cc-pV5Z with h functions on the host integral engine,
+    def2-SV(P)-JKFIT, REST's rimatr J and dm-only K, V^-1/2 metric): REST
+    published -111.9434834841 Eh (examples/RIHF-NH3-dimer/rest.out); the CPU
+    oracle from the same input reproduces it (tests/golden); the GPU SCF must
+    agree with both."""
+    g = json.loads((GOLDEN / "nh3_dimer_cation_rihf.json").read_text())
+    mol = Molecule.from_angstrom(g["symbols"], g["coords_angstrom"], charge=g["charge"], spin=g["spin"])
+    r = SCF(mol, g["basis"], g["auxbas"], ScfOptions(use_ri_symm=True, use_dm_only=True), ctx=ctx).run()
+    assert r.converged
+    assert (r.num_basis, r.num_auxbas) == (g["rest_num_basis"], g["rest_num_auxbas"])
+    assert abs(r.energy - g["rest_energy"]) < 1e-8
+    assert abs(r.energy - g["oracle_energy"]) < 1e-9

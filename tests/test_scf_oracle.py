@@ -98,6 +98,22 @@ def test_pen_rihf_energy_matches_rest():
     assert abs(r.energy - g["pyscf_energy"]) < 2e-7
 
 
+def test_nh3_dimer_cation_fixture_pins_the_oracle_to_rest():
+    """(NH3)2+ RI-UHF in aug-cc-pV5Z (REST examples/RIHF-NH3-dimer): the basis
+    sizes built here equal REST's (734 / 262), and the CPU oracle's SCF from the
+    same input (run by tests/golden/make_golden.py, about four minutes) lands on
+    REST's published energy -111.9434834841 Eh within 1e-9 Eh; PySCF's differs by
+    5e-9 Eh (another Bohr radius)."""
+    import json
+
+    g = json.loads((GOLDEN / "nh3_dimer_cation_rihf.json").read_text())
+    mol = Molecule.from_angstrom(g["symbols"], g["coords_angstrom"], charge=g["charge"], spin=g["spin"])
+    assert (mol.shells(g["basis"]).nfun, mol.shells(g["auxbas"]).nfun) == (g["rest_num_basis"], g["rest_num_auxbas"])
+    assert mol.nelec == 19 and g["spin"] == 2
+    assert abs(g["oracle_energy"] - g["rest_energy"]) < 1e-9
+    assert abs(g["oracle_energy"] - g["pyscf_energy"]) < 2e-8
+
+
 def test_density_difference_factor_is_exact():
     """The signed low-rank factor dD = V S V^T the mixed-precision SCF feeds to
     the split exchange build reproduces the density difference."""
