@@ -17,6 +17,9 @@ class OracleRIJK:
         self.rimatr = None
         self.num_basis = 0
 
+    def spawn(self):
+        return OracleRIJK()
+
     def fit_rimatr(self, metric_factor, int3c, num_basis):
         self.rimatr = O.fit_rimatr(np.asfortranarray(int3c), np.asarray(metric_factor))
         self.num_basis = num_basis

@@ -58,8 +58,14 @@ class RIJK:
         if st != 0:
             raise RijkError(st, f"cannot open an sm_100 context on device {device}")
         self._h = h
+        self.device = int(device)
         self.num_basis = 0
         self.num_auxbas = 0
+
+    def spawn(self) -> "RIJK":
+        """Another context on the same device (for a side calculation that must
+        not replace this context's tensor, such as the atoms of the SAD guess)."""
+        return RIJK(self.device)
 
     # -- plumbing ----------------------------------------------------------
     def close(self):

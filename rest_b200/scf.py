@@ -123,6 +123,7 @@ class SCF:
                  ctx: RIJK | None = None, device: int = 0):
         self.mol, self.opts = mol, opts or ScfOptions()
         self.ctx = ctx or RIJK(device)
+        self.basis_name, self.auxbas_name = basis, auxbas
         t0 = time.perf_counter()
         self.bas, self.aux = mol.shells(basis), mol.shells(auxbas)
         self.n, self.naux = self.bas.nfun, self.aux.nfun
@@ -313,9 +314,21 @@ class SCF:
         return fock, e
 
     def initial_density(self):
-        if self.opts.initial_guess != "hcore":
-            raise ValueError("bundled initial guesses: 'hcore'")
-        vals, vecs = self.diagonalize([self.h_upper] * self.spin_channel)
+        """REST's initial_guess (src/initial_guess/mod.rs:15-80): 'hcore'
+        diagonalises the core Hamiltonian; 'sad' builds the Fock matrix of the
+        superposed atomic densities (dm-only exchange), diagonalises it and
+        takes the density of its orbitals (:46-58)."""
+        if self.opts.initial_guess == "sad":
+            from .sad import sad_density
+
+            make = getattr(self.ctx, "spawn", None)
+            dm0 = sad_density(self.mol, self.basis_name, self.auxbas_name, make)
+            fock, _ = self.hamiltonian(dm0)
+            vals, vecs = self.diagonalize(fock)
+        elif self.opts.initial_guess == "hcore":
+            vals, vecs = self.diagonalize([self.h_upper] * self.spin_channel)
+        else:
+            raise ValueError("bundled initial guesses: 'hcore', 'sad'")
         occ, homo = self.occupation()
         return self.density(vecs, occ, homo), vecs, occ, homo
 

@@ -23,6 +23,7 @@ import numpy as np
 
 from .geometry import water_cluster
 from .guess import LearnedGuess, train
+from .sad import sad_density
 from .scf_batch import run_molecule_set
 
 BASIS, AUXBAS = "def2-SVP", "def2-SVP-JKFIT"
@@ -44,15 +45,27 @@ def evaluate(guess: LearnedGuess, mols, group_size: int = 32) -> dict:
     t_lrn = time.perf_counter() - t0
     t_pred = lrn.timings["setup_parts"].get("guess", 0.0)
     fallback = int(lrn.timings["setup_parts"].get("guess_fallbacks", 0))
+    # REST's SAD guess (src/initial_guess/sad.rs): atomic SCFs once per element,
+    # block-diagonal densities, the first Fock build from them in dm-only form
+    t0 = time.perf_counter()
+    dens = [sad_density(m, BASIS, AUXBAS)[0] for m in mols]
+    t_sad_dens = time.perf_counter() - t0
+    sad = run_molecule_set(mols, BASIS, AUXBAS, group_size=group_size, initial_densities=dens, **CRIT)
+    t_sad = time.perf_counter() - t0
     de = np.abs(np.array(lrn.energies) - np.array(ref.energies))
+    de_sad = np.abs(np.array(sad.energies) - np.array(ref.energies))
     return {
         "molecules": len(mols),
         "hcore": {"iterations_mean": float(np.mean(ref.iterations)), "wall_s": t_ref, "scf_s": ref.scf_s,
                   "converged": int(sum(ref.converged))},
+        "sad": {"iterations_mean": float(np.mean(sad.iterations)), "wall_s": t_sad, "scf_s": sad.scf_s,
+                "density_s": t_sad_dens, "converged": int(sum(sad.converged)),
+                "max_abs_energy_difference_vs_hcore": float(de_sad.max())},
         "learned": {"iterations_mean": float(np.mean(lrn.iterations)), "wall_s": t_lrn, "scf_s": lrn.scf_s,
                     "predict_s": t_pred, "converged": int(sum(lrn.converged)), "fallbacks": int(fallback)},
         "max_abs_energy_difference": float(de.max()),
         "iterations_saved_fraction": float(1.0 - np.mean(lrn.iterations) / np.mean(ref.iterations)),
+        "iterations_saved_fraction_vs_sad": float(1.0 - np.mean(lrn.iterations) / np.mean(sad.iterations)),
     }
 
 

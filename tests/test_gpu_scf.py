@@ -94,3 +94,13 @@ def test_nh3_dimer_cation_uhf_matches_rest(ctx):
     assert (r.num_basis, r.num_auxbas) == (g["rest_num_basis"], g["rest_num_auxbas"])
     assert abs(r.energy - g["rest_energy"]) < 1e-8
     assert abs(r.energy - g["oracle_energy"]) < 1e-9
+
+
+def test_sad_guess_on_the_device(ctx):
+    """REST's SAD guess with the atomic SCFs on device contexts of their own: the
+    molecule's context keeps its tensor, and water converges to the oracle's
+    energy."""
+    g, mol = _golden("water_rihf.json")
+    r = SCF(mol, g["basis"], g["auxbas"], ScfOptions(initial_guess="sad", **TIGHT), ctx=ctx).run()
+    assert r.converged
+    assert abs(r.energy - g["oracle_energy"]) < 1e-9
