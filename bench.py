@@ -583,6 +583,7 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
     from rest_b200.basis import int1e
     from rest_b200.geometry import water_cluster, water_cluster_set_spec
     from rest_b200.guess import LearnedGuess
+    from rest_b200.sad import sad_density
     from rest_b200.scf import SCF, ScfOptions
     from rest_b200.scf_batch import run_molecule_set
 
@@ -608,6 +609,9 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
         t0 = time.perf_counter()
         if kw.pop("learned", False):
             kw["guess"] = guess  # predicted on the device, checked against the driver's S
+        if kw.pop("sad", False):
+            # REST's SAD guess: atomic densities (cached after the first call) on the block diagonal
+            kw["initial_densities"] = [sad_density(m, "def2-SVP", "def2-SVP-JKFIT")[0] for m in mols]
         r = run_molecule_set(mols, "def2-SVP", "def2-SVP-JKFIT", group_size=group, device=device, **kw, **crit)
         wall = time.perf_counter() - t0
         extra = r.timings["setup_parts"].get("guess", 0.0)
@@ -621,8 +625,10 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
                     "setup_parts_s": r.timings["setup_parts"]}
         return r
 
+    sad_density(mols[0], "def2-SVP", "def2-SVP-JKFIT")  # the atomic SCFs, once, untimed like the model load
     ref = timed("batched_fp64", precision="fp64")
     mix = timed("batched_mixed", precision="mixed")
+    timed("batched_mixed_sad", precision="mixed", sad=True)
     lrn = timed("batched_mixed_learned_guess", precision="mixed", learned=True)
     e_ref = np.array(ref.energies)
     res["batched_mixed"]["max_abs_energy_error_vs_fp64"] = float(np.max(np.abs(np.array(mix.energies) - e_ref)))
@@ -652,15 +658,24 @@ def measure_molecule_set(device: int, nmol: int, plain_subset: int = 16, group: 
         for m in mols[:plain_subset]:
             e_plain.append(SCF(m, "def2-SVP", "def2-SVP-JKFIT", popts, ctx=sctx).run().energy)
         wall = time.perf_counter() - t0
+        # the same path from REST's SAD guess (atomic densities already cached)
+        sopts = ScfOptions(scf_acc_etot=1e-8, scf_acc_rho=1e-6, scf_acc_eev=1e-6, initial_guess="sad")
+        t0 = time.perf_counter()
+        for m in mols[:plain_subset]:
+            SCF(m, "def2-SVP", "def2-SVP-JKFIT", sopts, ctx=sctx).run()
+        wall_sad = time.perf_counter() - t0
     sctx.close()
     plain = plain_subset / wall
+    plain_sad = plain_subset / wall_sad
     res["plain_fp64_per_molecule"] = {"molecules_per_s": plain, "molecules_timed": plain_subset,
+                                      "molecules_per_s_from_sad": plain_sad,
                                       "host_cores": cores, "host_blas_threads": blas,
                                       "blas_calibration_s": {str(k): round(v, 3) for k, v in cal.items()},
                                       "max_abs_energy_error_vs_batched_fp64": float(
                                           np.max(np.abs(np.array(e_plain) - e_ref[:plain_subset])))}
-    for tag in ("batched_fp64", "batched_mixed", "batched_mixed_learned_guess"):
+    for tag in ("batched_fp64", "batched_mixed", "batched_mixed_sad", "batched_mixed_learned_guess"):
         res[tag]["speedup_vs_plain_fp64"] = res[tag]["molecules_per_s"] / plain
+        res[tag]["speedup_vs_plain_fp64_from_sad"] = res[tag]["molecules_per_s"] / plain_sad
     res["set"] = f"{nmol} water clusters (H2O)_k, k uniform in 1..16 (seeded), def2-SVP / def2-SVP-JKFIT, " \
                  f"RHF to 1e-8 Eh, groups of {group}, device Cholesky metric"
     res["oracle_subset"] = (f"clusters {sorted(oracle_sub)} (k = {[spec[i][0] for i in sorted(oracle_sub)]}): "

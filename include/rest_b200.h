@@ -411,6 +411,33 @@ int rijk_mlp_to_bf16(const float* src, uint16_t* dst, int64_t count, void* strea
 int rijk_guess_assemble(const float* y, const float* t_mean, const float* t_std, const int32_t* upairs,
                         int64_t npairs, const int32_t* atom_first, const int32_t* atom_type, const int32_t* atom_nfun,
                         const int32_t* atom_water, const double* rot, int64_t num_basis, double* dm, void* stream);
+/* Geometry of the learned guess for a set of water clusters (no counterpart in
+ * REST), all device pointers.  xyz: natom x 3 (A), molecule after molecule,
+ * each molecule O, H, H per water; atom_info: 3 int32 per atom (global index of
+ * its molecule's first atom, the molecule's atom count, element type 0 = O /
+ * 1 = H); table: the 516 constants (40 sample points x 3; for l = 1 then 2 the
+ * Cartesian exponents, the c2s expansion transposed (ncart x (2l+1)) and the
+ * pseudo-inverse of the harmonics at the samples ((2l+1) x 40); cutoff, radial
+ * width, 8 radial centres); elem_shells: per element type 16 int32 (shell
+ * count, then each shell's l, l <= 2, at most 14 functions).  Writes per water
+ * its frame (frames, 9: rows p, b, n) and per water and element the 14 x 14
+ * block rotation (rot, as rijk_guess_assemble reads it); per atom the number of
+ * atoms of its molecule within the cutoff (counts[2a], itself included) and of
+ * those with index >= a (counts[2a+1]), and its 16 radial counts (env). */
+int rijk_guess_geometry(const double* xyz, const int32_t* atom_info, int64_t natom, const double* table,
+                        const int32_t* elem_shells, double* frames, double* rot, int64_t* counts, double* env,
+                        void* stream);
+/* The pair rows of the learned guess from rijk_guess_geometry's output:
+ * pair_off / up_off are the exclusive scans of counts[2a] / counts[2a+1]
+ * (natom each), npairs / nup their totals.  Writes feats (npairs x 53, FP32,
+ * (feature - f_mean) / f_std) for the ordered pairs (A, B) within the cutoff,
+ * atom by atom in ascending B, and upairs (nup x 4 int32: A, B, row of (A, B),
+ * row of (B, A), all relative to the molecule's first atom and first pair row),
+ * the input of rijk_guess_assemble for each molecule. */
+int rijk_guess_pairs(const double* xyz, const int32_t* atom_info, int64_t natom, const double* table,
+                     const double* frames, const double* env, const int64_t* pair_off, const int64_t* up_off,
+                     int64_t npairs, int64_t nup, const double* f_mean, const double* f_std, float* feats,
+                     int32_t* upairs, void* stream);
 
 /* ---- MO-basis three-centre tensor -------------------------------------------- */
 /* generate_ri3mo_rayon / ao2mo_rayon (src/scf_io/mod.rs:2331-2359, :3270-3307):

@@ -18,7 +18,11 @@ back, symmetrised and assembled into the AO density that starts the SCF.
               (O: 14 functions, H: 5 in def2-SVP; unused entries masked),
               standardised per element pair and entry;
   kernels     forward, backward, masked MSE and Adam are the library's own
-              (rijk_mlp_*); torch only holds the device memory;
+              (rijk_mlp_*); at inference the frames, shell rotations, pairs and
+              standardised features of a whole molecule set are built on the
+              device (rijk_guess_geometry, rijk_guess_pairs) and the density is
+              assembled there (rijk_guess_assemble); torch only holds the device
+              memory (the host restatement below builds the training rows);
   fallback    a prediction whose electron count tr(D S) is off by more than 5 %
               (or not finite) is dropped for REST's own guess (hcore here).
 
@@ -49,10 +53,16 @@ DEFAULT_WEIGHTS = Path(__file__).resolve().parent / "data" / "guess_h2o_def2svp.
 # ---------------------------------------------------------------------------
 # geometry: frames, shell rotations, atom blocks
 # ---------------------------------------------------------------------------
+_C2S = {}  # l -> (Cartesian exponents, solid_harmonic_c2s(l)^T): exact-fraction expansion, built once
+
+
 def _harmonics(l: int, u: np.ndarray) -> np.ndarray:
     """Real solid harmonics of degree l at points u (S x 3): S x (2l+1)."""
-    mono = np.stack([u[:, 0] ** i * u[:, 1] ** j * u[:, 2] ** k for i, j, k in cart_components(l)], axis=1)
-    return mono @ solid_harmonic_c2s(l).T
+    if l not in _C2S:
+        _C2S[l] = (cart_components(l), np.ascontiguousarray(solid_harmonic_c2s(l).T))
+    comps, c2s_t = _C2S[l]
+    mono = np.stack([u[:, 0] ** i * u[:, 1] ** j * u[:, 2] ** k for i, j, k in comps], axis=1)
+    return mono @ c2s_t
 
 
 _SAMPLES = np.random.default_rng(12345).standard_normal((40, 3))
@@ -69,22 +79,30 @@ def shell_rotation(l: int, F: np.ndarray) -> np.ndarray:
     return gt.T
 
 
-def water_frames(mol):
-    """Per water (atoms 3w, 3w+1, 3w+2 = O, H1, H2): origin (A) and frame F (rows)."""
-    xyz = np.asarray(mol.coords) * ANG
+@dataclass
+class Frames:
+    xyz: np.ndarray  # (na, 3) coordinates in A
+    origin: np.ndarray  # (nw, 3) each water's O
+    F: np.ndarray  # (nw, 3, 3) each water's frame, axes as rows
+
+
+def water_frames(mol) -> Frames:
+    """Per water (atoms 3w, 3w+1, 3w+2 = O, H1, H2): origin (A) and frame F (rows),
+    all waters at once."""
+    xyz = np.asarray(mol.coords, dtype=np.float64) * ANG
     nw = len(mol.symbols) // 3
-    if [s for s in mol.symbols] != ["O", "H", "H"] * nw:
+    if list(mol.symbols) != ["O", "H", "H"] * nw:
         raise ValueError("the learned guess is trained on water clusters (atoms ordered O, H, H per water)")
-    frames = []
-    for w in range(nw):
-        o, h1, h2 = xyz[3 * w], xyz[3 * w + 1], xyz[3 * w + 2]
-        p = (h1 - o) - (h2 - o)
-        b = (h1 - o) + (h2 - o)
-        p /= np.linalg.norm(p)
-        b -= (b @ p) * p
-        b /= np.linalg.norm(b)
-        frames.append((o, np.stack([p, b, np.cross(p, b)])))
-    return xyz, frames
+    w = xyz.reshape(nw, 3, 3)
+    o, h1, h2 = w[:, 0], w[:, 1] - w[:, 0], w[:, 2] - w[:, 0]
+    p = h1 - h2
+    b = h1 + h2
+    p = p / np.linalg.norm(p, axis=1, keepdims=True)
+    b = b - np.sum(b * p, axis=1, keepdims=True) * p
+    b = b / np.linalg.norm(b, axis=1, keepdims=True)
+    n = np.stack([p[:, 1] * b[:, 2] - p[:, 2] * b[:, 1], p[:, 2] * b[:, 0] - p[:, 0] * b[:, 2],
+                  p[:, 0] * b[:, 1] - p[:, 1] * b[:, 0]], axis=1)
+    return Frames(xyz, o.copy(), np.stack([p, b, n], axis=1))
 
 
 def atom_layout(sh):
@@ -126,10 +144,9 @@ class PairSet:
     kind: np.ndarray  # (P,) 2 * type(A) + type(B)
 
 
-def pair_features(mol) -> PairSet:
-    xyz, frames = water_frames(mol)
-    origin = np.array([o for o, _ in frames])
-    Fs = np.stack([F for _, F in frames])
+def pair_features(mol, frames: Frames | None = None) -> PairSet:
+    fr = frames if frames is not None else water_frames(mol)
+    xyz, Fs = fr.xyz, fr.F
     na = len(mol.symbols)
     typ = np.array([ELEMENT[s] for s in mol.symbols])
     d = np.linalg.norm(xyz[:, None] - xyz[None], axis=-1)
@@ -137,11 +154,11 @@ def pair_features(mol) -> PairSet:
     env = np.concatenate([rad[:, typ == 0].sum(axis=1), rad[:, typ == 1].sum(axis=1)], axis=1)
     A, B = np.nonzero(d <= CUTOFF)
     wa, wb = A // 3, B // 3
-    F = Fs[wa]
-    db = np.einsum("pij,pj->pi", F, xyz[B] - xyz[A])
-    wat = xyz[3 * wb[:, None] + np.arange(3)] - xyz[A][:, None, :]  # B's water, relative to A
-    wat = np.einsum("pij,pkj->pki", F, wat).reshape(len(A), 9)
-    own = np.einsum("pij,pj->pi", F, xyz[A] - origin[wa])
+    loc = np.matmul(xyz, np.transpose(Fs, (0, 2, 1)))  # (nw, na, 3): every atom in every water's axes
+    la = loc[wa, A]
+    db = loc[wa, B] - la
+    wat = (loc[wa[:, None], 3 * wb[:, None] + np.arange(3)] - la[:, None, :]).reshape(len(A), 9)  # B's water
+    own = la - loc[wa, 3 * wa]  # A relative to its own water's O (the frame origin)
     eye = np.eye(2)
     feats = np.concatenate([eye[typ[A]], eye[typ[B]], db, np.linalg.norm(db, axis=1)[:, None],
                             (wa == wb).astype(float)[:, None], wat, own, env[A], env[B]], axis=1)
@@ -152,8 +169,8 @@ class Rotator:
     """Per water w and element: G(F_w), the rotation of that element's AO block
     into the water's frame (every atom of an element has the same shells)."""
 
-    def __init__(self, mol, sh):
-        Fs = np.stack([F for _, F in water_frames(mol)[1]])
+    def __init__(self, mol, sh, frames: Frames | None = None):
+        Fs = (frames if frames is not None else water_frames(mol)).F
         self.layout = atom_layout(sh)
         typ = np.array([ELEMENT[s] for s in mol.symbols])
         self.typ = typ
@@ -200,7 +217,7 @@ def shell_rotations(l: int, Fs: np.ndarray) -> np.ndarray:
         return np.ones((len(Fs), 1, 1))
     if l not in _PINV:
         _PINV[l] = np.linalg.pinv(_harmonics(l, _SAMPLES))
-    pts = np.einsum("sj,wjk->wsk", _SAMPLES, Fs).reshape(-1, 3)  # rows: F^T u_s for every frame
+    pts = np.matmul(_SAMPLES, Fs).reshape(-1, 3)  # rows: F^T u_s for every frame
     y_rot = _harmonics(l, pts).reshape(len(Fs), len(_SAMPLES), 2 * l + 1)
     return np.transpose(_PINV[l] @ y_rot, (0, 2, 1))
 
@@ -217,11 +234,11 @@ def local_blocks(mol, sh, D: np.ndarray, ps: PairSet):
     return T.reshape(len(ps.pairs), -1), M.reshape(len(ps.pairs), -1)
 
 
-def assembly_inputs(mol, sh, ps: PairSet):
+def assembly_inputs(mol, sh, ps: PairSet, rot: Rotator | None = None):
     """Host arrays of the device assembly (rijk_guess_assemble): unordered pairs
     (A, B, row of (A, B), row of (B, A)), per-atom first AO / type / AO count /
     water, and per water and element the 14 x 14 block rotation."""
-    rot = Rotator(mol, sh)
+    rot = rot if rot is not None else Rotator(mol, sh)
     na = len(mol.symbols)
     nw = na // 3
     R = np.zeros((nw, 2, BLOCK, BLOCK))
@@ -266,6 +283,113 @@ def _ck(st: int, what: str):
 
 def _p(t):
     return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+_GEO_TABLE = []  # the constants of rijk_guess_geometry, built once
+
+
+def geometry_table() -> np.ndarray:
+    """The 516 constants of the device geometry (rijk_guess_geometry): the 40
+    sample points; for l = 1, 2 the Cartesian exponents, the c2s expansion
+    transposed and the pseudo-inverse of the harmonics at the samples (the fit
+    shell_rotations makes); the cutoff, the radial width and the 8 centres."""
+    if not _GEO_TABLE:
+        parts = [_SAMPLES.ravel()]
+        for l in (1, 2):
+            if l not in _PINV:
+                _PINV[l] = np.linalg.pinv(_harmonics(l, _SAMPLES))
+            parts += [np.asarray(cart_components(l), dtype=np.float64).ravel(), solid_harmonic_c2s(l).T.ravel(),
+                      _PINV[l].ravel()]
+        parts += [np.array([CUTOFF, RAD_SIGMA]), RAD_MU]
+        t = np.ascontiguousarray(np.concatenate(parts), dtype=np.float64)
+        if t.size != 516:
+            raise AssertionError("geometry table layout")
+        _GEO_TABLE.append(t)
+    return _GEO_TABLE[0]
+
+
+@dataclass
+class DevicePairs:
+    """A molecule set's pair rows on the device (rijk_guess_geometry +
+    rijk_guess_pairs): standardised features (P x 53, FP32), unordered pairs
+    (U x 4 int32, molecule-relative), per atom first AO / type / AO count / water
+    (int32, molecule-relative), per water the block rotations; and on the host
+    the offsets of each molecule's rows (nmol + 1 each) and its AO count."""
+    feats: object
+    up: object
+    first: object
+    typ: object
+    nfun: object
+    water: object
+    rot: object
+    pair_off: np.ndarray
+    up_off: np.ndarray
+    atom_off: np.ndarray
+    nbas: np.ndarray
+
+
+def device_pairs(mols, basis: str, norm: Normaliser, dev) -> DevicePairs:
+    """The pair rows of a set of water clusters, built on the device; the host
+    sends coordinates and the per-atom layout, and reads back one scan."""
+    import torch
+
+    na = np.array([len(m.symbols) for m in mols], dtype=np.int64)
+    for m in mols:
+        if not m.symbols or list(m.symbols) != ["O", "H", "H"] * (len(m.symbols) // 3):
+            raise ValueError("the learned guess is trained on water clusters (atoms ordered O, H, H per water)")
+    atom_off = np.concatenate([[0], np.cumsum(na)])
+    natom = int(atom_off[-1])
+    if natom == 0:
+        raise ValueError("empty molecule set")
+    # every atom of an element carries that element's shells (one basis per element)
+    ref = mols[0].shells(basis)
+    shells = {t: [int(l) for l in ref.l[ref.atom == t]] for t in (0, 1)}
+    size = np.array([sum(2 * l + 1 for l in shells[t]) for t in (0, 1)], dtype=np.int64)
+    if max(size) > BLOCK or any(l > 2 for t in (0, 1) for l in shells[t]) or any(len(s) > 15 for s in shells.values()):
+        raise ValueError("the learned guess covers blocks of at most 14 functions with l <= 2")
+    typ = np.tile(np.array([0, 1, 1], dtype=np.int32), natom // 3)
+    nf = size[typ]
+    csum = np.cumsum(nf)
+    mstart = np.repeat(atom_off[:-1], na)
+    first = (csum - nf - np.concatenate([[0], csum])[mstart]).astype(np.int32)
+    nbas = np.add.reduceat(nf, atom_off[:-1]).astype(np.int64)
+    for m, nb in zip(mols, nbas):
+        sh = m.shells(basis)
+        if sh.nfun != nb or np.any(np.diff(sh.atom) < 0):
+            raise ValueError("shells of an atom must be contiguous and follow the element's basis")
+    info = np.stack([mstart, np.repeat(na, na), typ], axis=1).astype(np.int32)
+    water = ((np.arange(natom) - mstart) // 3).astype(np.int32)
+    xyz = np.concatenate([np.asarray(m.coords, dtype=np.float64) for m in mols]) * ANG
+    es = np.zeros((2, 16), dtype=np.int32)
+    for t in (0, 1):
+        es[t, 0] = len(shells[t])
+        es[t, 1:1 + len(shells[t])] = shells[t]
+
+    def dv(a, dtype):
+        return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).to(dev, non_blocking=False)
+
+    x_d, info_d = dv(xyz, torch.float64), dv(info, torch.int32)
+    tab_d, es_d = dv(geometry_table(), torch.float64), dv(es, torch.int32)
+    lay = dv(np.stack([first, typ, nf.astype(np.int32), water]), torch.int32)  # rows: first, type, nfun, water
+    nw = natom // 3
+    frames = torch.empty(nw, 9, dtype=torch.float64, device=dev)
+    rot = torch.empty(nw, 2, BLOCK, BLOCK, dtype=torch.float64, device=dev)
+    counts = torch.empty(natom, 2, dtype=torch.int64, device=dev)
+    env = torch.empty(natom, 16, dtype=torch.float64, device=dev)
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    _ck(lib().rijk_guess_geometry(_p(x_d), _p(info_d), natom, _p(tab_d), _p(es_d), _p(frames), _p(rot), _p(counts),
+                                  _p(env), stream), "guess_geometry")
+    incl = torch.cumsum(counts, dim=0)
+    excl = (incl - counts).t().contiguous()  # rows: pair offsets, unordered-pair offsets
+    incl_h = incl.cpu().numpy()  # the one host read: each molecule's pair and unordered-pair rows
+    start = np.concatenate([np.zeros((1, 2), dtype=np.int64), incl_h])[atom_off]
+    npairs, nup = int(start[-1, 0]), int(start[-1, 1])
+    feats = torch.empty(npairs, NFEAT, dtype=torch.float32, device=dev)
+    up = torch.empty(nup, 4, dtype=torch.int32, device=dev)
+    fm, fs = dv(norm.f_mean, torch.float64), dv(norm.f_std, torch.float64)
+    _ck(lib().rijk_guess_pairs(_p(x_d), _p(info_d), natom, _p(tab_d), _p(frames), _p(env), _p(excl[0]),
+                               _p(excl[1]), npairs, nup, _p(fm), _p(fs), _p(feats), _p(up), stream), "guess_pairs")
+    return DevicePairs(feats, up, lay[0], lay[1], lay[2], lay[3], rot, start[:, 0], start[:, 1], atom_off, nbas)
 
 
 class PairMLP:
@@ -523,15 +647,45 @@ class LearnedGuess:
     def density(self, mol, ovlp: np.ndarray | None = None, tol: float = 0.05, on_device: bool = False):
         """Predicted AO density (host array, or device tensor with on_device),
         or None when its electron count tr(D S) is off by more than ``tol``."""
+        D = self.densities([mol], None if ovlp is None else [ovlp], tol)[0]
+        return D if D is None or on_device else D.cpu().numpy()
+
+    def densities(self, mols, ovlps: list | None = None, tol: float = 0.05) -> list:
+        """density() for a molecule set, on the device: pair rows built by the
+        geometry kernels, one network pass over the pairs of every molecule,
+        one assembly launch per molecule, and one host read of all electron
+        counts.  Returns device tensors (n x n, FP64), None where the
+        electron-count check fails."""
         import torch
 
-        sh = mol.shells(self.basis)
-        ps = pair_features(mol)
-        D = self.assemble_device(mol, sh, ps, self._forward(ps))
-        if ovlp is not None:
-            S = ovlp if torch.is_tensor(ovlp) else torch.as_tensor(np.asarray(ovlp), device=D.device)
-            ne = float((D * S).sum())
-            if not np.isfinite(ne) or abs(ne - mol.nelec) > tol * mol.nelec:
-                return None
-            D *= mol.nelec / ne
-        return D if on_device else D.cpu().numpy()
+        dev = self.net.dev
+        if not mols:
+            return []
+        if not hasattr(self, "_tstats"):
+            self._tstats = (torch.tensor(self.norm.t_mean, dtype=torch.float32, device=dev),
+                            torch.tensor(self.norm.t_std, dtype=torch.float32, device=dev))
+        g = device_pairs(mols, self.basis, self.norm, dev)
+        y = self.net.forward(self.net.to_bf16(g.feats))
+        tm, ts = self._tstats
+        out = []
+        for i in range(len(mols)):
+            p0, p1 = int(g.pair_off[i]), int(g.pair_off[i + 1])
+            u0, u1 = int(g.up_off[i]), int(g.up_off[i + 1])
+            a0, a1 = int(g.atom_off[i]), int(g.atom_off[i + 1])
+            n = int(g.nbas[i])
+            D = torch.empty(n, n, dtype=torch.float64, device=dev)
+            _ck(lib().rijk_guess_assemble(_p(y[p0:p1]), _p(tm), _p(ts), _p(g.up[u0:u1]), u1 - u0,
+                                          _p(g.first[a0:a1]), _p(g.typ[a0:a1]), _p(g.nfun[a0:a1]),
+                                          _p(g.water[a0:a1]), _p(g.rot[a0 // 3:a1 // 3]), n, _p(D), self.net.stream),
+                "guess_assemble")
+            out.append(D)
+        if ovlps is None:
+            return out
+        ne = torch.stack([(D * (S if torch.is_tensor(S) else torch.as_tensor(np.asarray(S), device=dev))).sum()
+                          for D, S in zip(out, ovlps)]).cpu().numpy()
+        for i, mol in enumerate(mols):
+            if not np.isfinite(ne[i]) or abs(ne[i] - mol.nelec) > tol * mol.nelec:
+                out[i] = None
+            else:
+                out[i] *= mol.nelec / ne[i]
+        return out

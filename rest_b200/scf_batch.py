@@ -649,8 +649,8 @@ class BatchedRHF:
         fails the check starts from hcore."""
         if guess is not None:
             t0 = time.perf_counter()
-            initial_densities = [guess.density(m, ovlp=self.S[i, :self.n[i], :self.n[i]], on_device=True)
-                                 for i, m in enumerate(self.mols)]
+            initial_densities = guess.densities(self.mols, [self.S[i, :self.n[i], :self.n[i]]
+                                                            for i in range(len(self.mols))])
             self.setup_parts["guess"] = self.setup_parts.get("guess", 0.0) + time.perf_counter() - t0
             self.setup_parts["guess_fallbacks"] = self.setup_parts.get("guess_fallbacks", 0) + sum(
                 d is None for d in initial_densities)

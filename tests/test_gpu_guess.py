@@ -189,3 +189,55 @@ def test_device_assembly_matches_host_assembly(k):
     got = guess.assemble_device(mol, sh, ps, y).cpu().numpy()
     assert np.max(np.abs(got - ref)) <= 1e-6 * np.max(np.abs(ref))
     assert np.array_equal(got, got.T)
+
+
+def test_device_pair_rows_match_host():
+    """rijk_guess_geometry + rijk_guess_pairs over a molecule set of uneven
+    sizes against the host restatement (pair_features, Rotator,
+    assembly_inputs): the same pairs in the same order, the same unordered-pair
+    rows, layout and rotations; features equal to FP32 rounding of the
+    standardised values."""
+    from rest_b200.guess import Rotator, assembly_inputs, device_pairs, pair_features, water_frames
+
+    guess = LearnedGuess.load()
+    mols = [water_cluster(k, seed=300 + k) for k in (1, 2, 7, 16, 3, 24)]
+    g = device_pairs(mols, guess.basis, guess.norm, torch.device("cuda"))
+    feats, up = g.feats.cpu().numpy(), g.up.cpu().numpy()
+    rot = g.rot.cpu().numpy()
+    lay = [t.cpu().numpy() for t in (g.first, g.typ, g.nfun, g.water)]
+    for i, m in enumerate(mols):
+        sh = m.shells(guess.basis)
+        fr = water_frames(m)
+        ps = pair_features(m, fr)
+        r = Rotator(m, sh, fr)
+        h_up, h_first, h_typ, h_nfun, h_water, h_rot = assembly_inputs(m, sh, ps, r)
+        p0, p1 = g.pair_off[i], g.pair_off[i + 1]
+        a0, a1 = g.atom_off[i], g.atom_off[i + 1]
+        assert p1 - p0 == len(ps.pairs) and g.nbas[i] == sh.nfun
+        ref = guess.norm.feats(ps.feats)
+        assert np.max(np.abs(feats[p0:p1] - ref)) <= 2e-6 * max(1.0, np.abs(ref).max())
+        assert np.array_equal(up[g.up_off[i]:g.up_off[i + 1]], h_up)
+        for got, want in zip(lay, (h_first, h_typ, h_nfun, h_water)):
+            assert np.array_equal(got[a0:a1], want)
+        assert np.max(np.abs(rot[a0 // 3:a1 // 3] - h_rot)) <= 1e-12
+
+
+def test_batched_densities_match_single_molecule_path():
+    """densities() over a set (device pair rows, one network pass) gives each
+    molecule the density of the host-feature path for that molecule alone, and
+    the electron-count check scales it to the molecule's electrons."""
+    from rest_b200.basis import int1e
+    from rest_b200.guess import pair_features
+
+    guess = LearnedGuess.load()
+    mols = [water_cluster(k, seed=500 + k) for k in (2, 9, 16, 5)]
+    ovl = [int1e(m, m.shells(guess.basis), "ovlp") for m in mols]
+    got = guess.densities(mols, ovl)
+    for m, s, d in zip(mols, ovl, got):
+        sh = m.shells(guess.basis)
+        ps = pair_features(m)
+        ref = guess.assemble_device(m, sh, ps, guess._forward(ps)).cpu().numpy()
+        ref *= m.nelec / float(np.sum(ref * s))
+        assert d is not None
+        assert np.max(np.abs(d.cpu().numpy() - ref)) <= 1e-10 * np.max(np.abs(ref))
+        assert abs(float(np.sum(d.cpu().numpy() * s)) - m.nelec) < 1e-9
