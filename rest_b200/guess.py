@@ -328,11 +328,25 @@ class DevicePairs:
     nbas: np.ndarray
 
 
-def device_pairs(mols, basis: str, norm: Normaliser, dev) -> DevicePairs:
-    """The pair rows of a set of water clusters, built on the device; the host
-    sends coordinates and the per-atom layout, and reads back one scan."""
-    import torch
+@dataclass
+class PairLayout:
+    """Host side of device_pairs: coordinates (A) and per-atom layout of a set
+    of water clusters, molecule after molecule."""
+    xyz: np.ndarray  # (natom, 3)
+    info: np.ndarray  # (natom, 3) int32: first atom of the molecule, its atom count, element type
+    first: np.ndarray  # (natom,) int32 first AO within the molecule
+    typ: np.ndarray  # (natom,) int32 0 = O, 1 = H
+    nfun: np.ndarray  # (natom,) int32 AO count
+    water: np.ndarray  # (natom,) int32 water index within the molecule
+    elem_shells: np.ndarray  # (2, 16) int32 per element: shell count, then each shell's l
+    atom_off: np.ndarray  # (nmol + 1,) first atom of each molecule
+    nbas: np.ndarray  # (nmol,) AO count of each molecule
 
+
+def pair_layout(mols, basis: str) -> PairLayout:
+    """The per-atom layout the geometry kernels take, vectorised over the set;
+    every atom of an element carries that element's shells (one basis per
+    element), checked against each molecule's AO count."""
     na = np.array([len(m.symbols) for m in mols], dtype=np.int64)
     for m in mols:
         if not m.symbols or list(m.symbols) != ["O", "H", "H"] * (len(m.symbols) // 3):
@@ -341,11 +355,10 @@ def device_pairs(mols, basis: str, norm: Normaliser, dev) -> DevicePairs:
     natom = int(atom_off[-1])
     if natom == 0:
         raise ValueError("empty molecule set")
-    # every atom of an element carries that element's shells (one basis per element)
     ref = mols[0].shells(basis)
     shells = {t: [int(l) for l in ref.l[ref.atom == t]] for t in (0, 1)}
     size = np.array([sum(2 * l + 1 for l in shells[t]) for t in (0, 1)], dtype=np.int64)
-    if max(size) > BLOCK or any(l > 2 for t in (0, 1) for l in shells[t]) or any(len(s) > 15 for s in shells.values()):
+    if max(size) > BLOCK or any(l > 2 for t in (0, 1) for l in shells[t]) or any(len(v) > 15 for v in shells.values()):
         raise ValueError("the learned guess covers blocks of at most 14 functions with l <= 2")
     typ = np.tile(np.array([0, 1, 1], dtype=np.int32), natom // 3)
     nf = size[typ]
@@ -357,20 +370,31 @@ def device_pairs(mols, basis: str, norm: Normaliser, dev) -> DevicePairs:
         sh = m.shells(basis)
         if sh.nfun != nb or np.any(np.diff(sh.atom) < 0):
             raise ValueError("shells of an atom must be contiguous and follow the element's basis")
-    info = np.stack([mstart, np.repeat(na, na), typ], axis=1).astype(np.int32)
-    water = ((np.arange(natom) - mstart) // 3).astype(np.int32)
-    xyz = np.concatenate([np.asarray(m.coords, dtype=np.float64) for m in mols]) * ANG
     es = np.zeros((2, 16), dtype=np.int32)
     for t in (0, 1):
         es[t, 0] = len(shells[t])
         es[t, 1:1 + len(shells[t])] = shells[t]
+    return PairLayout(xyz=np.concatenate([np.asarray(m.coords, dtype=np.float64) for m in mols]) * ANG,
+                      info=np.stack([mstart, np.repeat(na, na), typ], axis=1).astype(np.int32), first=first, typ=typ,
+                      nfun=nf.astype(np.int32), water=((np.arange(natom) - mstart) // 3).astype(np.int32),
+                      elem_shells=es, atom_off=atom_off, nbas=nbas)
+
+
+def device_pairs(mols, basis: str, norm: Normaliser, dev) -> DevicePairs:
+    """The pair rows of a set of water clusters, built on the device; the host
+    sends coordinates and the per-atom layout, and reads back one scan."""
+    import torch
+
+    lo = pair_layout(mols, basis)
+    natom = len(lo.typ)
+    atom_off, nbas = lo.atom_off, lo.nbas
 
     def dv(a, dtype):
         return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).to(dev, non_blocking=False)
 
-    x_d, info_d = dv(xyz, torch.float64), dv(info, torch.int32)
-    tab_d, es_d = dv(geometry_table(), torch.float64), dv(es, torch.int32)
-    lay = dv(np.stack([first, typ, nf.astype(np.int32), water]), torch.int32)  # rows: first, type, nfun, water
+    x_d, info_d = dv(lo.xyz, torch.float64), dv(lo.info, torch.int32)
+    tab_d, es_d = dv(geometry_table(), torch.float64), dv(lo.elem_shells, torch.int32)
+    lay = dv(np.stack([lo.first, lo.typ, lo.nfun, lo.water]), torch.int32)  # rows: first, type, nfun, water
     nw = natom // 3
     frames = torch.empty(nw, 9, dtype=torch.float64, device=dev)
     rot = torch.empty(nw, 2, BLOCK, BLOCK, dtype=torch.float64, device=dev)

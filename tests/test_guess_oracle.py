@@ -79,3 +79,35 @@ def test_oracle_gradients_match_finite_differences():
             fd = (mo.network_loss_and_grads(x, wp, bs, t, mask, 13.0)[0]
                   - mo.network_loss_and_grads(x, wm, bs, t, mask, 13.0)[0]) / (2 * h)
             assert abs(fd - grads[li][0][i, j]) < 1e-7 * max(1.0, abs(fd))
+
+
+def test_pair_layout_and_row_arithmetic_match_host_assembly_inputs():
+    """The host half of the device geometry (pair_layout) and, restated in
+    NumPy, the row arithmetic of the pair kernel (rows at the exclusive scan of
+    the neighbour counts; the row of (B, A) from B's neighbours before A) give
+    the host assembly inputs of every molecule of a set of uneven sizes."""
+    from rest_b200.guess import CUTOFF, assembly_inputs, geometry_table, pair_layout
+
+    mols = [water_cluster(k, seed=40 + k) for k in (1, 4, 2, 9)]
+    lo = pair_layout(mols, "def2-SVP")
+    assert geometry_table().size == 516
+    assert list(lo.elem_shells[0, :7]) == [6, 0, 0, 0, 1, 1, 2] and list(lo.elem_shells[1, :4]) == [3, 0, 0, 1]
+    for i, m in enumerate(mols):
+        a0, a1 = lo.atom_off[i], lo.atom_off[i + 1]
+        sh = m.shells("def2-SVP")
+        ps = pair_features(m)
+        up, first, typ, nfun, water, _ = assembly_inputs(m, sh, ps)
+        for got, want in ((lo.first, first), (lo.typ, typ), (lo.nfun, nfun), (lo.water, water)):
+            assert np.array_equal(got[a0:a1], want)
+        assert lo.nbas[i] == sh.nfun
+        assert np.all(lo.info[a0:a1, 0] == a0) and np.all(lo.info[a0:a1, 1] == a1 - a0)
+        x = lo.xyz[a0:a1]
+        near = np.linalg.norm(x[:, None] - x[None], axis=-1) <= CUTOFF
+        off = np.concatenate([[0], np.cumsum(near.sum(axis=1))])
+        rows = []
+        for a in range(a1 - a0):
+            nb = np.nonzero(near[a])[0]
+            for r, b in enumerate(nb):
+                if b >= a:
+                    rows.append((a, b, off[a] + r, off[b] + int(near[b, :a].sum())))
+        assert np.array_equal(np.array(rows, dtype=np.int32), up)
