@@ -200,6 +200,8 @@ int sync_and_check(rijk_ctx* ctx, cudaStream_t st) {
     RIJK_CK(cudaMemset(ctx->d_err, 0, sizeof(int)));
     if (h == rijk::DEV_NONFINITE)
       return set_err(ctx, RIJK_ERR_NONFINITE, "a density, orbital or occupation element read was NaN or Inf");
+    if (h == rijk::DEV_TENSOR_MAP)
+      return set_err(ctx, RIJK_ERR_CUDA, "a tensor map of the split exchange could not be encoded");
     return set_err(ctx, RIJK_ERR_TIMEOUT, "a device-side wait exceeded its time budget");
   }
   return RIJK_OK;

@@ -50,6 +50,7 @@ enum DevErr : int {
   DEV_OK = 0,
   DEV_WAIT_TIMEOUT = 1,
   DEV_NONFINITE = 2,
+  DEV_TENSOR_MAP = 3,  // set by the host: a kernel's tensor map could not be encoded, nothing was launched
 };
 
 // The error word a kernel receives is the first of four ints a context owns:

@@ -470,9 +470,11 @@ __global__ void __launch_bounds__(256) k_tc_wreduce(const double* __restrict__ w
 // stage is then A (32 KB) + half of V, and V crosses from L2 once per pair.
 //
 // Synchronisation (one MMA issuer, thread 32 of CTA 0):
-//  * each CTA's producer fills its own stage and arms its own full[s];
-//  * CTA 1's thread 32 waits its full[s] and arrives on CTA 0's pfull[s], so
-//    CTA 0 issues only when both halves of the stage have landed;
+//  * CTA 0's producer arms CTA 0's full[s] with the bytes of both CTAs' halves;
+//    both CTAs' producers fill their own stage with tiled tensor copies of the
+//    .cta_group::2 form whose completion lands on CTA 0's full[s] (no
+//    multicast: each CTA reads only its own operands), so the issuer waits on
+//    one local barrier per stage;
 //  * the issuer's commits arrive on empty[s] and acc_full[b] of both CTAs
 //    (commit multicast over the pair);
 //  * the four epilogue warps of each CTA arrive on CTA 0's acc_empty[b]
@@ -564,23 +566,47 @@ __device__ __forceinline__ void tc2_commit_pair(uint64_t* bar) {
                : "memory");
 }
 
+// Tiled tensor copies (this GPU's memory, no multicast) into this CTA's shared
+// memory whose completion is counted on the mbarrier at shared::cluster address
+// `bar`, which may belong to the other CTA of the pair.
+__device__ __forceinline__ void tma2_load_2d(void* smem_dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+      "%3}], [%4];" ::"r"(smem_u32(smem_dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma2_load_3d(void* smem_dst, const CUtensorMap* map, int x, int y, int z,
+                                             uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+      "%3, %4}], [%5];" ::"r"(smem_u32(smem_dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
+// Operand maps of the paired kernel: direct blocks of a split plane as rows of
+// 64 BF16 (box 64 x 128: one 16 KB block), the mirrored halves (mirror_map), and
+// the halves of V as rows of 64 BF16 (box 64 x npad/2).
+struct PairMaps {
+  CUtensorMap dhi, dlo, mhi, mlo, vhi, vlo;
+};
+
 template <int NPAD>
 __global__ void __launch_bounds__(192, 1)
-    k_half_tc_pair(const __nv_bfloat16* __restrict__ Bhi, const __nv_bfloat16* __restrict__ Blo, int nmb, int nkb,
-                   const __nv_bfloat16* __restrict__ Vhi, const __nv_bfloat16* __restrict__ Vlo, int nib, int64_t np,
-                   int64_t ntp, __nv_bfloat16* __restrict__ Xhi, __nv_bfloat16* __restrict__ Xlo, int* err,
-                   const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo, int use_tm,
-                   int64_t p0) {
+    k_half_tc_pair(int nmb, int nkb, int nib, int64_t np, int64_t ntp, __nv_bfloat16* __restrict__ Xhi,
+                   __nv_bfloat16* __restrict__ Xlo, int* err, const __grid_constant__ PairMaps maps, int64_t p0,
+                   const double* __restrict__ Vd, int64_t ldv, int ncols, int nrows, double* __restrict__ wpart) {
   const int64_t nsq = (int64_t)nmb * (nmb + 1) / 2;
   using C = HalfTcPair<NPAD>;
   constexpr int S = C::STAGES;
   constexpr int NH = NPAD / 2;  // V columns (B rows) per CTA
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_BYTES);  // used in CTA 0
   uint64_t* empty = full + S;
-  uint64_t* pfull = empty + S;
-  uint64_t* acc_full = pfull + S;      // [2]
+  uint64_t* acc_full = empty + S;      // [2]
   uint64_t* acc_empty = acc_full + 2;  // [2], used in CTA 0
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -592,7 +618,6 @@ __global__ void __launch_bounds__(192, 1)
     for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
-      mbar_init(&pfull[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
@@ -620,30 +645,23 @@ __global__ void __launch_bounds__(192, 1)
         ok = __shfl_sync(0xffffffffu, ok, 0);
         if (!ok) break;
         uint8_t* st = smem + s * C::STAGE_BYTES;
-        if (lane == 0) mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
+        const uint32_t fb = cluster_addr(&full[s], 0);
+        if (lane == 0 && rank == 0) mbar_arrive_expect_tx(&full[s], 2 * C::STAGE_BYTES);
         __syncwarp();
         const int Kb = kb >> 1, j = kb & 1;
         if (mb <= Kb) {
-          const int64_t boff = ((pl * nsq + sq_index(mb, Kb)) * 2 + j) * BLOCK_ELEMS;
-          if (lane == 0) bulk_g2s(st, Bhi + boff, BLOCK_BYTES, &full[s]);
-          if (lane == 1) bulk_g2s(st + BLOCK_BYTES, Blo + boff, BLOCK_BYTES, &full[s]);
-        } else if (use_tm) {
-          const int z = (int)(((p0 + pl) * nsq + sq_index(Kb, mb)) * 16);
-          if (lane == 0) tma_load_3d(st, &tm_hi, 0, 2 * j, z, &full[s]);
-          if (lane == 1) tma_load_3d(st + BLOCK_BYTES, &tm_lo, 0, 2 * j, z, &full[s]);
+          const int y = (int)((((p0 + pl) * nsq + sq_index(mb, Kb)) * 2 + j) * TC_M);
+          if (lane == 0) tma2_load_2d(st, &maps.dhi, 0, y, fb);
+          if (lane == 1) tma2_load_2d(st + BLOCK_BYTES, &maps.dlo, 0, y, fb);
         } else {
-          const int64_t sbase = (pl * nsq + sq_index(Kb, mb)) * 2 * BLOCK_ELEMS + (int64_t)(8 * j) * 64;
-          const int run = lane & 15;
-          const int64_t src = sbase + (int64_t)(run >> 3) * BLOCK_ELEMS + (int64_t)((run & 7) * (TC_M / 8)) * 64;
-          if (lane < 16)
-            bulk_g2s(st + run * 1024, Bhi + src, 1024, &full[s]);
-          else
-            bulk_g2s(st + BLOCK_BYTES + run * 1024, Blo + src, 1024, &full[s]);
+          const int z = (int)(((p0 + pl) * nsq + sq_index(Kb, mb)) * 16);
+          if (lane == 0) tma2_load_3d(st, &maps.mhi, 0, 2 * j, z, fb);
+          if (lane == 1) tma2_load_3d(st + BLOCK_BYTES, &maps.mlo, 0, 2 * j, z, fb);
         }
         // V in halves: stage kb holds half 0 then half 1, each (NH x 64) K-major
-        const int64_t voff = ((int64_t)kb * 2 + rank) * NH * TC_KB;
-        if (lane == 2) bulk_g2s(st + 2 * BLOCK_BYTES, Vhi + voff, C::VH_BYTES, &full[s]);
-        if (lane == 3) bulk_g2s(st + 2 * BLOCK_BYTES + C::VH_BYTES, Vlo + voff, C::VH_BYTES, &full[s]);
+        const int yv = (kb * 2 + (int)rank) * NH;
+        if (lane == 2) tma2_load_2d(st + 2 * BLOCK_BYTES, &maps.vhi, 0, yv, fb);
+        if (lane == 3) tma2_load_2d(st + 2 * BLOCK_BYTES + C::VH_BYTES, &maps.vlo, 0, yv, fb);
       }
     }
   } else if (warp == 1) {
@@ -660,8 +678,7 @@ __global__ void __launch_bounds__(192, 1)
         for (int kb = 0; kb < nkb && ok; ++kb) {
           const int64_t g = lt * nkb + kb;
           const int s = (int)(g % S);
-          ok = mbar_wait_cluster_bounded(&full[s], (uint32_t)((g / S) & 1), err) &&
-               mbar_wait_cluster_bounded(&pfull[s], (uint32_t)((g / S) & 1), err);
+          ok = mbar_wait_cluster_bounded(&full[s], (uint32_t)((g / S) & 1), err);
           if (!ok) break;
           tc_fence_after();
           const uint8_t* st = smem + s * C::STAGE_BYTES;
@@ -684,16 +701,6 @@ __global__ void __launch_bounds__(192, 1)
         }
         tc2_commit_pair(&acc_full[b]);
       }
-    } else if (lane == 0) {
-      // CTA 1: tell CTA 0's issuer when this CTA's half of each stage has landed
-      const uint32_t remote = 0;
-      for (int64_t lt = 0; lt < my_tiles && ok; ++lt)
-        for (int kb = 0; kb < nkb && ok; ++kb) {
-          const int64_t g = lt * nkb + kb;
-          const int s = (int)(g % S);
-          ok = mbar_wait_cluster_bounded(&full[s], (uint32_t)((g / S) & 1), err);
-          if (ok) mbar_arrive_cluster(cluster_addr(&pfull[s], remote));
-        }
     }
   } else {
     // epilogue warps 2..5: this CTA's 128 rows of accumulator b
@@ -712,12 +719,20 @@ __global__ void __launch_bounds__(192, 1)
       const int64_t tile = pair + lt * NPR;
       const int64_t pl = 2 * (tile / nmb) + (int64_t)rank;
       const int mb = (int)(tile % nmb);
+      const int row = mb * TC_M + m;
+      double jacc = 0.0;
       if (pl < np) {
         const int64_t xbase = ((pl * nmb + mb) * (int64_t)nib) * BLOCK_ELEMS;
 #pragma unroll 1
         for (int c0 = 0; c0 < NPAD; c0 += 32) {
           float v[32];
           tc_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * NPAD + c0), v);
+          // with wpart: this row's share of J's scalar <V, X_P> (V in FP64)
+          if (wpart && row < nrows) {
+#pragma unroll 8
+            for (int jj = 0; jj < 32 && c0 + jj < ncols; ++jj)
+              jacc = fma((double)v[jj], Vd[(int64_t)(c0 + jj) * ldv + row], jacc);
+          }
           const int ib = c0 / TC_KB;
 #pragma unroll
           for (int gq = 0; gq < 4; ++gq) {
@@ -733,6 +748,11 @@ __global__ void __launch_bounds__(192, 1)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive_cluster(b ? acc_empty1 : acc_empty0);
+      if (wpart && pl < np) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) jacc += __shfl_xor_sync(0xffffffffu, jacc, o);
+        if (lane == 0) wpart[(pl * nmb + mb) * 4 + quad] = jacc;
+      }
     }
   }
   tc_fence_before();
@@ -1008,6 +1028,8 @@ __global__ void __launch_bounds__(256) k_rank_tc_finalize(int64_t n, int64_t npa
 // ============================================================================
 // host launchers
 // ============================================================================
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
+
 TcGeom make_tc_geom(const Geom& g, int ncols) {
   TcGeom t;
   t.nmb = (int)cdiv_t(g.n, TC_M);
@@ -1017,18 +1039,23 @@ TcGeom make_tc_geom(const Geom& g, int ncols) {
   t.block_elems = BLOCK_ELEMS;
   // SM-pair (cta_group::2) kernels: measured on B200 at n = 600 / 1200, the
   // paired rank update is faster from about eight 128-row blocks on (5.46 vs
-  // 6.25 ms at n = 1200, slower at n = 600 where each CTA has few k steps),
-  // and the paired half-transform is not (10.0 vs 9.3 ms at n = 1200).
-  // RIJK_TC_PAIR=0 / 1 turns both off / on.
+  // 6.25 ms at n = 1200, slower at n = 600 where each CTA has few k steps);
+  // the paired half-transform, its copies completing on CTA 0's barrier, is
+  // faster at n = 1200 (8.35 vs 9.89 ms in one run).  RIJK_TC_PAIR=0 / 1 turns
+  // both off / on.
   const char* e = getenv("RIJK_TC_PAIR");
   if (e && e[0] == '0') {
     t.pair = t.pair_rank = 0;
   } else if (e && e[0] == '1') {
     t.pair = t.pair_rank = 1;
   } else {
-    t.pair = 0;
-    t.pair_rank = t.nmb >= 8 ? 1 : 0;
+    t.pair = t.pair_rank = t.nmb >= 8 ? 1 : 0;
   }
+  // the paired half-transform reads every operand by tensor copies: only
+  // tensors whose planes the maps' 32-bit row index covers (V's halves are
+  // split in the paired layout, so this is decided before anything runs)
+  if (t.pair && (!tensor_map_encoder() || g.naux * ((int64_t)t.nmb * (t.nmb + 1) / 2) * 2 * TC_M > INT32_MAX))
+    t.pair = 0;
   return t;
 }
 
@@ -1152,13 +1179,40 @@ static void half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void*
     half_tc_ks<NPAD, 64>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, mhi, mlo, tm, jw);
 }
 
+// Rows of 64 BF16 of a plane (box 64 x box_rows), for the paired kernel's
+// direct blocks and V halves: one box is a contiguous run of the plane.
+static bool row_map(CUtensorMap* m, const void* plane, int64_t rows, int box_rows) {
+  auto enc = tensor_map_encoder();
+  if (!enc || rows <= 0 || rows > (int64_t)INT32_MAX || box_rows <= 0 || box_rows > 256) return false;
+  const cuuint64_t dims[2] = {64, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {128};  // bytes, dim 1
+  const cuuint32_t box[2] = {64, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(plane), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int NPAD>
 static void half_tc_pair(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
-                         const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st) {
+                         const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st,
+                         const TcJ* jw) {
   using C = HalfTcPair<NPAD>;
+  // the maps cover the whole split tensor (g.naux rows of squares), from p = 0
+  const int64_t nsq = (int64_t)t.nmb * (t.nmb + 1) / 2;
+  PairMaps maps;
+  const bool tm = mirror_map(&maps.mhi, Bhi, g.naux * nsq * 16) && mirror_map(&maps.mlo, Blo, g.naux * nsq * 16) &&
+                  row_map(&maps.dhi, Bhi, g.naux * nsq * 2 * TC_M, TC_M) &&
+                  row_map(&maps.dlo, Blo, g.naux * nsq * 2 * TC_M, TC_M) &&
+                  row_map(&maps.vhi, Vhi, (int64_t)t.nkb * NPAD, NPAD / 2) &&
+                  row_map(&maps.vlo, Vlo, (int64_t)t.nkb * NPAD, NPAD / 2);
+  if (!tm) {  // make_tc_geom pairs only what the maps cover; should an encode fail, say so and launch nothing
+    static const int map_err = DEV_TENSOR_MAP;
+    (void)cudaMemcpyAsync(err, &map_err, sizeof(int), cudaMemcpyHostToDevice, st);
+    return;
+  }
   auto kern = k_half_tc_pair<NPAD>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-  const int64_t per_p = tc_row_elems(g);
   const int64_t ntp = cdiv_t(np, 2) * t.nmb;  // (aux-row pair, row block) tiles
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1196,32 +1250,28 @@ static void half_tc_pair(const Geom& g, const TcGeom& t, const void* Bhi, const 
   }
   const int64_t pairs = std::max<int64_t>(1, std::min<int64_t>(ntp, resident));
   cfg.gridDim = dim3((unsigned)(2 * pairs), 1, 1);
-  const int64_t rows = g.naux * (int64_t)t.nmb * (t.nmb + 1) / 2 * 16;
-  CUtensorMap mhi, mlo;
-  const bool tm = mirror_map(&mhi, Bhi, rows) && mirror_map(&mlo, Blo, rows);
-  if (!tm) {
-    memset(&mhi, 0, sizeof(mhi));
-    memset(&mlo, 0, sizeof(mlo));
-  }
   count_launch();
   // a failed launch stays the thread's last CUDA error, which the caller checks
-  (void)cudaLaunchKernelEx(&cfg, kern, static_cast<const __nv_bfloat16*>(Bhi) + p0 * per_p,
-                     static_cast<const __nv_bfloat16*>(Blo) + p0 * per_p, t.nmb, t.nkb,
-                     static_cast<const __nv_bfloat16*>(Vhi), static_cast<const __nv_bfloat16*>(Vlo), t.nib, np, ntp,
-                     static_cast<__nv_bfloat16*>(Xhi), static_cast<__nv_bfloat16*>(Xlo), err, mhi, mlo, tm ? 1 : 0,
-                     p0);
+  (void)cudaLaunchKernelEx(&cfg, kern, t.nmb, t.nkb, t.nib, np, ntp, static_cast<__nv_bfloat16*>(Xhi),
+                           static_cast<__nv_bfloat16*>(Xlo), err, maps, p0, jw ? jw->Vd : nullptr, jw ? jw->ldv : 0,
+                           jw ? jw->ncols : 0, (int)g.n, jw ? jw->wpart : nullptr);
+  if (jw) {
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv_t(np, 8), 148 * 8));
+    count_launch();
+    k_tc_wreduce<<<blocks, 256, 0, st>>>(jw->wpart, np, 4 * t.nmb, jw->sgn, p0, jw->w);
+  }
 }
 
 void launch_half_tc(const Geom& g, const TcGeom& t, const void* Bhi, const void* Blo, int64_t p0, int64_t np,
                     const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st,
                     const TcJ* jw) {
-  if (t.pair && !jw) {
+  if (t.pair) {
     if (t.npad == 64)
-      half_tc_pair<64>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
+      half_tc_pair<64>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, jw);
     else if (t.npad == 128)
-      half_tc_pair<128>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
+      half_tc_pair<128>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, jw);
     else
-      half_tc_pair<256>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st);
+      half_tc_pair<256>(g, t, Bhi, Blo, p0, np, Vhi, Vlo, Xhi, Xlo, err, st, jw);
     return;
   }
   if (t.npad == 64)

@@ -40,8 +40,8 @@ def _split_k_occ(ctx, c, occ):
 @pytest.mark.parametrize("n,naux,nocc", [(64, 24, 8), (100, 40, 16), (200, 30, 40), (300, 20, 24), (520, 6, 72),
                                          (100, 41, 16), (520, 7, 72), (200, 31, 160), (390, 9, 130)])
 def test_split_exchange_is_exact_on_bf16_representable_input(ctx, monkeypatch, env, n, naux, nocc):
-    """Every kernel form: the defaults (one SM per half-transform tile with K 64
-    per stage, the rank update on SM pairs from eight 128-row blocks on), both
+    """Every kernel form: the defaults (one SM per tile with K 64 per stage,
+    both kernels on SM pairs from eight 128-row blocks on), both
     kernels on SM pairs (cta_group::2), and one SM each with K 32 per stage; odd
     aux counts (a pair whose second aux row is missing), odd 128-row block
     counts (K block groups with rows beyond n) and every column padding (64,
@@ -95,13 +95,19 @@ def test_split_lowrank_signed(ctx, n, naux, npos, nneg):
     assert np.max(np.abs(got - ref)) <= 1e-4 * np.max(np.abs(ref))
 
 
+@pytest.mark.parametrize("env", [{}, {"RIJK_TC_PAIR": "1"}])
 @pytest.mark.parametrize("n,naux,npos,nneg,exact", [(120, 41, 20, 12, True), (200, 30, 150, 0, True),
                                                     (260, 1000, 300, 40, False), (390, 500, 64, 70, False)])
-def test_split_lowrank_j_and_k(ctx, n, naux, npos, nneg, exact):
+def test_split_lowrank_j_and_k(ctx, monkeypatch, env, n, naux, npos, nneg, exact):
     """rijk_vjk_upper_lowrank_split_dev: J of dD = V S V^T from the split
     half-transform's epilogue and K of the same difference, against the FP64
     density-form builds; bit for bit on integer-valued input (every product and
-    sum exact), else within 1e-4 of max |J| and |K|."""
+    sum exact), else within 1e-4 of max |J| and |K|; with the half-transform on
+    one SM per tile and on SM pairs (odd aux counts: a pair without its second
+    row)."""
+    monkeypatch.delenv("RIJK_TC_PAIR", raising=False)
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
     import torch
 
     rng = np.random.default_rng(n + naux)
