@@ -886,19 +886,21 @@ __global__ void __launch_bounds__(128, 1)
 // Blocks below the diagonal (the (2c+1, 2c) block of a diagonal group) and
 // blocks beyond n are computed but not written.  Same partial layout as
 // k_rank_tc: part[(sp pairs + q) 128 x 128], q = Jb (Jb + 1) / 2 + Ib.
-// Synchronisation as in k_half_tc_pair (relay of CTA 1's stage arrivals, commit
-// multicast over the pair, bounded waits, a cluster barrier before release).
+// Synchronisation as in k_half_tc_pair (each CTA's X blocks by .cta_group::2
+// tensor copies completing on CTA 0's full barrier, which CTA 0 arms with both
+// CTAs' bytes; commit multicast over the pair, bounded waits, a cluster barrier
+// before release).  mxh / mxl: the X planes as rows of 64 BF16, box 64 x 128
+// (one 16 KB block).
 __global__ void __launch_bounds__(128, 1)
-    k_rank_tc_pair(const __nv_bfloat16* __restrict__ Xhi, const __nv_bfloat16* __restrict__ Xlo, int nmb, int nib,
+    k_rank_tc_pair(const __grid_constant__ CUtensorMap mxh, const __grid_constant__ CUtensorMap mxl, int nmb, int nib,
                    int npos_blocks, int64_t np, int splits, int64_t ngroups, float* __restrict__ part, int* err) {
   using C = RankTc;
   constexpr int S = C::STAGES;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_BYTES);  // used in CTA 0
   uint64_t* empty = full + S;
-  uint64_t* pfull = empty + S;
-  uint64_t* accf = pfull + S;
+  uint64_t* accf = empty + S;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t rank = cluster_ctarank();
@@ -916,7 +918,6 @@ __global__ void __launch_bounds__(128, 1)
     for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
-      mbar_init(&pfull[s], 1);
     }
     mbar_init(accf, 1);
     mbar_fence_init();
@@ -936,21 +937,21 @@ __global__ void __launch_bounds__(128, 1)
       const int64_t p = pa + t / nib;
       const int ib = (int)(t % nib);
       uint8_t* st = smem + s * C::STAGE_BYTES;
-      mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
-      const int64_t ao = ((p * nmb + Ia) * (int64_t)nib + ib) * BLOCK_ELEMS;
-      const int64_t bo = ((p * nmb + Ja) * (int64_t)nib + ib) * BLOCK_ELEMS;
-      bulk_g2s(st, Xhi + ao, BLOCK_BYTES, &full[s]);
-      bulk_g2s(st + BLOCK_BYTES, Xlo + ao, BLOCK_BYTES, &full[s]);
-      bulk_g2s(st + 2 * BLOCK_BYTES, Xhi + bo, BLOCK_BYTES, &full[s]);
-      bulk_g2s(st + 3 * BLOCK_BYTES, Xlo + bo, BLOCK_BYTES, &full[s]);
+      const uint32_t fb = cluster_addr(&full[s], 0);
+      if (rank == 0) mbar_arrive_expect_tx(&full[s], 2 * C::STAGE_BYTES);
+      const int ya = (int)(((p * nmb + Ia) * (int64_t)nib + ib) * TC_M);
+      const int yb = (int)(((p * nmb + Ja) * (int64_t)nib + ib) * TC_M);
+      tma2_load_2d(st, &mxh, 0, ya, fb);
+      tma2_load_2d(st + BLOCK_BYTES, &mxl, 0, ya, fb);
+      tma2_load_2d(st + 2 * BLOCK_BYTES, &mxh, 0, yb, fb);
+      tma2_load_2d(st + 3 * BLOCK_BYTES, &mxl, 0, yb, fb);
     }
   } else if (warp == 1 && lane == 0 && rank == 0) {
     constexpr uint32_t id_pos = idesc_bf16(2 * TC_M, 2 * TC_M, false);
     constexpr uint32_t id_neg = idesc_bf16(2 * TC_M, 2 * TC_M, true);
     for (int64_t t = 0; t < nsteps && ok; ++t) {
       const int s = (int)(t % S);
-      ok = mbar_wait_cluster_bounded(&full[s], (uint32_t)((t / S) & 1), err) &&
-           mbar_wait_cluster_bounded(&pfull[s], (uint32_t)((t / S) & 1), err);
+      ok = mbar_wait_cluster_bounded(&full[s], (uint32_t)((t / S) & 1), err);
       if (!ok) break;
       tc_fence_after();
       const int ib = (int)(t % nib);
@@ -971,12 +972,6 @@ __global__ void __launch_bounds__(128, 1)
       tc2_commit_pair(&empty[s]);
     }
     tc2_commit_pair(accf);
-  } else if (warp == 1 && lane == 0) {
-    for (int64_t t = 0; t < nsteps && ok; ++t) {
-      const int s = (int)(t % S);
-      ok = mbar_wait_cluster_bounded(&full[s], (uint32_t)((t / S) & 1), err);
-      if (ok) mbar_arrive_cluster(cluster_addr(&pfull[s], 0));
-    }
   }
   __syncwarp();
   const bool acc_ok = __syncthreads_and(ok) && nsteps > 0 && mbar_wait_cluster_bounded(accf, 0, err);
@@ -1294,7 +1289,9 @@ int tc_rank_splits(const TcGeom& t, int64_t np) {
 void launch_rank_tc(const Geom& g, const TcGeom& t, const void* Xhi, const void* Xlo, int64_t np, int npos_blocks,
                     int splits, float* part, int* err, cudaStream_t st) {
   const int64_t pairs = (int64_t)t.nmb * (t.nmb + 1) / 2;
-  if (t.pair_rank) {
+  CUtensorMap mxh, mxl;
+  const int64_t xrows = np * t.nmb * (int64_t)t.nib * TC_M;  // the chunk's X planes as rows of 64 BF16
+  if (t.pair_rank && row_map(&mxh, Xhi, xrows, TC_M) && row_map(&mxl, Xlo, xrows, TC_M)) {
     const int64_t nmg = cdiv_t(t.nmb, 2), ngroups = nmg * (nmg + 1) / 2;
     cudaFuncSetAttribute(k_rank_tc_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RankTc::SMEM);
     cudaLaunchAttribute attr[1];
@@ -1311,12 +1308,12 @@ void launch_rank_tc(const Geom& g, const TcGeom& t, const void* Xhi, const void*
     cfg.numAttrs = 1;
     count_launch();
     // a failed launch stays the thread's last CUDA error, which the caller checks
-    (void)cudaLaunchKernelEx(&cfg, k_rank_tc_pair, static_cast<const __nv_bfloat16*>(Xhi),
-                             static_cast<const __nv_bfloat16*>(Xlo), t.nmb, t.nib, npos_blocks, np, splits, ngroups,
-                             part, err);
+    (void)cudaLaunchKernelEx(&cfg, k_rank_tc_pair, mxh, mxl, t.nmb, t.nib, npos_blocks, np, splits, ngroups, part,
+                             err);
     (void)g;
     return;
   }
+  // one SM per K block (also where the X planes are beyond the maps' row index)
   cudaFuncSetAttribute(k_rank_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RankTc::SMEM);
   dim3 grid((unsigned)pairs, (unsigned)splits);
   count_launch();
