@@ -114,6 +114,9 @@ struct TcGeom {
   int64_t block_elems = 0;
   int pair = 0;       // half-transform on SM pairs (cta_group::2); V stored in column halves
   int pair_rank = 0;  // rank update on SM pairs (cta_group::2)
+  int ncols = 0;      // V columns actually used
+  int nv = 0;         // V rows per K block as laid out: the paired half-transform's MMA width
+                      // (ncols rounded up to 16, in two halves), else npad
 };
 TcGeom make_tc_geom(const Geom& g, int ncols);
 // BF16 elements of one plane (hi or lo) of the split tensor

@@ -595,13 +595,14 @@ struct PairMaps {
 
 template <int NPAD>
 __global__ void __launch_bounds__(192, 1)
-    k_half_tc_pair(int nmb, int nkb, int nib, int64_t np, int64_t ntp, __nv_bfloat16* __restrict__ Xhi,
+    k_half_tc_pair(int nmb, int nkb, int nib, int nv, int64_t np, int64_t ntp, __nv_bfloat16* __restrict__ Xhi,
                    __nv_bfloat16* __restrict__ Xlo, int* err, const __grid_constant__ PairMaps maps, int64_t p0,
                    const double* __restrict__ Vd, int64_t ldv, int ncols, int nrows, double* __restrict__ wpart) {
   const int64_t nsq = (int64_t)nmb * (nmb + 1) / 2;
   using C = HalfTcPair<NPAD>;
   constexpr int S = C::STAGES;
-  constexpr int NH = NPAD / 2;  // V columns (B rows) per CTA
+  const int NH = nv / 2;  // V columns (B rows) per CTA; nv: the MMA's N, a multiple of 16 up to NPAD
+  const uint32_t stage_tx = 2 * BLOCK_BYTES + 2 * (uint32_t)NH * TC_KB * 2;  // bytes one CTA lands per stage
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_BYTES);  // used in CTA 0
@@ -646,7 +647,7 @@ __global__ void __launch_bounds__(192, 1)
         if (!ok) break;
         uint8_t* st = smem + s * C::STAGE_BYTES;
         const uint32_t fb = cluster_addr(&full[s], 0);
-        if (lane == 0 && rank == 0) mbar_arrive_expect_tx(&full[s], 2 * C::STAGE_BYTES);
+        if (lane == 0 && rank == 0) mbar_arrive_expect_tx(&full[s], 2 * stage_tx);
         __syncwarp();
         const int Kb = kb >> 1, j = kb & 1;
         if (mb <= Kb) {
@@ -666,8 +667,8 @@ __global__ void __launch_bounds__(192, 1)
     }
   } else if (warp == 1) {
     if (lane == 0 && rank == 0) {
-      constexpr uint32_t idesc_k = idesc_bf16(2 * TC_M, NPAD, false);
-      constexpr uint32_t idesc_mn = idesc_bf16(2 * TC_M, NPAD, false, true);
+      const uint32_t idesc_k = idesc_bf16(2 * TC_M, nv, false);
+      const uint32_t idesc_mn = idesc_bf16(2 * TC_M, nv, false, true);
       for (int64_t lt = 0; lt < my_tiles && ok; ++lt) {
         const int b = (int)(lt & 1);
         const int mb = (int)((pair + lt * NPR) % nmb);
@@ -726,7 +727,12 @@ __global__ void __launch_bounds__(192, 1)
 #pragma unroll 1
         for (int c0 = 0; c0 < NPAD; c0 += 32) {
           float v[32];
-          tc_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * NPAD + c0), v);
+          if (c0 < nv)  // warp-uniform
+            tc_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * NPAD + c0), v);
+          // X's columns from nv on (beyond the MMA's N) are written as zeros
+#pragma unroll
+          for (int i = 0; i < 32; ++i)
+            if (c0 + i >= nv) v[i] = 0.0f;
           // with wpart: this row's share of J's scalar <V, X_P> (V in FP64)
           if (wpart && row < nrows) {
 #pragma unroll 8
@@ -782,7 +788,7 @@ __device__ __forceinline__ int64_t tri_root_tc(int64_t t) {
 
 __global__ void __launch_bounds__(128, 1)
     k_rank_tc(const __nv_bfloat16* __restrict__ Xhi, const __nv_bfloat16* __restrict__ Xlo, int nmb, int nib,
-              int npos_blocks, int64_t np, int splits, float* __restrict__ part, int* err) {
+              int ncols, int npos_blocks, int64_t np, int splits, float* __restrict__ part, int* err) {
   using C = RankTc;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -841,6 +847,7 @@ __global__ void __launch_bounds__(128, 1)
       const uint8_t* st = smem + s * C::STAGE_BYTES;
 #pragma unroll
       for (int ks = 0; ks < TC_KB / 16; ++ks) {
+        if (ib * TC_KB + ks * 16 >= ncols) break;  // X's padding columns: no work
         const uint32_t kof = 2 * ks * (TC_M / 8) * 128;
         const uint64_t dah = smem_desc(st + kof, (TC_M / 8) * 128, 128);
         const uint64_t dal = smem_desc(st + BLOCK_BYTES + kof, (TC_M / 8) * 128, 128);
@@ -893,7 +900,8 @@ __global__ void __launch_bounds__(128, 1)
 // (one 16 KB block).
 __global__ void __launch_bounds__(128, 1)
     k_rank_tc_pair(const __grid_constant__ CUtensorMap mxh, const __grid_constant__ CUtensorMap mxl, int nmb, int nib,
-                   int npos_blocks, int64_t np, int splits, int64_t ngroups, float* __restrict__ part, int* err) {
+                   int ncols, int npos_blocks, int64_t np, int splits, int64_t ngroups, float* __restrict__ part,
+                   int* err) {
   using C = RankTc;
   constexpr int S = C::STAGES;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -959,6 +967,7 @@ __global__ void __launch_bounds__(128, 1)
       const uint8_t* st = smem + s * C::STAGE_BYTES;
 #pragma unroll
       for (int ks = 0; ks < TC_KB / 16; ++ks) {
+        if (ib * TC_KB + ks * 16 >= ncols) break;  // X's padding columns: no work
         const uint32_t kof = 2 * ks * (TC_M / 8) * 128;
         const uint64_t dah = smem_desc(st + kof, (TC_M / 8) * 128, 128);
         const uint64_t dal = smem_desc(st + BLOCK_BYTES + kof, (TC_M / 8) * 128, 128);
@@ -1051,6 +1060,10 @@ TcGeom make_tc_geom(const Geom& g, int ncols) {
   // split in the paired layout, so this is decided before anything runs)
   if (t.pair && (!tensor_map_encoder() || g.naux * ((int64_t)t.nmb * (t.nmb + 1) / 2) * 2 * TC_M > INT32_MAX))
     t.pair = 0;
+  // the paired MMAs run N = ncols rounded up to 16 (16..256) rather than the
+  // 64 / 128 / 256 of X's layout: 200 occupied columns take N = 208, not 256
+  t.ncols = ncols;
+  t.nv = t.pair ? std::min(t.npad, std::max(16, (ncols + 15) / 16 * 16)) : t.npad;
   return t;
 }
 
@@ -1075,10 +1088,10 @@ void launch_split_tensor(const Geom& g, const double* B, int64_t p0, int64_t np,
 
 void launch_split_cols(const Geom& g, const TcGeom& t, const double* V, int64_t ldv, int ncols, void* hi, void* lo,
                        cudaStream_t st) {
-  const int64_t total = (int64_t)t.npad * TC_KB * t.nkb;
+  const int64_t total = (int64_t)(t.pair ? t.nv : t.npad) * TC_KB * t.nkb;
   const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv_t(total, 256), 148 * 8));
   count_launch();
-  k_split_cols<<<blocks, 256, 0, st>>>(V, ldv, g.n, ncols, t.npad, t.nkb, t.pair ? 2 : 1,
+  k_split_cols<<<blocks, 256, 0, st>>>(V, ldv, g.n, ncols, t.pair ? t.nv : t.npad, t.nkb, t.pair ? 2 : 1,
                                        static_cast<__nv_bfloat16*>(hi), static_cast<__nv_bfloat16*>(lo));
 }
 
@@ -1199,8 +1212,8 @@ static void half_tc_pair(const Geom& g, const TcGeom& t, const void* Bhi, const 
   const bool tm = mirror_map(&maps.mhi, Bhi, g.naux * nsq * 16) && mirror_map(&maps.mlo, Blo, g.naux * nsq * 16) &&
                   row_map(&maps.dhi, Bhi, g.naux * nsq * 2 * TC_M, TC_M) &&
                   row_map(&maps.dlo, Blo, g.naux * nsq * 2 * TC_M, TC_M) &&
-                  row_map(&maps.vhi, Vhi, (int64_t)t.nkb * NPAD, NPAD / 2) &&
-                  row_map(&maps.vlo, Vlo, (int64_t)t.nkb * NPAD, NPAD / 2);
+                  row_map(&maps.vhi, Vhi, (int64_t)t.nkb * t.nv, t.nv / 2) &&
+                  row_map(&maps.vlo, Vlo, (int64_t)t.nkb * t.nv, t.nv / 2);
   if (!tm) {  // make_tc_geom pairs only what the maps cover; should an encode fail, say so and launch nothing
     static const int map_err = DEV_TENSOR_MAP;
     (void)cudaMemcpyAsync(err, &map_err, sizeof(int), cudaMemcpyHostToDevice, st);
@@ -1247,7 +1260,7 @@ static void half_tc_pair(const Geom& g, const TcGeom& t, const void* Bhi, const 
   cfg.gridDim = dim3((unsigned)(2 * pairs), 1, 1);
   count_launch();
   // a failed launch stays the thread's last CUDA error, which the caller checks
-  (void)cudaLaunchKernelEx(&cfg, kern, t.nmb, t.nkb, t.nib, np, ntp, static_cast<__nv_bfloat16*>(Xhi),
+  (void)cudaLaunchKernelEx(&cfg, kern, t.nmb, t.nkb, t.nib, t.nv, np, ntp, static_cast<__nv_bfloat16*>(Xhi),
                            static_cast<__nv_bfloat16*>(Xlo), err, maps, p0, jw ? jw->Vd : nullptr, jw ? jw->ldv : 0,
                            jw ? jw->ncols : 0, (int)g.n, jw ? jw->wpart : nullptr);
   if (jw) {
@@ -1308,8 +1321,8 @@ void launch_rank_tc(const Geom& g, const TcGeom& t, const void* Xhi, const void*
     cfg.numAttrs = 1;
     count_launch();
     // a failed launch stays the thread's last CUDA error, which the caller checks
-    (void)cudaLaunchKernelEx(&cfg, k_rank_tc_pair, mxh, mxl, t.nmb, t.nib, npos_blocks, np, splits, ngroups, part,
-                             err);
+    (void)cudaLaunchKernelEx(&cfg, k_rank_tc_pair, mxh, mxl, t.nmb, t.nib, t.ncols, npos_blocks, np, splits, ngroups,
+                             part, err);
     (void)g;
     return;
   }
@@ -1318,8 +1331,8 @@ void launch_rank_tc(const Geom& g, const TcGeom& t, const void* Xhi, const void*
   dim3 grid((unsigned)pairs, (unsigned)splits);
   count_launch();
   k_rank_tc<<<grid, 128, RankTc::SMEM, st>>>(static_cast<const __nv_bfloat16*>(Xhi),
-                                             static_cast<const __nv_bfloat16*>(Xlo), t.nmb, t.nib, npos_blocks, np,
-                                             splits, part, err);
+                                             static_cast<const __nv_bfloat16*>(Xlo), t.nmb, t.nib, t.ncols,
+                                             npos_blocks, np, splits, part, err);
   (void)g;
 }
 
