@@ -1041,19 +1041,20 @@ TcGeom make_tc_geom(const Geom& g, int ncols) {
   t.npad = ncols <= 64 ? 64 : ncols <= 128 ? 128 : 256;
   t.nib = t.npad / TC_KB;
   t.block_elems = BLOCK_ELEMS;
-  // SM-pair (cta_group::2) kernels: measured on B200 at n = 600 / 1200, the
-  // paired rank update is faster from about eight 128-row blocks on (5.46 vs
-  // 6.25 ms at n = 1200, slower at n = 600 where each CTA has few k steps);
-  // the paired half-transform, its copies completing on CTA 0's barrier, is
-  // faster at n = 1200 (8.35 vs 9.89 ms in one run).  RIJK_TC_PAIR=0 / 1 turns
-  // both off / on.
+  // SM-pair (cta_group::2) kernels, their copies completing on CTA 0's
+  // barrier: measured on B200 (one SM per tile -> pair, ms), the half-transform
+  // n = 600: 0.754 -> 0.698, 768: 1.442 -> 1.348, 1200: 9.86 -> 8.05; the rank
+  // update n = 600: 0.387 -> 0.472 (few k steps per CTA), 768: 0.745 -> 0.593,
+  // 1200: 6.28 -> 4.38.  So the half-transform pairs from five 128-row blocks,
+  // the rank update from six.  RIJK_TC_PAIR=0 / 1 turns both off / on.
   const char* e = getenv("RIJK_TC_PAIR");
   if (e && e[0] == '0') {
     t.pair = t.pair_rank = 0;
   } else if (e && e[0] == '1') {
     t.pair = t.pair_rank = 1;
   } else {
-    t.pair = t.pair_rank = t.nmb >= 8 ? 1 : 0;
+    t.pair = t.nmb >= 5 ? 1 : 0;
+    t.pair_rank = t.nmb >= 6 ? 1 : 0;
   }
   // the paired half-transform reads every operand by tensor copies: only
   // tensors whose planes the maps' 32-bit row index covers (V's halves are

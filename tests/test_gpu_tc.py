@@ -41,7 +41,8 @@ def _split_k_occ(ctx, c, occ):
                                          (100, 41, 16), (520, 7, 72), (200, 31, 160), (390, 9, 130)])
 def test_split_exchange_is_exact_on_bf16_representable_input(ctx, monkeypatch, env, n, naux, nocc):
     """Every kernel form: the defaults (one SM per tile with K 64 per stage,
-    both kernels on SM pairs from eight 128-row blocks on), both
+    the half-transform on SM pairs from five 128-row blocks on and the rank
+    update from six), both
     kernels on SM pairs (cta_group::2), and one SM each with K 32 per stage; odd
     aux counts (a pair whose second aux row is missing), odd 128-row block
     counts (K block groups with rows beyond n) and every column padding (64,
