@@ -260,7 +260,10 @@ struct HalfTcP {
 // seen as rows of 1024 BF16 (one group of 8 rows of a square, all 16 of its K
 // groups), as dims {256, 4, rows}; the box {256, 2, 16} at (0, 2 j, 16 square)
 // is K half j of the square's 16 row groups, landing at 1 KB per group.
-template <int NPAD, int KS>
+// WJ: with J's epilogue (wpart non-null).  A separate instantiation, because
+// its loop over the accumulator's columns indexes v at run time, which puts v
+// in local memory; without J, v stays in registers.
+template <int NPAD, int KS, bool WJ>
 __global__ void __launch_bounds__(192, 1)
     k_half_tc_persistent(const __nv_bfloat16* __restrict__ Bhi, const __nv_bfloat16* __restrict__ Blo, int nmb,
                          int nkb, const __nv_bfloat16* __restrict__ Vhi, const __nv_bfloat16* __restrict__ Vlo,
@@ -414,10 +417,12 @@ __global__ void __launch_bounds__(192, 1)
       for (int c0 = 0; c0 < NPAD; c0 += 32) {
         float v[32];
         tc_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * NPAD + c0), v);
-        if (wpart && row < nrows) {
+        if constexpr (WJ) {
+          if (row < nrows) {
 #pragma unroll 8
-          for (int jj = 0; jj < 32 && c0 + jj < ncols; ++jj)
-            jacc = fma((double)v[jj], Vd[(int64_t)(c0 + jj) * ldv + row], jacc);
+            for (int jj = 0; jj < 32 && c0 + jj < ncols; ++jj)
+              jacc = fma((double)v[jj], Vd[(int64_t)(c0 + jj) * ldv + row], jacc);
+          }
         }
         const int ib = c0 / TC_KB;
 #pragma unroll
@@ -433,7 +438,7 @@ __global__ void __launch_bounds__(192, 1)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[b]);
-      if (wpart) {
+      if constexpr (WJ) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) jacc += __shfl_xor_sync(0xffffffffu, jacc, o);
         if (lane == 0) wpart[tile * 4 + quad] = jacc;
@@ -593,7 +598,7 @@ struct PairMaps {
   CUtensorMap dhi, dlo, mhi, mlo, vhi, vlo;
 };
 
-template <int NPAD>
+template <int NPAD, bool WJ>
 __global__ void __launch_bounds__(192, 1)
     k_half_tc_pair(int nmb, int nkb, int nib, int nv, int64_t np, int64_t ntp, __nv_bfloat16* __restrict__ Xhi,
                    __nv_bfloat16* __restrict__ Xlo, int* err, const __grid_constant__ PairMaps maps, int64_t p0,
@@ -734,10 +739,12 @@ __global__ void __launch_bounds__(192, 1)
           for (int i = 0; i < 32; ++i)
             if (c0 + i >= nv) v[i] = 0.0f;
           // with wpart: this row's share of J's scalar <V, X_P> (V in FP64)
-          if (wpart && row < nrows) {
+          if constexpr (WJ) {
+            if (row < nrows) {
 #pragma unroll 8
-            for (int jj = 0; jj < 32 && c0 + jj < ncols; ++jj)
-              jacc = fma((double)v[jj], Vd[(int64_t)(c0 + jj) * ldv + row], jacc);
+              for (int jj = 0; jj < 32 && c0 + jj < ncols; ++jj)
+                jacc = fma((double)v[jj], Vd[(int64_t)(c0 + jj) * ldv + row], jacc);
+            }
           }
           const int ib = c0 / TC_KB;
 #pragma unroll
@@ -754,7 +761,7 @@ __global__ void __launch_bounds__(192, 1)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive_cluster(b ? acc_empty1 : acc_empty0);
-      if (wpart && pl < np) {
+      if (WJ && pl < np) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) jacc += __shfl_xor_sync(0xffffffffu, jacc, o);
         if (lane == 0) wpart[(pl * nmb + mb) * 4 + quad] = jacc;
@@ -1142,12 +1149,13 @@ static void half_tc_ks(const Geom& g, const TcGeom& t, const void* Bhi, const vo
                        const void* Vhi, const void* Vlo, void* Xhi, void* Xlo, int* err, cudaStream_t st,
                        const CUtensorMap& mhi, const CUtensorMap& mlo, bool tm, const TcJ* jw) {
   using C = HalfTcP<NPAD, KS>;
-  cudaFuncSetAttribute(k_half_tc_persistent<NPAD, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+  auto kern = jw ? k_half_tc_persistent<NPAD, KS, true> : k_half_tc_persistent<NPAD, KS, false>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
   const int64_t per_p = tc_row_elems(g);
   const int64_t ntiles = np * t.nmb;
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, sm_count()));
   count_launch();
-  k_half_tc_persistent<NPAD, KS><<<grid, 192, C::SMEM, st>>>(
+  kern<<<grid, 192, C::SMEM, st>>>(
       static_cast<const __nv_bfloat16*>(Bhi) + p0 * per_p, static_cast<const __nv_bfloat16*>(Blo) + p0 * per_p,
       t.nmb, t.nkb, static_cast<const __nv_bfloat16*>(Vhi), static_cast<const __nv_bfloat16*>(Vlo), t.nib, ntiles,
       static_cast<__nv_bfloat16*>(Xhi), static_cast<__nv_bfloat16*>(Xlo), err, mhi, mlo, tm ? 1 : 0, p0,
@@ -1220,7 +1228,7 @@ static void half_tc_pair(const Geom& g, const TcGeom& t, const void* Bhi, const 
     (void)cudaMemcpyAsync(err, &map_err, sizeof(int), cudaMemcpyHostToDevice, st);
     return;
   }
-  auto kern = k_half_tc_pair<NPAD>;
+  auto kern = jw ? k_half_tc_pair<NPAD, true> : k_half_tc_pair<NPAD, false>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
   const int64_t ntp = cdiv_t(np, 2) * t.nmb;  // (aux-row pair, row block) tiles
   cudaLaunchAttribute attr[1];
