@@ -889,6 +889,7 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
     # the pool only while held plus new memory stays within the budget, else
     # the pool is closed and the group starts afresh.
     pool, held = [], []
+    group_iters = 0  # batched iterations run: per group, its slowest molecule's count
     try:
         for idx in reversed(groups):
             idx = sorted(idx, key=lambda i: -need[i])
@@ -915,6 +916,7 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
                 teardown += time.perf_counter() - tt
             setup += r.setup_s
             scf += r.scf_s
+            group_iters += max(r.iterations) if r.iterations else 0
             for k in eig:
                 eig[k] += r.timings["eigensolves"][k]
             for k, v in list(r.timings["setup_parts"].items()) + list(r.timings["scf_parts"].items()):
@@ -932,6 +934,7 @@ def run_molecule_set(mols: list, basis: str, auxbas: str, group_size: int = 64, 
         teardown += time.perf_counter() - tt
     parts["teardown"] = teardown
     parts["groups"] = len(groups)
+    parts["group_iterations"] = group_iters
     parts["free_bytes_at_start"] = float(budget / memory_fraction)
     return BatchResult(energies, conv, iters, setup, scf,
                        {"fp64_k_builds": nfp64, "split_k_builds": nsplit, "eigensolves": eig, "setup_parts": parts},
