@@ -81,20 +81,19 @@ def shell_rotation(l: int, F: np.ndarray) -> np.ndarray:
 
 @dataclass
 class Frames:
-    xyz: np.ndarray  # (na, 3) coordinates in A
-    origin: np.ndarray  # (nw, 3) each water's O
+    xyz: np.ndarray  # (na, 3) coordinates in A; water w's origin is its O, xyz[3 w]
     F: np.ndarray  # (nw, 3, 3) each water's frame, axes as rows
 
 
 def water_frames(mol) -> Frames:
-    """Per water (atoms 3w, 3w+1, 3w+2 = O, H1, H2): origin (A) and frame F (rows),
-    all waters at once."""
+    """Per water (atoms 3w, 3w+1, 3w+2 = O, H1, H2): its frame F (rows), all
+    waters at once; the frame's origin is the water's O."""
     xyz = np.asarray(mol.coords, dtype=np.float64) * ANG
     nw = len(mol.symbols) // 3
     if list(mol.symbols) != ["O", "H", "H"] * nw:
         raise ValueError("the learned guess is trained on water clusters (atoms ordered O, H, H per water)")
     w = xyz.reshape(nw, 3, 3)
-    o, h1, h2 = w[:, 0], w[:, 1] - w[:, 0], w[:, 2] - w[:, 0]
+    h1, h2 = w[:, 1] - w[:, 0], w[:, 2] - w[:, 0]
     p = h1 - h2
     b = h1 + h2
     p = p / np.linalg.norm(p, axis=1, keepdims=True)
@@ -102,7 +101,7 @@ def water_frames(mol) -> Frames:
     b = b / np.linalg.norm(b, axis=1, keepdims=True)
     n = np.stack([p[:, 1] * b[:, 2] - p[:, 2] * b[:, 1], p[:, 2] * b[:, 0] - p[:, 0] * b[:, 2],
                   p[:, 0] * b[:, 1] - p[:, 1] * b[:, 0]], axis=1)
-    return Frames(xyz, o.copy(), np.stack([p, b, n], axis=1))
+    return Frames(xyz, np.stack([p, b, n], axis=1))
 
 
 def atom_layout(sh):
