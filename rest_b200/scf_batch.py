@@ -727,10 +727,13 @@ class BatchedRHF:
             err = F @ D @ self.S
             err = err - err.transpose(1, 2)
             act = torch.tensor(active, device=self.dev)
-            slot = torch.tensor([count[i] % m for i in range(B)], device=self.dev)
-            rows = torch.arange(B, device=self.dev)
-            err_hist[rows[act], slot[act]] = err[act].reshape(int(act.sum()), -1)
-            f_hist[rows[act], slot[act]] = F[act]
+            # the active molecules' rows as an index built on the host: no
+            # device-to-host synchronisation (a boolean mask would need one)
+            live = [i for i in range(B) if active[i]]
+            rows = torch.tensor(live, device=self.dev)
+            slot = torch.tensor([count[i] % m for i in live], device=self.dev)
+            err_hist[rows, slot] = err.index_select(0, rows).reshape(len(live), -1)
+            f_hist[rows, slot] = F.index_select(0, rows)
             for i in range(B):
                 if active[i]:
                     count[i] += 1
