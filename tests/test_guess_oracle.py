@@ -111,3 +111,21 @@ def test_pair_layout_and_row_arithmetic_match_host_assembly_inputs():
                 if b >= a:
                     rows.append((a, b, off[a] + r, off[b] + int(near[b, :a].sum())))
         assert np.array_equal(np.array(rows, dtype=np.int32), up)
+
+
+def test_pair_layout_refuses_what_the_geometry_kernels_cannot_take():
+    """The host checks in front of rijk_guess_geometry: atoms not ordered O, H, H
+    per water, an empty molecule or set, and element blocks beyond 14 functions
+    or l > 2 are refused before anything reaches the device."""
+    import pytest
+
+    from rest_b200.guess import pair_layout
+
+    bad_order = Molecule.from_angstrom(["H", "O", "H"], [[0, 0, 0], [0, 0, 1], [0, 1, 0]])
+    empty = Molecule.from_angstrom([], np.zeros((0, 3)))
+    water = water_cluster(2, seed=1)
+    for mols in ([bad_order], [water, empty], []):
+        with pytest.raises(ValueError):
+            pair_layout(mols, "def2-SVP")
+    with pytest.raises(ValueError, match="14 functions"):
+        pair_layout([water], "aug-cc-pV5Z")
