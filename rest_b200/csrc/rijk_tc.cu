@@ -27,6 +27,13 @@
 // seen with the rows and K exchanged, are the MN-major canonical layout (each
 // core matrix is 8 K-rows of 16 bytes along M), which the MMA takes with the
 // A-major bit of the instruction descriptor set.
+//
+// Kernel forms (make_tc_geom chooses): one SM per tile, or a cluster of two
+// SMs running M = 256 MMAs (cta_group::2) whose copies complete on the first
+// CTA's barrier.  The paired half-transform runs N = the used columns rounded
+// up to 16 (V laid out at that width, in two halves); the rank updates skip the
+// k-steps of X's padding columns.  J's scalars w_P = <V, X_P> can come out of
+// the half-transform's epilogue (a separate instantiation).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
